@@ -1,0 +1,198 @@
+/*
+ * ocfd_ec_gpu.h -- C-ABI of the B200 (sm_100a) implementation of the OpenCFD-EC 3D v1.16a
+ * per-iteration hot path: multi-block residual (MUSCL/WENO reconstruction, Roe/HLLC/AUSMPW/
+ * Van Leer/Steger-Warming/HLL fluxes, central viscous fluxes, SA/SST sources), LU-SGS and RK3
+ * updates, flow limiter, physical boundary conditions, block-interface halos, residual norms
+ * and force integration.
+ *
+ * Plain C: pointers and sizes only, no C++ or torch types. Every entry point returns 0
+ * (OCFD_OK) or a negative OCFD_ERR_* code; ocfd_last_error() returns a message for the last
+ * failing call on a handle.
+ *
+ * Index conventions follow the reference (sub_modules.f90:20, sub_init.f90:444-541):
+ *   a block with nx,ny,nz NODES has (nx-1)(ny-1)(nz-1) cells indexed 1..n-1; cell arrays carry
+ *   LAP=4 ghost layers (1-LAP..n+LAP-1); all host arrays are Fortran column-major (first index
+ *   fastest).  The conserved state at the boundary is the Fortran array
+ *   U(NVAR, 1-LAP:nx+LAP-1, 1-LAP:ny+LAP-1, 1-LAP:nz+LAP-1) (sub_init.f90:469).
+ *
+ * Connectivity is the reference's internal .inc record: 21 ints per subface, in the field
+ * order ib,ie,jb,je,kb,ke,bc,face,f_no, ib1,ie1,jb1,je1,kb1,ke1,nb1,face1,f_no1,L1,L2,L3
+ * (sub_IO.f90:700-705; produced from Gridgen bc3d.inp by sub_convert_inp.f90:25-248).
+ * Block numbers nb1 are 1-based like the reference.
+ */
+#ifndef OCFD_EC_GPU_H
+#define OCFD_EC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OCFD_ABI_VERSION 1
+
+/* error codes */
+#define OCFD_OK 0
+#define OCFD_ERR_ARG (-1)         /* bad argument / unsupported option                       */
+#define OCFD_ERR_CUDA (-2)        /* CUDA runtime error                                       */
+#define OCFD_ERR_OOM (-3)         /* device allocation failed                                 */
+#define OCFD_ERR_NAN (-4)         /* NaN in the residual (replaces the reference's `stop`,
+                                     sub_time_advance.f90:358-365)                            */
+#define OCFD_ERR_TIMEOUT (-5)     /* a bounded device-side wait gave up                       */
+#define OCFD_ERR_UNSUPPORTED (-6) /* boundary type / model outside the implemented hot path  */
+#define OCFD_ERR_NOSYM (-7)       /* a required symbol or library is missing                  */
+
+/* numeric constants of the reference (sub_modules.f90:21-47) */
+#define OCFD_SCHEME_UD1 0
+#define OCFD_SCHEME_NND2 1
+#define OCFD_SCHEME_UD3 2
+#define OCFD_SCHEME_MUSCL2U 3
+#define OCFD_SCHEME_MUSCL2C 4
+#define OCFD_SCHEME_MUSCL3 5
+#define OCFD_SCHEME_OMUSCL2 6
+#define OCFD_SCHEME_WENO5 7
+#define OCFD_SCHEME_UD5 8
+#define OCFD_SCHEME_WENO7 9
+#define OCFD_SCHEME_CD2 20
+#define OCFD_SCHEME_NONE (-1)
+#define OCFD_FLUX_STEGER_WARMING 1
+#define OCFD_FLUX_HLL 2
+#define OCFD_FLUX_HLLC 3
+#define OCFD_FLUX_ROE 4
+#define OCFD_FLUX_VAN_LEER 5
+#define OCFD_FLUX_AUSM 6 /* dispatches to AUSMPW, as the reference does (sub_Residual.f90:326) */
+#define OCFD_BC_WALL 2
+#define OCFD_BC_SYMMETRY 3
+#define OCFD_BC_FARFIELD 4
+#define OCFD_BC_INFLOW 5
+#define OCFD_BC_OUTFLOW 6
+#define OCFD_BC_EXTRAPOLATE 401
+#define OCFD_BC_INNER (-1)
+#define OCFD_TIME_LU_SGS 0
+#define OCFD_TIME_RK3 3
+#define OCFD_TURB_NONE 0
+#define OCFD_TURB_SA 2
+#define OCFD_TURB_SST 3
+
+/* precision modes */
+#define OCFD_PREC_FP64 0  /* plain FP64 everywhere (parity path)                               */
+#define OCFD_PREC_MIXED 1 /* FP32 reconstruction/fluxes/sources/metrics/Res/dt/Lc/Lv;
+                             FP64 state U, DU, LU-SGS diagonal + divide, norms, forces       */
+
+/*
+ * Flow and control parameters: the namelist &control_ec values of the reference
+ * (sub_read_parameter.f90:114-129) AFTER set_const_para (sub_read_parameter.f90:371-429),
+ * i.e. exactly the Fortran module variables of Global_Var once read_parameter returns:
+ * aoa/aos/a_alfa/a_beta in radians, twall divided by t_inf, lpmin/lpmax divided by
+ * gamma*Ma^2, cv/cp derived. ocfd_default_params() + ocfd_finalize_params() reproduce
+ * set_default_parameter + set_const_para for callers that start from raw namelist values.
+ */
+typedef struct ocfd_params {
+  int nvar;                   /* NVAR: 5 (laminar/Euler), 6 (SA), 7 (SST)                  */
+  int iflag_scheme;           /* interior reconstruction scheme id                          */
+  int bound_scheme;           /* scheme for faces < LAP from a physical boundary           */
+  int iflag_flux;             /* flux id                                                     */
+  int iflag_reconstruction;   /* 0 primitive, 1 conservative, 2 characteristic              */
+  int iflag_turbulence_model; /* 0, 2 (SA) or 3 (SST)                                       */
+  int time_method;            /* 0 LU-SGS, 3 RK3                                            */
+  int if_viscous;             /* 0 Euler, 1 Navier-Stokes                                   */
+  int iflag_local_dt;         /* 1 local time step, 0 global                               */
+  int if_dtime_mesh;          /* 1: scale dt by the mesh-quality factor                    */
+  int iflag_limit_flow;       /* 1: flow limiter after every update                        */
+  int if_scheme_positivity;   /* 1: first-order fallback on negative rho/p after reconstr. */
+  int cood_y_up;              /* 1: y axis up, 0: z axis up                                */
+  int precision;              /* OCFD_PREC_FP64 or OCFD_PREC_MIXED                         */
+  double ma, re, gamma, prl, prt, t_inf, twall, kt_inf, wt_inf;
+  double aoa, aos, a_alfa, a_beta; /* radians                                               */
+  double cfl, dt_global, dtmin, dtmax, w_lu, mut_max, p_outlet;
+  double ldmin, ldmax, lpmin, lpmax, lumax, lsamax;
+  double ref_s, ref_l, centroid[3];
+  double cv, cp;
+} ocfd_params;
+
+/* Opaque solver handle: all blocks of one case resident on one GPU. */
+typedef struct ocfd_handle ocfd_handle;
+
+/* ---- parameters --------------------------------------------------------------------- */
+
+/* Defaults of set_default_parameter (sub_read_parameter.f90:30-106); raw (pre-set_const) form,
+ * angles in degrees, twall in K. */
+int ocfd_default_params(ocfd_params* p);
+/* set_const_para (sub_read_parameter.f90:371-429): derives nvar, converts angles to radians,
+ * twall/=t_inf, scales lpmin/lpmax, maps a_alfa/a_beta by cood_y_up, computes cv/cp. */
+int ocfd_finalize_params(ocfd_params* p);
+
+/* ---- lifetime ------------------------------------------------------------------------- */
+
+/*
+ * Creates a case on the current CUDA device (replaces the per-block part of Init,
+ * sub_init.f90:7-54, for the hot path):
+ *   nblk            number of blocks
+ *   nijk[3*b..]     nodes nx,ny,nz of block b (b = 0..nblk-1)
+ *   xyz[b]          node coordinates of block b, 3*nx*ny*nz doubles: x(1:nx,1:ny,1:nz) then y
+ *                   then z, i fastest (the PLOT3D record read at sub_IO.f90:36-44)
+ *   nsub[b]         subfaces of block b
+ *   inc             concatenated .inc records, 21 ints per subface, blocks in order
+ *   dw[b]           wall distance at cell centres ((nx-1)(ny-1)(nz-1) doubles) or NULL; when the
+ *                   pointer array itself is NULL and a turbulence model is on, the distance is
+ *                   computed on the device (sub_comput_dw.f90:43-101)
+ * Geometry (coordinate ghosts sub_update_buffer_mpi.f90:230-512, metrics sub_geometry.f90:6-346,
+ * mesh-quality dt factor sub_geometry.f90:361-515) is computed on the device.  The flow is set
+ * to freestream (init_flow_zero, sub_init.f90:302-410) with BC + halo applied.
+ */
+int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, const double* const* xyz,
+                const int* nsub, const int* inc, const double* const* dw, ocfd_handle** out);
+int ocfd_destroy(ocfd_handle* h);
+const char* ocfd_last_error(const ocfd_handle* h);
+
+/* ---- state ---------------------------------------------------------------------------- */
+
+/* Number of doubles in the Fortran U array of block b: NVAR*(nx+7)*(ny+7)*(nz+7). */
+long long ocfd_state_size(const ocfd_handle* h, int blk);
+/* Copy the Fortran-layout U(NVAR,1-LAP:n+LAP-1,...) of block blk to / from the device. */
+int ocfd_set_state(ocfd_handle* h, int blk, const double* U);
+int ocfd_get_state(ocfd_handle* h, int blk, double* U);
+/* Re-initialise to freestream (Init_flow with Iflag_init=0, sub_init.f90:264-438). */
+int ocfd_init_flow(ocfd_handle* h);
+
+/* ---- the hot path --------------------------------------------------------------------- */
+
+/*
+ * nsteps calls of NS_Time_advance(1) (sub_time_advance.f90:6-23; the driver call at
+ * opencfd_ec3d_v1.16a.f90:167): residual + LU-SGS (or the 3 RK3 stages), U update, flow
+ * limiter, BC, halo, vt/k/w clamps.  kstep and tt (may be NULL) receive the step counter and
+ * time after the last step (tt advances by dt_global per step, sub_time_advance.f90:115).
+ * Asynchronous on the device; the NaN check happens in ocfd_residual.
+ */
+int ocfd_advance(ocfd_handle* h, int nsteps, int* kstep, double* tt);
+
+/* Comput_Residual_one_mesh (sub_Residual.f90:14-127) alone: the residual Res, the local time
+ * step and, when with_lusgs != 0, the LU-SGS increment DU from the current state, without
+ * updating U.  Used to check one residual evaluation in isolation. */
+int ocfd_compute_residual(ocfd_handle* h, int with_lusgs);
+
+/* comput_max_Res_onemesh (sub_time_advance.f90:330-380): FP64 max and RMS of the last
+ * residual over all interior cells; arrays of 7 (entries >= NVAR are 0).  Returns
+ * OCFD_ERR_NAN if any residual is NaN (the reference stops there). */
+int ocfd_residual(ocfd_handle* h, double* res_max, double* res_rms);
+
+/* comput_force (sub_Post.f90:4-265): ft[9] = pressure force (3), viscous force (3), moments
+ * (3), normalised by 2/Ref_S and 2/(Ref_S Ref_L); cl, cd, cs projected by AoA / Cood_Y_UP. */
+int ocfd_forces(ocfd_handle* h, double* ft, double* cl, double* cd, double* cs);
+
+/* Number of bound-violation cells the limiter repaired on the last update of block blk and
+ * the block's sticky IF_OverLimit flag (sub_limitflow.f90:82-171). */
+int ocfd_limiter_status(ocfd_handle* h, int blk, int* n_limited, int* overlimit);
+
+/* Debug / parity access to one per-block array, copied to host in the reference's index
+ * ranges.  name: "Res" (NVAR,-1:n+1 interior used), "dt", "DU", "mu", "mu_t", "vol",
+ * "dtime_mesh", "dw", "Si","Sj","Sk", "ni1".."nk3", "ix1".."kz0", "xc","yc","zc", "surf1".."surf6".
+ * Layouts are given by ocfd_array_shape. */
+int ocfd_array_shape(const ocfd_handle* h, int blk, const char* name, int* lo, int* hi, int* nv);
+int ocfd_get_array(ocfd_handle* h, int blk, const char* name, double* out);
+
+/* Library build/ABI information: "ocfd-b200 <abi> sm_100a ..." */
+const char* ocfd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OCFD_EC_GPU_H */

@@ -1,0 +1,741 @@
+// C-ABI of libocfd_b200.so (include/ocfd_ec_gpu.h): host orchestration of the device hot path.
+//
+// A handle holds all blocks of one case resident on the current device: one arena (arena.h),
+// the block / subface tables, the setup geometry and the captured CUDA graph of one
+// NS_Time_advance step.  All compute happens in the kernels of solver.cuh / setup.cu; the host
+// code below only builds tables, fills the node-coordinate ghost layer (a copy / linear
+// extrapolation, sub_update_buffer_mpi.f90:230-512) and moves data.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/ocfd_ec_gpu.h"
+#include "arena.h"
+#include "runner.h"
+#include "setup.h"
+
+using namespace ocfd;
+
+namespace {
+
+struct DevMem {
+  std::vector<void*> ptrs;
+  size_t bytes = 0;
+  template <class T>
+  T* alloc(size_t n, cudaError_t& err) {
+    if (err != cudaSuccess) return nullptr;
+    if (n == 0) n = 1;
+    void* p = nullptr;
+    err = cudaMalloc(&p, n * sizeof(T));
+    if (err != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, n * sizeof(T));
+    ptrs.push_back(p);
+    bytes += n * sizeof(T);
+    return (T*)p;
+  }
+  void release() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+constexpr int LAPH = 4;
+
+}  // namespace
+
+struct ocfd_handle {
+  ocfd_params P;
+  int nvar = 5, prec = 0, nblk = 0, nsolve = 1;
+  std::vector<BlkD> blk;
+  std::vector<SubD> sub;
+  std::vector<long long> pre_box, pre_cell, pre_face, pre_col, pre_subcell, pre_halo;
+  std::vector<int4> cchunk, wchunk;
+  SolveP sp;
+  long long tot_box = 0, tot_cell = 0, tot_face = 0, tot_node = 0, tot_col = 0, tot_subcell = 0, tot_halo = 0;
+  long long ncell = 0;
+  int max_plane = 3;
+  DevMem mem;
+  // device pointers
+  BlkD* d_blk = nullptr;
+  SubD* d_sub = nullptr;
+  SolveP* d_sp = nullptr;
+  long long *d_pre_box = nullptr, *d_pre_cell = nullptr, *d_pre_face = nullptr, *d_pre_col = nullptr, *d_pre_subcell = nullptr, *d_pre_halo = nullptr;
+  int4 *d_cchunk = nullptr, *d_wchunk = nullptr;
+  double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr, *d_Md = nullptr, *d_vold = nullptr, *d_dtmd = nullptr, *d_dwd = nullptr;
+  double *d_xc = nullptr, *d_yc = nullptr, *d_zc = nullptr;
+  float *d_Mf = nullptr, *d_volf = nullptr, *d_dtmf = nullptr, *d_dwf = nullptr;
+  unsigned char *d_bci = nullptr, *d_bcj = nullptr, *d_bck = nullptr;
+  double *d_U = nullptr, *d_Un = nullptr, *d_DU = nullptr;
+  void *d_P = nullptr, *d_mu = nullptr, *d_mut = nullptr, *d_Kt = nullptr, *d_Wt = nullptr, *d_f1 = nullptr;
+  void *d_Res = nullptr, *d_dt = nullptr, *d_Lc = nullptr, *d_Lv = nullptr, *d_Fi = nullptr, *d_Fv = nullptr, *d_Ft = nullptr;
+  int* d_flags = nullptr;
+  double *d_norm_part = nullptr, *d_norm_out = nullptr, *d_force_part = nullptr, *d_stage = nullptr;
+  unsigned long long* d_nan = nullptr;
+  long long max_box_b = 0;
+  Arena<double> A64;
+  Arena<float> A32;
+  std::unique_ptr<Runner> run;
+  cudaStream_t st = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int kstep = 0;
+  double tt = 0.0;
+  std::string err;
+};
+
+static int fail(ocfd_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+static int cuda_fail(ocfd_handle* h, cudaError_t e, const char* where) {
+  return fail(h, e == cudaErrorMemoryAllocation ? OCFD_ERR_OOM : OCFD_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+extern "C" const char* ocfd_version(void) { return "ocfd-b200 abi 1 sm_100a (FP64 + mixed FP32/FP64)"; }
+
+extern "C" int ocfd_default_params(ocfd_params* p) {  // set_default_parameter, sub_read_parameter.f90:30-106
+  if (!p) return OCFD_ERR_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->ma = 1.0; p->re = 1000.0; p->gamma = 1.4; p->aoa = 0.0; p->aos = 0.0; p->p_outlet = -1.0;
+  p->iflag_turbulence_model = 0; p->if_viscous = 1; p->iflag_local_dt = 1; p->dt_global = 0.01; p->cfl = 1.0;
+  p->dtmax = 10.0; p->dtmin = 1.e-9; p->time_method = 0; p->w_lu = 1.0; p->if_dtime_mesh = 1;
+  p->iflag_scheme = 5; p->iflag_flux = 5; p->iflag_reconstruction = 0; p->t_inf = 288.15; p->twall = -1.0;
+  p->kt_inf = 1.e-5; p->wt_inf = 0.01; p->mut_max = -1.0; p->bound_scheme = 4; p->ref_s = 1.0; p->ref_l = 1.0;
+  p->cood_y_up = 1; p->iflag_limit_flow = 1; p->prl = 0.7; p->prt = 0.9;
+  p->ldmin = 1.e-6; p->ldmax = 1000.0; p->lpmin = 1.e-6; p->lpmax = 1000.0; p->lumax = 1000.0; p->lsamax = 1000.0;
+  p->if_scheme_positivity = 1; p->precision = OCFD_PREC_FP64;
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_finalize_params(ocfd_params* p) {  // set_const_para, sub_read_parameter.f90:371-429
+  if (!p) return OCFD_ERR_ARG;
+  const double PI = 3.1415926535897932;
+  p->twall = p->twall / p->t_inf;
+  p->lpmin = p->lpmin / (p->gamma * p->ma * p->ma);
+  p->lpmax = p->lpmax / (p->gamma * p->ma * p->ma);
+  if (p->bound_scheme == -1) p->bound_scheme = p->iflag_scheme;
+  if (p->if_viscous == 0) p->iflag_turbulence_model = 0;
+  if (p->iflag_turbulence_model == 2 || p->iflag_turbulence_model == 21) p->nvar = 6;
+  else if (p->iflag_turbulence_model == 3) p->nvar = 7;
+  else p->nvar = 5;
+  p->aoa = p->aoa * PI / 180.0;
+  p->aos = p->aos * PI / 180.0;
+  if (p->cood_y_up == 1) { p->a_alfa = p->aoa; p->a_beta = p->aos; }
+  else { p->a_alfa = p->aos; p->a_beta = p->aoa; }
+  p->cv = 1.0 / (p->gamma * (p->gamma - 1.0) * p->ma * p->ma);
+  p->cp = p->cv * p->gamma;
+  return OCFD_OK;
+}
+
+static void fill_solve(const ocfd_params& p, int nvar, SolveP& s) {
+  s.nvar = nvar; s.scheme = p.iflag_scheme; s.bound_scheme = p.bound_scheme; s.flux = p.iflag_flux; s.recon = p.iflag_reconstruction;
+  s.turb = p.if_viscous ? p.iflag_turbulence_model : 0; s.viscous = p.if_viscous; s.local_dt = p.iflag_local_dt; s.dtime_mesh = p.if_dtime_mesh;
+  s.limit_flow = p.iflag_limit_flow; s.positivity = p.if_scheme_positivity; s.time_method = p.time_method;
+  s.gamma = p.gamma; s.ma = p.ma; s.re = p.re; s.cv = p.cv; s.cp = p.cp; s.prl = p.prl; s.prt = p.prt; s.tsb = 110.4 / p.t_inf;
+  s.twall = p.twall; s.kt_inf = p.kt_inf; s.wt_inf = p.wt_inf; s.a_alfa = p.a_alfa; s.a_beta = p.a_beta; s.cfl = p.cfl;
+  s.dt_global = p.dt_global; s.dtmin = p.dtmin; s.dtmax = p.dtmax; s.w_lu = p.w_lu; s.mut_max = p.mut_max; s.p_outlet = p.p_outlet;
+  s.ldmin = p.ldmin; s.ldmax = p.ldmax; s.lpmin = p.lpmin; s.lpmax = p.lpmax; s.lumax = p.lumax; s.lsamax = p.lsamax;
+  s.p00 = 1.0 / (p.gamma * p.ma * p.ma);
+  s.d_inf = 1.0;
+  s.u_inf = std::cos(p.a_alfa) * std::cos(p.a_beta);
+  s.v_inf = std::sin(p.a_alfa) * std::cos(p.a_beta);
+  s.w_inf = std::sin(p.a_beta);
+  s.p_inf = 1.0 / (p.gamma * p.ma * p.ma);
+  s.cen[0] = p.centroid[0]; s.cen[1] = p.centroid[1]; s.cen[2] = p.centroid[2];
+}
+
+// node coordinates with one ghost layer: interface copy (Coordinate_send_mpi, 250-352), linear
+// extrapolation on physical faces and edge / vertex averaging (coordinate_boundary_and_corner,
+// get_xyz_conner, 413-512)
+static void coordinate_ghosts(const std::vector<BlkD>& blk, const std::vector<SubD>& sub, std::vector<std::vector<double>>& X) {
+  auto at = [&](int b, int c, int i, int j, int k) -> double& {
+    const BlkD& B = blk[b];
+    return X[b][(size_t)c * B.NXn * B.NYn * B.NZn + (size_t)i + (size_t)B.NXn * ((size_t)j + (size_t)B.NYn * k)];
+  };
+  for (const SubD& S : sub) {
+    if (S.bc >= 0) continue;
+    int kb[3] = {S.ib, S.jb, S.kb}, ke[3] = {S.ie, S.je, S.ke};
+    int d = (S.face - 1) % 3;
+    if (S.face <= 3) kb[d] += 1; else kb[d] -= 1;
+    ke[d] = kb[d];
+    int kb1[3] = {S.ib1, S.jb1, S.kb1}, ke1[3] = {S.ie1, S.je1, S.ke1};
+    int d1 = (S.face1 - 1) % 3;
+    if (S.face1 <= 3) kb1[d1] -= 1; else kb1[d1] += 1;
+    ke1[d1] = kb1[d1];
+    int L[3] = {std::abs(S.L1), std::abs(S.L2), std::abs(S.L3)};
+    int Pq[3] = {S.L1 >= 0 ? 1 : -1, S.L2 >= 0 ? 1 : -1, S.L3 >= 0 ? 1 : -1};
+    int ks[3];
+    for (int q = 0; q < 3; q++) ks[q] = Pq[q] > 0 ? kb[q] : ke[q];
+    for (int kk = kb1[2]; kk <= ke1[2]; kk++)
+      for (int jj = kb1[1]; jj <= ke1[1]; jj++)
+        for (int ii = kb1[0]; ii <= ke1[0]; ii++) {
+          int ka[3] = {ii - kb1[0], jj - kb1[1], kk - kb1[2]};
+          int i1 = ks[0] + ka[L[0] - 1] * Pq[0], j1 = ks[1] + ka[L[1] - 1] * Pq[1], k1 = ks[2] + ka[L[2] - 1] * Pq[2];
+          for (int c = 0; c < 3; c++) at(S.nb1, c, ii, jj, kk) = at(S.blk, c, i1, j1, k1);
+        }
+  }
+  for (const SubD& S : sub) {
+    if (S.bc < 0) continue;
+    int b = S.blk, i1 = S.ib, i2 = S.ie, j1 = S.jb, j2 = S.je, k1 = S.kb, k2 = S.ke;
+    for (int c = 0; c < 3; c++) {
+      if (S.face == 1) { for (int k = k1; k <= k2; k++) for (int j = j1; j <= j2; j++) at(b, c, i1 - 1, j, k) = 2.0 * at(b, c, i1, j, k) - at(b, c, i1 + 1, j, k); }
+      else if (S.face == 2) { for (int k = k1; k <= k2; k++) for (int i = i1; i <= i2; i++) at(b, c, i, j1 - 1, k) = 2.0 * at(b, c, i, j1, k) - at(b, c, i, j1 + 1, k); }
+      else if (S.face == 3) { for (int j = j1; j <= j2; j++) for (int i = i1; i <= i2; i++) at(b, c, i, j, k1 - 1) = 2.0 * at(b, c, i, j, k1) - at(b, c, i, j, k1 + 1); }
+      else if (S.face == 4) { for (int k = k1; k <= k2; k++) for (int j = j1; j <= j2; j++) at(b, c, i2 + 1, j, k) = 2.0 * at(b, c, i2, j, k) - at(b, c, i2 - 1, j, k); }
+      else if (S.face == 5) { for (int k = k1; k <= k2; k++) for (int i = i1; i <= i2; i++) at(b, c, i, j2 + 1, k) = 2.0 * at(b, c, i, j2, k) - at(b, c, i, j2 - 1, k); }
+      else { for (int j = j1; j <= j2; j++) for (int i = i1; i <= i2; i++) at(b, c, i, j, k2 + 1) = 2.0 * at(b, c, i, j, k2) - at(b, c, i, j, k2 - 1); }
+    }
+  }
+  for (size_t b = 0; b < blk.size(); b++) {
+    int nx = blk[b].nx, ny = blk[b].ny, nz = blk[b].nz;
+    for (int c = 0; c < 3; c++) {
+      auto x = [&](int i, int j, int k) -> double& { return at((int)b, c, i, j, k); };
+      for (int k = 1; k <= nz; k++) {
+        x(0, 0, k) = (x(1, 0, k) + x(0, 1, k)) * 0.5;
+        x(nx + 1, 0, k) = (x(nx, 0, k) + x(nx + 1, 1, k)) * 0.5;
+        x(0, ny + 1, k) = (x(1, ny + 1, k) + x(0, ny, k)) * 0.5;
+        x(nx + 1, ny + 1, k) = (x(nx, ny + 1, k) + x(nx + 1, ny, k)) * 0.5;
+      }
+      for (int j = 1; j <= ny; j++) {
+        x(0, j, 0) = (x(1, j, 0) + x(0, j, 1)) * 0.5;
+        x(nx + 1, j, 0) = (x(nx, j, 0) + x(nx + 1, j, 1)) * 0.5;
+        x(0, j, nz + 1) = (x(1, j, nz + 1) + x(0, j, nz)) * 0.5;
+        x(nx + 1, j, nz + 1) = (x(nx, j, nz + 1) + x(nx + 1, j, nz)) * 0.5;
+      }
+      for (int i = 1; i <= nx; i++) {
+        x(i, 0, 0) = (x(i, 1, 0) + x(i, 0, 1)) * 0.5;
+        x(i, ny + 1, 0) = (x(i, ny, 0) + x(i, ny + 1, 1)) * 0.5;
+        x(i, 0, nz + 1) = (x(i, 1, nz + 1) + x(i, 0, nz)) * 0.5;
+        x(i, ny + 1, nz + 1) = (x(i, ny, nz + 1) + x(i, ny + 1, nz)) * 0.5;
+      }
+      for (int v = 0; v < 8; v++) {
+        int ia = (v & 1) ? nx + 1 : 0, ib = (v & 1) ? nx : 1;
+        int ja = (v & 2) ? ny + 1 : 0, jb = (v & 2) ? ny : 1;
+        int ka = (v & 4) ? nz + 1 : 0, kb = (v & 4) ? nz : 1;
+        x(ia, ja, ka) = (2.0 * (x(ib, ja, ka) + x(ia, jb, ka) + x(ia, ja, kb)) - (x(ib, jb, ka) + x(ib, ja, kb) + x(ia, jb, kb))) / 3.0;
+      }
+    }
+  }
+}
+
+static long long subcell_count(const SubD& S) {
+  if (S.face == 1 || S.face == 4) return (long long)(S.je - S.jb) * (S.ke - S.kb);
+  if (S.face == 2 || S.face == 5) return (long long)(S.ie - S.ib) * (S.ke - S.kb);
+  return (long long)(S.ie - S.ib) * (S.je - S.jb);
+}
+
+template <class T>
+static void fill_arena(ocfd_handle* h, Arena<T>& A, const T* M, const T* vol, const T* dtm, const T* dw) {
+  A.blk = h->d_blk; A.nblk = h->nblk;
+  A.pre_box = h->d_pre_box; A.pre_cell = h->d_pre_cell; A.pre_face = h->d_pre_face; A.pre_col = h->d_pre_col;
+  A.sub = h->d_sub; A.nsub = (int)h->sub.size();
+  A.pre_subcell = h->d_pre_subcell; A.pre_halo = h->d_pre_halo;
+  A.cchunk = h->d_cchunk; A.ncchunk = (int)h->cchunk.size();
+  A.wchunk = h->d_wchunk; A.nwchunk = (int)h->wchunk.size();
+  A.sp = h->d_sp; A.nsolve = h->nsolve;
+  A.tot_box = h->tot_box; A.tot_cell = h->tot_cell; A.tot_face = h->tot_face; A.tot_node = h->tot_node; A.tot_col = h->tot_col;
+  A.tot_subcell = h->tot_subcell; A.tot_halo = h->tot_halo;
+  A.x = h->d_x; A.y = h->d_y; A.z = h->d_z; A.Md = h->d_Md; A.M = M;
+  A.vold = h->d_vold; A.dwd = h->d_dwd; A.vol = vol; A.dtm = dtm; A.dw = dw;
+  A.xc = h->d_xc; A.yc = h->d_yc; A.zc = h->d_zc;
+  A.bci = h->d_bci; A.bcj = h->d_bcj; A.bck = h->d_bck;
+  A.U = h->d_U; A.Un = h->d_Un; A.P = (T*)h->d_P; A.mu = (T*)h->d_mu; A.mut = (T*)h->d_mut; A.Kt = (T*)h->d_Kt; A.Wt = (T*)h->d_Wt;
+  A.f1 = (T*)h->d_f1; A.Res = (T*)h->d_Res; A.DU = h->d_DU; A.dt = (T*)h->d_dt; A.Lc = (T*)h->d_Lc; A.Lv = (T*)h->d_Lv;
+  A.Fi = (T*)h->d_Fi; A.Fv = (T*)h->d_Fv; A.Ft = (T*)h->d_Ft; A.flags = h->d_flags;
+}
+
+template <class T>
+static cudaError_t up(T* d, const std::vector<T>& v) {
+  if (v.empty()) return cudaSuccess;
+  return cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, const double* const* xyz, const int* nsub, const int* inc,
+                           const double* const* dw, ocfd_handle** out) {
+  if (!p || nblk <= 0 || !nijk || !xyz || !nsub || !inc || !out) return OCFD_ERR_ARG;
+  std::unique_ptr<ocfd_handle> hp(new ocfd_handle());
+  ocfd_handle* h = hp.get();
+  h->P = *p;
+  int tm = p->if_viscous ? p->iflag_turbulence_model : 0;
+  h->nvar = (tm == 2) ? 6 : (tm == 3 ? 7 : 5);
+  if (tm != 0 && tm != 2 && tm != 3) return OCFD_ERR_UNSUPPORTED;
+  if (p->time_method != 0 && p->time_method != 3) return OCFD_ERR_UNSUPPORTED;
+  if (p->iflag_flux < 1 || p->iflag_flux > 6) return OCFD_ERR_ARG;
+  h->prec = p->precision;
+  h->nblk = nblk;
+  fill_solve(*p, h->nvar, h->sp);
+  // ---- tables
+  h->blk.resize(nblk);
+  h->pre_box.assign(nblk + 1, 0); h->pre_cell.assign(nblk + 1, 0); h->pre_face.assign(nblk + 1, 0); h->pre_col.assign(nblk + 1, 0);
+  long long onode = 0, obci = 0, obcj = 0, obck = 0;
+  const int* q = inc;
+  for (int b = 0; b < nblk; b++) {
+    BlkD& B = h->blk[b];
+    B.nx = nijk[3 * b]; B.ny = nijk[3 * b + 1]; B.nz = nijk[3 * b + 2];
+    if (B.nx < 2 || B.ny < 2 || B.nz < 2) return OCFD_ERR_ARG;
+    B.NX = B.nx + 7; B.NY = B.ny + 7; B.NZ = B.nz + 7;
+    B.NXn = B.nx + 2; B.NYn = B.ny + 2; B.NZn = B.nz + 2;
+    B.solve = 0;
+    B.obox = h->pre_box[b]; B.oface = h->pre_face[b]; B.ocell = h->pre_cell[b]; B.ocol = h->pre_col[b]; B.onode = onode;
+    B.obci = obci; B.obcj = obcj; B.obck = obck;
+    long long box = (long long)B.NX * B.NY * B.NZ;
+    h->max_box_b = std::max(h->max_box_b, box);
+    h->pre_box[b + 1] = h->pre_box[b] + box;
+    h->pre_face[b + 1] = h->pre_face[b] + (long long)B.nx * B.ny * B.nz;
+    h->pre_cell[b + 1] = h->pre_cell[b] + (long long)(B.nx - 1) * (B.ny - 1) * (B.nz - 1);
+    h->pre_col[b + 1] = h->pre_col[b] + (long long)(B.ny - 1) * (B.nz - 1);
+    onode += (long long)B.NXn * B.NYn * B.NZn;
+    obci += (long long)(B.ny - 1) * (B.nz - 1);
+    obcj += (long long)(B.nx - 1) * (B.nz - 1);
+    obck += (long long)(B.nx - 1) * (B.ny - 1);
+    h->max_plane = std::max(h->max_plane, B.nx + B.ny + B.nz - 3);
+    B.sub0 = (int)h->sub.size(); B.nsub = nsub[b];
+    for (int s = 0; s < nsub[b]; s++, q += 21) {
+      SubD S;
+      S.blk = b;
+      S.ib = q[0]; S.ie = q[1]; S.jb = q[2]; S.je = q[3]; S.kb = q[4]; S.ke = q[5]; S.bc = q[6]; S.face = q[7]; S.f_no = q[8];
+      S.ib1 = q[9]; S.ie1 = q[10]; S.jb1 = q[11]; S.je1 = q[12]; S.kb1 = q[13]; S.ke1 = q[14]; S.nb1 = q[15] - 1; S.face1 = q[16];
+      S.f_no1 = q[17]; S.L1 = q[18]; S.L2 = q[19]; S.L3 = q[20];
+      if (S.face < 1 || S.face > 6) return fail(nullptr, OCFD_ERR_ARG, "bad face");
+      if (S.bc < 0 && (S.nb1 < 0 || S.nb1 >= nblk)) return OCFD_ERR_ARG;
+      if (S.bc > 0 && !(S.bc == 2 || S.bc == 3 || S.bc == 4 || S.bc == 5 || S.bc == 6 || S.bc == 401)) return OCFD_ERR_UNSUPPORTED;
+      h->sub.push_back(S);
+    }
+  }
+  h->tot_box = h->pre_box[nblk]; h->tot_face = h->pre_face[nblk]; h->tot_cell = h->pre_cell[nblk]; h->tot_col = h->pre_col[nblk];
+  h->tot_node = onode;
+  h->ncell = h->tot_cell;
+  int ns = (int)h->sub.size();
+  h->pre_subcell.assign(ns + 1, 0); h->pre_halo.assign(ns + 1, 0);
+  for (int s = 0; s < ns; s++) {
+    const SubD& S = h->sub[s];
+    h->pre_subcell[s + 1] = h->pre_subcell[s] + subcell_count(S);
+    long long nh = 0;
+    if (S.bc < 0) {
+      int kb1[3] = {S.ib1, S.jb1, S.kb1}, ke1[3] = {S.ie1 - 1, S.je1 - 1, S.ke1 - 1};
+      int d1 = (S.face1 - 1) % 3;
+      if (S.face1 <= 3) kb1[d1] -= LAPH;
+      ke1[d1] = kb1[d1] + LAPH - 1;
+      nh = (long long)(ke1[0] - kb1[0] + 1) * (ke1[1] - kb1[1] + 1) * (ke1[2] - kb1[2] + 1);
+    }
+    h->pre_halo[s + 1] = h->pre_halo[s] + nh;
+  }
+  h->tot_subcell = h->pre_subcell[ns]; h->tot_halo = h->pre_halo[ns];
+  for (int b = 0; b < nblk; b++) {
+    long long n = h->pre_cell[b + 1] - h->pre_cell[b];
+    for (long long s0 = 0; s0 < n; s0 += 8192) h->cchunk.push_back(make_int4(b, (int)s0, (int)std::min<long long>(8192, n - s0), 0));
+  }
+  for (int s = 0; s < ns; s++) {
+    if (h->sub[s].bc != 2) continue;
+    long long n = subcell_count(h->sub[s]);
+    for (long long s0 = 0; s0 < n; s0 += 4096) h->wchunk.push_back(make_int4(s, (int)s0, (int)std::min<long long>(4096, n - s0), 0));
+  }
+  // physical-face flags (set_BcK, sub_init.f90:545-577)
+  std::vector<unsigned char> bci(obci, 0), bcj(obcj, 0), bck(obck, 0);
+  for (const SubD& S : h->sub) {
+    if (S.bc < 0) continue;
+    const BlkD& B = h->blk[S.blk];
+    unsigned char bit = S.face <= 3 ? 1 : 2;
+    if (S.face == 1 || S.face == 4) for (int k = S.kb; k <= S.ke - 1; k++) for (int j = S.jb; j <= S.je - 1; j++) bci[B.obci + (j - 1) + (long long)(B.ny - 1) * (k - 1)] |= bit;
+    if (S.face == 2 || S.face == 5) for (int k = S.kb; k <= S.ke - 1; k++) for (int i = S.ib; i <= S.ie - 1; i++) bcj[B.obcj + (i - 1) + (long long)(B.nx - 1) * (k - 1)] |= bit;
+    if (S.face == 3 || S.face == 6) for (int j = S.jb; j <= S.je - 1; j++) for (int i = S.ib; i <= S.ie - 1; i++) bck[B.obck + (i - 1) + (long long)(B.nx - 1) * (j - 1)] |= bit;
+  }
+  // node coordinates + ghost layer
+  std::vector<std::vector<double>> X(nblk);
+  for (int b = 0; b < nblk; b++) {
+    const BlkD& B = h->blk[b];
+    size_t nn = (size_t)B.NXn * B.NYn * B.NZn;
+    X[b].assign(3 * nn, 0.0);
+    size_t np = (size_t)B.nx * B.ny * B.nz;
+    for (int c = 0; c < 3; c++)
+      for (int k = 1; k <= B.nz; k++)
+        for (int j = 1; j <= B.ny; j++)
+          for (int i = 1; i <= B.nx; i++)
+            X[b][c * nn + i + (size_t)B.NXn * (j + (size_t)B.NYn * k)] = xyz[b][c * np + (i - 1) + (size_t)B.nx * ((j - 1) + (size_t)B.ny * (k - 1))];
+  }
+  coordinate_ghosts(h->blk, h->sub, X);
+  std::vector<double> hx(onode), hy(onode), hz(onode);
+  for (int b = 0; b < nblk; b++) {
+    const BlkD& B = h->blk[b];
+    size_t nn = (size_t)B.NXn * B.NYn * B.NZn;
+    std::memcpy(&hx[B.onode], &X[b][0], nn * 8);
+    std::memcpy(&hy[B.onode], &X[b][nn], nn * 8);
+    std::memcpy(&hz[B.onode], &X[b][2 * nn], nn * 8);
+  }
+  std::vector<double> Xw;
+  int turb = h->sp.turb;
+  bool need_dw = turb != 0 && !(dw && dw[0]);
+  if (need_dw) {
+    for (const SubD& S : h->sub) {
+      if (S.bc != 2) continue;
+      const BlkD& B = h->blk[S.blk];
+      for (int k = S.kb; k <= S.ke; k++)
+        for (int j = S.jb; j <= S.je; j++)
+          for (int i = S.ib; i <= S.ie; i++) {
+            size_t o = (size_t)i + (size_t)B.NXn * ((size_t)j + (size_t)B.NYn * k);
+            size_t nn = (size_t)B.NXn * B.NYn * B.NZn;
+            Xw.push_back(X[S.blk][o]); Xw.push_back(X[S.blk][nn + o]); Xw.push_back(X[S.blk][2 * nn + o]);
+          }
+    }
+  }
+  X.clear();
+  // ---- device memory
+  cudaError_t e = cudaSuccess;
+  DevMem& M = h->mem;
+  const long long tb = h->tot_box, tf = h->tot_face, tc = h->tot_cell;
+  const int NV = h->nvar;
+  const size_t ts = h->prec == OCFD_PREC_MIXED ? sizeof(float) : sizeof(double);
+  h->d_blk = M.alloc<BlkD>(nblk, e);
+  h->d_sub = M.alloc<SubD>(std::max(1, ns), e);
+  h->d_sp = M.alloc<SolveP>(1, e);
+  h->d_pre_box = M.alloc<long long>(nblk + 1, e); h->d_pre_cell = M.alloc<long long>(nblk + 1, e);
+  h->d_pre_face = M.alloc<long long>(nblk + 1, e); h->d_pre_col = M.alloc<long long>(nblk + 1, e);
+  h->d_pre_subcell = M.alloc<long long>(ns + 1, e); h->d_pre_halo = M.alloc<long long>(ns + 1, e);
+  h->d_cchunk = M.alloc<int4>(h->cchunk.size(), e); h->d_wchunk = M.alloc<int4>(std::max<size_t>(1, h->wchunk.size()), e);
+  h->d_x = M.alloc<double>(onode, e); h->d_y = M.alloc<double>(onode, e); h->d_z = M.alloc<double>(onode, e);
+  h->d_Md = M.alloc<double>((size_t)M_COUNT * tf, e);
+  h->d_vold = M.alloc<double>(tc, e); h->d_dtmd = M.alloc<double>(tc, e); h->d_dwd = M.alloc<double>(tc, e);
+  h->d_xc = M.alloc<double>(tb, e); h->d_yc = M.alloc<double>(tb, e); h->d_zc = M.alloc<double>(tb, e);
+  h->d_bci = M.alloc<unsigned char>(obci, e); h->d_bcj = M.alloc<unsigned char>(obcj, e); h->d_bck = M.alloc<unsigned char>(obck, e);
+  h->d_U = M.alloc<double>((size_t)NV * tb, e);
+  if (p->time_method == 3) h->d_Un = M.alloc<double>((size_t)NV * tb, e);
+  h->d_DU = M.alloc<double>((size_t)std::max(NV, 5) * tc, e);
+  h->d_P = M.alloc<char>(ts * P_COUNT * tb, e);
+  h->d_mu = M.alloc<char>(ts * tb, e);
+  h->d_mut = M.alloc<char>(ts * tb, e);
+  if (turb == 3) { h->d_Kt = M.alloc<char>(ts * tb, e); h->d_Wt = M.alloc<char>(ts * tb, e); h->d_f1 = M.alloc<char>(ts * tf, e); }
+  h->d_Res = M.alloc<char>(ts * NV * tc, e);
+  h->d_dt = M.alloc<char>(ts * tc, e);
+  h->d_Lc = M.alloc<char>(ts * 3 * tc, e);
+  h->d_Lv = M.alloc<char>(ts * 3 * tc, e);
+  h->d_Fi = M.alloc<char>(std::max(ts * 15 * tf, sizeof(double) * 3 * tf), e);
+  if (p->if_viscous) h->d_Fv = M.alloc<char>(ts * 12 * tf, e);
+  if (turb != 0) h->d_Ft = M.alloc<char>(ts * 6 * tf, e);
+  h->d_flags = M.alloc<int>(4 * nblk, e);
+  h->d_norm_part = M.alloc<double>(14 * h->cchunk.size(), e);
+  h->d_norm_out = M.alloc<double>(14 * h->nsolve, e);
+  h->d_force_part = M.alloc<double>(9 * std::max<size_t>(1, h->wchunk.size()), e);
+  h->d_nan = M.alloc<unsigned long long>(1, e);
+  h->d_stage = M.alloc<double>((size_t)NV * h->max_box_b, e);
+  if (h->prec == OCFD_PREC_MIXED) {
+    h->d_Mf = M.alloc<float>((size_t)M_COUNT * tf, e);
+    h->d_volf = M.alloc<float>(tc, e); h->d_dtmf = M.alloc<float>(tc, e); h->d_dwf = M.alloc<float>(tc, e);
+  }
+  double* d_Xw = nullptr;
+  if (need_dw && !Xw.empty()) d_Xw = M.alloc<double>(Xw.size(), e);
+  if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "allocation"); }
+  // ---- uploads
+  if ((e = up(h->d_blk, h->blk)) || (e = up(h->d_sub, h->sub)) || (e = cudaMemcpy(h->d_sp, &h->sp, sizeof(SolveP), cudaMemcpyHostToDevice)) ||
+      (e = up(h->d_pre_box, h->pre_box)) || (e = up(h->d_pre_cell, h->pre_cell)) || (e = up(h->d_pre_face, h->pre_face)) ||
+      (e = up(h->d_pre_col, h->pre_col)) || (e = up(h->d_pre_subcell, h->pre_subcell)) || (e = up(h->d_pre_halo, h->pre_halo)) ||
+      (e = up(h->d_cchunk, h->cchunk)) || (e = up(h->d_wchunk, h->wchunk)) || (e = up(h->d_x, hx)) || (e = up(h->d_y, hy)) ||
+      (e = up(h->d_z, hz)) || (e = up(h->d_bci, bci)) || (e = up(h->d_bcj, bcj)) || (e = up(h->d_bck, bck))) {
+    M.release();
+    return cuda_fail(nullptr, e, "upload");
+  }
+  if (d_Xw) cudaMemcpy(d_Xw, Xw.data(), Xw.size() * 8, cudaMemcpyHostToDevice);
+  if (dw && dw[0] && turb != 0) {
+    std::vector<double> hdw(tc);
+    for (int b = 0; b < nblk; b++) std::memcpy(&hdw[h->pre_cell[b]], dw[b], (h->pre_cell[b + 1] - h->pre_cell[b]) * 8);
+    cudaMemcpy(h->d_dwd, hdw.data(), tc * 8, cudaMemcpyHostToDevice);
+  }
+  // mu = 1/Re everywhere (allocate_mem_Blocks, sub_init.f90:507)
+  {
+    size_t n = (size_t)tb;
+    if (h->prec == OCFD_PREC_MIXED) { std::vector<float> v(n, (float)(1.0 / p->re)); cudaMemcpy(h->d_mu, v.data(), n * 4, cudaMemcpyHostToDevice); }
+    else { std::vector<double> v(n, 1.0 / p->re); cudaMemcpy(h->d_mu, v.data(), n * 8, cudaMemcpyHostToDevice); }
+  }
+  if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "stream"); }
+  // ---- geometry on the device
+  GeoArgs G;
+  G.blk = h->d_blk; G.nblk = nblk; G.pre_face = h->d_pre_face; G.pre_cell = h->d_pre_cell; G.pre_box = h->d_pre_box;
+  G.tot_face = tf; G.tot_cell = tc; G.tot_box = tb; G.tot_node = onode;
+  G.x = h->d_x; G.y = h->d_y; G.z = h->d_z; G.M = h->d_Md; G.scratch = (double*)h->d_Fi;
+  G.vol = h->d_vold; G.dtm = h->d_dtmd; G.dw = h->d_dwd; G.xc = h->d_xc; G.yc = h->d_yc; G.zc = h->d_zc;
+  G.Xw = d_Xw; G.nwall = need_dw ? (long long)(Xw.size() / 3) : 0;
+  if ((e = run_geometry(G, h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "geometry"); }
+  if (h->prec == OCFD_PREC_MIXED) {
+    convert_to_float(h->d_Md, h->d_Mf, (long long)M_COUNT * tf, h->st);
+    convert_to_float(h->d_vold, h->d_volf, tc, h->st);
+    convert_to_float(h->d_dtmd, h->d_dtmf, tc, h->st);
+    convert_to_float(h->d_dwd, h->d_dwf, tc, h->st);
+  }
+  if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "geometry sync"); }
+  // ---- runner
+  RunInfo I;
+  I.nvar = NV; I.time_method = p->time_method; I.viscous = p->if_viscous; I.turb = turb; I.max_plane = h->max_plane;
+  I.ncchunk = (int)h->cchunk.size(); I.nwchunk = (int)h->wchunk.size();
+  if (h->prec == OCFD_PREC_MIXED) {
+    fill_arena<float>(h, h->A32, h->d_Mf, h->d_volf, h->d_dtmf, h->d_dwf);
+    h->run.reset(make_runner_mixed(h->A32, I));
+  } else {
+    fill_arena<double>(h, h->A64, h->d_Md, h->d_vold, h->d_dtmd, h->d_dwd);
+    h->run.reset(make_runner_fp64(h->A64, I));
+  }
+  if (!h->run) { M.release(); return OCFD_ERR_UNSUPPORTED; }
+  h->run->init_flow(h->st);
+  if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "init"); }
+  int bcerr = 0;
+  {
+    std::vector<int> fl(4 * nblk);
+    cudaMemcpy(fl.data(), h->d_flags, fl.size() * 4, cudaMemcpyDeviceToHost);
+    for (int b = 0; b < nblk; b++) bcerr |= fl[3 * nblk + b];
+  }
+  if (bcerr) { M.release(); return OCFD_ERR_UNSUPPORTED; }
+  *out = hp.release();
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_destroy(ocfd_handle* h) {
+  if (!h) return OCFD_OK;
+  if (h->st) cudaStreamSynchronize(h->st);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->run.reset();
+  h->mem.release();
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+  return OCFD_OK;
+}
+
+extern "C" const char* ocfd_last_error(const ocfd_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+extern "C" long long ocfd_state_size(const ocfd_handle* h, int b) {
+  if (!h || b < 0 || b >= h->nblk) return -1;
+  const BlkD& B = h->blk[b];
+  return (long long)h->nvar * B.NX * B.NY * B.NZ;
+}
+
+extern "C" int ocfd_set_state(ocfd_handle* h, int b, const double* U) {
+  if (!h || !U || b < 0 || b >= h->nblk) return OCFD_ERR_ARG;
+  const BlkD& B = h->blk[b];
+  long long box = (long long)B.NX * B.NY * B.NZ;
+  cudaError_t e = cudaMemcpyAsync(h->d_stage, U, (size_t)h->nvar * box * 8, cudaMemcpyHostToDevice, h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "set_state");
+  h->run->scatter_state(h->st, b, h->d_stage, box);
+  if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) return cuda_fail(h, e, "set_state");
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_get_state(ocfd_handle* h, int b, double* U) {
+  if (!h || !U || b < 0 || b >= h->nblk) return OCFD_ERR_ARG;
+  const BlkD& B = h->blk[b];
+  long long box = (long long)B.NX * B.NY * B.NZ;
+  h->run->gather_state(h->st, b, h->d_stage, box);
+  cudaError_t e = cudaMemcpyAsync(U, h->d_stage, (size_t)h->nvar * box * 8, cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "get_state");
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_init_flow(ocfd_handle* h) {
+  if (!h) return OCFD_ERR_ARG;
+  h->run->init_flow(h->st);
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "init_flow");
+  h->kstep = 0;
+  h->tt = 0.0;
+  return OCFD_OK;
+}
+
+static int ensure_graph(ocfd_handle* h) {
+  if (h->gexec) return OCFD_OK;
+  if (std::getenv("OCFD_NO_GRAPH")) return OCFD_OK;
+  cudaError_t e = cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(h, e, "capture begin");
+  h->run->step(h->st);
+  e = cudaStreamEndCapture(h->st, &h->graph);
+  if (e != cudaSuccess) return cuda_fail(h, e, "capture end");
+  e = cudaGraphInstantiate(&h->gexec, h->graph, 0);
+  if (e != cudaSuccess) return cuda_fail(h, e, "graph instantiate");
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_advance(ocfd_handle* h, int nsteps, int* kstep, double* tt) {
+  if (!h || nsteps < 0) return OCFD_ERR_ARG;
+  int rc = ensure_graph(h);
+  if (rc) return rc;
+  for (int s = 0; s < nsteps; s++) {
+    if (h->gexec) {
+      cudaError_t e = cudaGraphLaunch(h->gexec, h->st);
+      if (e != cudaSuccess) return cuda_fail(h, e, "graph launch");
+    } else {
+      h->run->step(h->st);
+    }
+    h->tt = h->tt + h->P.dt_global;
+    h->kstep = h->kstep + 1;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(h, e, "advance");
+  if (kstep) *kstep = h->kstep;
+  if (tt) *tt = h->tt;
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_compute_residual(ocfd_handle* h, int with_lusgs) {
+  if (!h) return OCFD_ERR_ARG;
+  h->run->residual(h->st, with_lusgs != 0);
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "compute_residual");
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_residual(ocfd_handle* h, double* rmax, double* rrms) {
+  if (!h || !rmax || !rrms) return OCFD_ERR_ARG;
+  unsigned long long init = ~0ULL;
+  cudaMemcpyAsync(h->d_nan, &init, 8, cudaMemcpyHostToDevice, h->st);
+  h->run->norms(h->st, h->d_norm_part, h->d_norm_out, h->d_nan);
+  double out[14];
+  unsigned long long nan_at = 0;
+  cudaMemcpyAsync(out, h->d_norm_out, sizeof(out), cudaMemcpyDeviceToHost, h->st);
+  cudaMemcpyAsync(&nan_at, h->d_nan, 8, cudaMemcpyDeviceToHost, h->st);
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "residual");
+  for (int m = 0; m < 7; m++) {
+    rmax[m] = m < h->nvar ? out[m] : 0.0;
+    rrms[m] = m < h->nvar ? std::sqrt(out[7 + m] / (double)h->ncell) : 0.0;
+  }
+  if (nan_at != ~0ULL) {
+    long long g = (long long)(nan_at / 8);
+    int m = (int)(nan_at % 8);
+    int b = (int)(std::upper_bound(h->pre_cell.begin(), h->pre_cell.end(), g) - h->pre_cell.begin()) - 1;
+    const BlkD& B = h->blk[b];
+    long long l = g - h->pre_cell[b];
+    int i = (int)(l % (B.nx - 1)) + 1, j = (int)((l / (B.nx - 1)) % (B.ny - 1)) + 1, k = (int)(l / ((long long)(B.nx - 1) * (B.ny - 1))) + 1;
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "NaN in residual: block %d i,j,k,m = %d %d %d %d", b + 1, i, j, k, m + 1);
+    return fail(h, OCFD_ERR_NAN, buf);
+  }
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_forces(ocfd_handle* h, double* ft, double* cl, double* cd, double* cs) {
+  if (!h || !ft) return OCFD_ERR_ARG;
+  size_t nw = h->wchunk.size();
+  std::vector<double> part(9 * std::max<size_t>(nw, 1), 0.0);
+  if (nw) {
+    h->run->forces(h->st, h->d_force_part);
+    cudaMemcpyAsync(part.data(), h->d_force_part, nw * 9 * 8, cudaMemcpyDeviceToHost, h->st);
+  }
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "forces");
+  // per block in subface order, then over blocks (sub_Post.f90:31-202)
+  double Ft[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  std::vector<double> blk(9 * h->nblk, 0.0);
+  for (size_t c = 0; c < nw; c++) {
+    int b = h->sub[h->wchunk[c].x].blk;
+    for (int q = 0; q < 9; q++) blk[9 * b + q] = blk[9 * b + q] + part[9 * c + q];
+  }
+  for (int b = 0; b < h->nblk; b++)
+    for (int q = 0; q < 9; q++) Ft[q] = Ft[q] + blk[9 * b + q];
+  const ocfd_params& P = h->P;
+  for (int q = 0; q < 6; q++) ft[q] = 2.0 * Ft[q] / P.ref_s;
+  for (int q = 6; q < 9; q++) ft[q] = 2.0 * Ft[q] / (P.ref_s * P.ref_l);
+  double Fx = ft[0] + ft[3], Fy = ft[1] + ft[4], Fz = ft[2] + ft[5];
+  double L, D, S;
+  if (P.cood_y_up == 1) { L = Fy * std::cos(P.aoa) - Fx * std::sin(P.aoa); D = Fx * std::cos(P.aoa) + Fy * std::sin(P.aoa); S = Fz; }
+  else { L = Fz * std::cos(P.aoa) - Fx * std::sin(P.aoa); D = Fx * std::cos(P.aoa) + Fz * std::sin(P.aoa); S = Fy; }
+  if (cl) *cl = L;
+  if (cd) *cd = D;
+  if (cs) *cs = S;
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_limiter_status(ocfd_handle* h, int b, int* n, int* ov) {
+  if (!h || b < 0 || b >= h->nblk) return OCFD_ERR_ARG;
+  int a = 0, c = 0;
+  cudaMemcpyAsync(&a, h->d_flags + h->nblk + b, 4, cudaMemcpyDeviceToHost, h->st);
+  cudaMemcpyAsync(&c, h->d_flags + b, 4, cudaMemcpyDeviceToHost, h->st);
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "limiter_status");
+  if (n) *n = a;
+  if (ov) *ov = c;
+  return OCFD_OK;
+}
+
+// ---- debug / parity array access --------------------------------------------------------
+namespace {
+struct ArrDesc {
+  int space;  // 0 box, 1 face, 2 cell, 3 node
+  int nv;
+  const void* base;
+  bool is_double;
+  long long plane;  // plane stride
+  int lo[3], hi[3];
+};
+}  // namespace
+
+static bool describe(const ocfd_handle* h, int b, const std::string& s, ArrDesc& d) {
+  const BlkD& B = h->blk[b];
+  bool dbl = h->prec != OCFD_PREC_MIXED;
+  auto set_box = [&](int l, int hoff) { d.space = 0; for (int q = 0; q < 3; q++) d.lo[q] = l; d.hi[0] = B.nx + hoff; d.hi[1] = B.ny + hoff; d.hi[2] = B.nz + hoff; d.plane = h->tot_box; };
+  auto set_face = [&]() { d.space = 1; for (int q = 0; q < 3; q++) d.lo[q] = 1; d.hi[0] = B.nx; d.hi[1] = B.ny; d.hi[2] = B.nz; d.plane = h->tot_face; };
+  auto set_cell = [&]() { d.space = 2; for (int q = 0; q < 3; q++) d.lo[q] = 1; d.hi[0] = B.nx - 1; d.hi[1] = B.ny - 1; d.hi[2] = B.nz - 1; d.plane = h->tot_cell; };
+  d.nv = 1;
+  static const char* mnames[] = {"Si", "Sj", "Sk", "ni1", "ni2", "ni3", "nj1", "nj2", "nj3", "nk1", "nk2", "nk3",
+                                 "ix1", "iy1", "iz1", "jx1", "jy1", "jz1", "kx1", "ky1", "kz1", "ix2", "iy2", "iz2", "jx2", "jy2", "jz2", "kx2", "ky2", "kz2",
+                                 "ix3", "iy3", "iz3", "jx3", "jy3", "jz3", "kx3", "ky3", "kz3", "ix0", "iy0", "iz0", "jx0", "jy0", "jz0", "kx0", "ky0", "kz0"};
+  for (int q = 0; q < 48; q++)
+    if (s == mnames[q]) { set_face(); d.base = h->d_Md + (size_t)q * h->tot_face; d.is_double = true; return true; }
+  if (s == "U") { set_box(-3, 3); d.nv = h->nvar; d.base = h->d_U; d.is_double = true; return true; }
+  if (s == "mu") { set_box(-1, 1); d.base = h->d_mu; d.is_double = dbl; return true; }
+  if (s == "mu_t") { set_box(-1, 1); d.base = h->d_mut; d.is_double = dbl; return true; }
+  if (s == "xc") { set_box(-3, 3); d.base = h->d_xc; d.is_double = true; return true; }
+  if (s == "yc") { set_box(-3, 3); d.base = h->d_yc; d.is_double = true; return true; }
+  if (s == "zc") { set_box(-3, 3); d.base = h->d_zc; d.is_double = true; return true; }
+  if (s == "vol") { set_cell(); d.base = h->d_vold; d.is_double = true; return true; }
+  if (s == "dw") { set_cell(); d.base = h->d_dwd; d.is_double = true; return true; }
+  if (s == "dtime_mesh") { set_cell(); d.base = h->d_dtmd; d.is_double = true; return true; }
+  if (s == "dt") { set_cell(); d.base = h->d_dt; d.is_double = dbl; return true; }
+  if (s == "Res") { set_cell(); d.nv = h->nvar; d.base = h->d_Res; d.is_double = dbl; return true; }
+  if (s == "DU") { set_cell(); d.nv = h->nvar; d.base = h->d_DU; d.is_double = true; return true; }
+  return false;
+}
+
+extern "C" int ocfd_array_shape(const ocfd_handle* h, int b, const char* name, int* lo, int* hi, int* nv) {
+  if (!h || !name || b < 0 || b >= h->nblk) return OCFD_ERR_ARG;
+  ArrDesc d;
+  if (!describe(h, b, name, d)) return OCFD_ERR_ARG;
+  for (int q = 0; q < 3; q++) { lo[q] = d.lo[q]; hi[q] = d.hi[q]; }
+  *nv = d.nv;
+  return OCFD_OK;
+}
+
+// copies the array in the requested Fortran bounds; variable-major planes are interleaved back
+// to the Fortran (m fastest) order
+extern "C" int ocfd_get_array(ocfd_handle* h, int b, const char* name, double* out) {
+  if (!h || !name || !out || b < 0 || b >= h->nblk) return OCFD_ERR_ARG;
+  ArrDesc d;
+  if (!describe(h, b, name, d)) return OCFD_ERR_ARG;
+  const BlkD& B = h->blk[b];
+  long long off, n0, n1, n2;
+  int base_lo;
+  if (d.space == 0) { off = B.obox; n0 = B.NX; n1 = B.NY; n2 = B.NZ; base_lo = -3; }
+  else if (d.space == 1) { off = B.oface; n0 = B.nx; n1 = B.ny; n2 = B.nz; base_lo = 1; }
+  else { off = B.ocell; n0 = B.nx - 1; n1 = B.ny - 1; n2 = B.nz - 1; base_lo = 1; }
+  long long cnt = n0 * n1 * n2;
+  size_t es = d.is_double ? 8 : 4;
+  std::vector<char> tmp(cnt * es * d.nv);
+  for (int m = 0; m < d.nv; m++) {
+    cudaError_t e = cudaMemcpy(&tmp[m * cnt * es], (const char*)d.base + (size_t)(m * d.plane + off) * es, cnt * es, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(h, e, "get_array");
+  }
+  long long w0 = d.hi[0] - d.lo[0] + 1, w1 = d.hi[1] - d.lo[1] + 1;
+  for (int k = d.lo[2]; k <= d.hi[2]; k++)
+    for (int j = d.lo[1]; j <= d.hi[1]; j++)
+      for (int i = d.lo[0]; i <= d.hi[0]; i++) {
+        long long src = (i - base_lo) + n0 * ((j - base_lo) + n1 * (long long)(k - base_lo));
+        long long dst = (i - d.lo[0]) + w0 * ((j - d.lo[1]) + w1 * (long long)(k - d.lo[2]));
+        for (int m = 0; m < d.nv; m++) {
+          double v = d.is_double ? ((double*)tmp.data())[m * cnt + src] : (double)((float*)tmp.data())[m * cnt + src];
+          out[dst * d.nv + m] = v;
+        }
+      }
+  return OCFD_OK;
+}

@@ -1,0 +1,157 @@
+// Kernel sequencing of one time step, templated on the flux precision T and NVAR.
+#pragma once
+#include "runner.h"
+#include "solver.cuh"
+
+namespace ocfd {
+
+static inline int grid_of(long long n, int threads = 256) {
+  long long g = (n + threads - 1) / threads;
+  if (g > 148LL * 16) g = 148LL * 16;
+  return g < 1 ? 1 : (int)g;
+}
+
+template <class T, int NV>
+__global__ void k_scatter_state(Arena<T> A, int b, const double* aos, long long box_b) {
+  const BlkD& B = A.blk[b];
+  OCFD_GRID_STRIDE(l, box_b) {
+#pragma unroll
+    for (int m = 0; m < NV; m++) A.U[m * A.tot_box + B.obox + l] = aos[l * NV + m];
+  }
+}
+template <class T, int NV>
+__global__ void k_gather_state(Arena<T> A, int b, double* aos, long long box_b) {
+  const BlkD& B = A.blk[b];
+  OCFD_GRID_STRIDE(l, box_b) {
+#pragma unroll
+    for (int m = 0; m < NV; m++) aos[l * NV + m] = A.U[m * A.tot_box + B.obox + l];
+  }
+}
+
+template <class T, int NV>
+class RunnerT : public Runner {
+ public:
+  RunnerT(const Arena<T>& A, const RunInfo& I) : A_(A), I_(I) {}
+
+  void residual(cudaStream_t st, bool lusgs) override {
+    const Arena<T>& A = A_;
+    const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
+    k_prim<T><<<grid_of(tb), 256, 0, st>>>(A);
+    if (I_.viscous) {
+      k_mu<T><<<grid_of(tc), 256, 0, st>>>(A);
+      if (I_.turb == 2 && NV == 6) {
+        k_sa_pre<T><<<grid_of(tb), 256, 0, st>>>(A);
+        k_sa_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
+        k_sa_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
+        k_sa_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+        k_sa_res<T><<<grid_of(tc), 256, 0, st>>>(A);
+        k_mu_finish<T, 1><<<grid_of(tb), 256, 0, st>>>(A);
+      } else if (I_.turb == 3 && NV == 7) {
+        k_sst_pre<T><<<grid_of(tb), 256, 0, st>>>(A);
+        k_sst_src<T><<<grid_of(tc), 256, 0, st>>>(A);
+        k_sst_mut_ghost<T, 0><<<grid_of(tb), 256, 0, st>>>(A);
+        k_sst_mut_ghost<T, 1><<<grid_of(tb), 256, 0, st>>>(A);
+        k_sst_mut_ghost<T, 2><<<grid_of(tb), 256, 0, st>>>(A);
+        k_amut<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
+        k_sst_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
+        k_sst_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
+        k_sst_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+        k_sst_res<T><<<grid_of(tc), 256, 0, st>>>(A);
+        k_mu_finish<T, 1><<<grid_of(tb), 256, 0, st>>>(A);
+      } else {
+        cudaMemsetAsync(A.mut, 0, sizeof(T) * tb, st);
+      }
+      k_amut<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
+    }
+    k_inv_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
+    k_inv_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
+    k_inv_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+    k_inv_kbc<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
+    if (I_.viscous) {
+      k_visc_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
+      k_visc_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
+      k_visc_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+    }
+    k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
+    if (lusgs) {
+      int gc = grid_of(A.tot_col, 128);
+      for (int p = 3; p <= I_.max_plane; p++) k_lusgs<T, NV, false><<<gc, 128, 0, st>>>(A, p);
+      for (int p = I_.max_plane; p >= 3; p--) k_lusgs<T, NV, true><<<gc, 128, 0, st>>>(A, p);
+    }
+  }
+
+  void bc_halo(cudaStream_t st) override {
+    const Arena<T>& A = A_;
+    k_bc<T, NV><<<A.nblk, 256, 0, st>>>(A);
+    if (A.tot_halo > 0) k_halo<T, NV><<<grid_of(A.tot_halo), 256, 0, st>>>(A);
+    k_corner<T, NV><<<A.nblk, 256, 0, st>>>(A);
+  }
+
+  void limit(cudaStream_t st) {
+    const Arena<T>& A = A_;
+    k_limit_fix<T><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+    if (NV == 6) {
+      k_sa_limit_check<T><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+      k_sa_limit_par<T><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+      k_sa_limit_serial<T><<<A.nblk, 32, 0, st>>>(A);
+    }
+  }
+
+  void step(cudaStream_t st) override {
+    const Arena<T>& A = A_;
+    if (I_.time_method == 0) {
+      residual(st, true);
+      cudaMemsetAsync(A.flags + A.nblk, 0, sizeof(int) * 2 * A.nblk, st);
+      k_update<T, NV, 0><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+      limit(st);
+      bc_halo(st);
+    } else {
+      k_copy_un<T, NV><<<grid_of((long long)NV * A.tot_box), 256, 0, st>>>(A);
+      for (int krk = 1; krk <= 3; krk++) {
+        residual(st, false);
+        cudaMemsetAsync(A.flags + A.nblk, 0, sizeof(int) * 2 * A.nblk, st);
+        if (krk == 1) k_update<T, NV, 1><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+        else if (krk == 2) k_update<T, NV, 2><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+        else k_update<T, NV, 3><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+        limit(st);
+        bc_halo(st);
+      }
+    }
+    if (NV >= 6) k_vtkw<T, NV><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+  }
+
+  void init_flow(cudaStream_t st) override {
+    k_init_flow<T, NV><<<grid_of(A_.tot_box), 256, 0, st>>>(A_);
+    bc_halo(st);
+  }
+
+  void norms(cudaStream_t st, double* part, double* out, unsigned long long* nan_at) override {
+    k_norms<T, NV><<<A_.ncchunk, 256, 0, st>>>(A_, part, nan_at);
+    k_norms_combine<T><<<(A_.nsolve + 63) / 64, 64, 0, st>>>(A_, part, out);
+  }
+
+  void forces(cudaStream_t st, double* part) override {
+    if (A_.nwchunk > 0) k_forces<T><<<A_.nwchunk, 256, 0, st>>>(A_, part);
+  }
+
+  void scatter_state(cudaStream_t st, int blk, const double* aos, long long box_b) override {
+    k_scatter_state<T, NV><<<grid_of(box_b), 256, 0, st>>>(A_, blk, aos, box_b);
+  }
+  void gather_state(cudaStream_t st, int blk, double* aos, long long box_b) override {
+    k_gather_state<T, NV><<<grid_of(box_b), 256, 0, st>>>(A_, blk, aos, box_b);
+  }
+
+ private:
+  Arena<T> A_;
+  RunInfo I_;
+};
+
+template <class T>
+Runner* make_runner_t(const Arena<T>& A, const RunInfo& I) {
+  if (I.nvar == 5) return new RunnerT<T, 5>(A, I);
+  if (I.nvar == 6) return new RunnerT<T, 6>(A, I);
+  if (I.nvar == 7) return new RunnerT<T, 7>(A, I);
+  return nullptr;
+}
+
+}  // namespace ocfd

@@ -1,0 +1,39 @@
+// Step runner interface: one implementation per (flux precision, NVAR), created by
+// make_runner_fp64 / make_runner_mixed (solver_fp64.cu, solver_mixed.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "arena.h"
+
+namespace ocfd {
+
+struct RunInfo {
+  int nvar, time_method, viscous, turb;
+  int max_plane;          // max over blocks of nx+ny+nz-3 (last LU-SGS hyperplane)
+  int ncchunk, nwchunk;   // reduction chunk counts
+};
+
+class Runner {
+ public:
+  virtual ~Runner() {}
+  // one NS_Time_advance (sub_time_advance.f90:6-23) on stream st
+  virtual void step(cudaStream_t st) = 0;
+  // residual only (Comput_Residual_one_mesh without LU-SGS), for parity checks
+  virtual void residual(cudaStream_t st, bool lusgs) = 0;
+  // freestream + BC + halo + corners (init_flow_zero, sub_init.f90:302-410)
+  virtual void init_flow(cudaStream_t st) = 0;
+  // BC + halo + corners only
+  virtual void bc_halo(cudaStream_t st) = 0;
+  // residual norms: 14 doubles per solve into out (max[7], sum of squares[7])
+  virtual void norms(cudaStream_t st, double* part, double* out, unsigned long long* nan_at) = 0;
+  // force partial sums: 9 doubles per wall chunk
+  virtual void forces(cudaStream_t st, double* part) = 0;
+  // AoS Fortran U(NV, box) of one block <-> device planes
+  virtual void scatter_state(cudaStream_t st, int blk, const double* aos, long long box_b) = 0;
+  virtual void gather_state(cudaStream_t st, int blk, double* aos, long long box_b) = 0;
+};
+
+Runner* make_runner_fp64(const Arena<double>& A, const RunInfo& I);
+Runner* make_runner_mixed(const Arena<float>& A, const RunInfo& I);
+
+}  // namespace ocfd

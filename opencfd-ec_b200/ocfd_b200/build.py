@@ -1,0 +1,71 @@
+"""Builds libocfd_b200.so in-tree with nvcc for sm_100a.
+
+The FP64 translation units (setup.cu, solver_fp64.cu) are compiled with --fmad=false so every
+a*b+c is rounded twice, as the FP64 reference evaluates it; the mixed-precision unit keeps FMA.
+"""
+import os
+import subprocess
+import sys
+
+from . import ROOT_DIR
+
+CSRC = os.path.join(ROOT_DIR, "csrc")
+LIB_PATH = os.path.join(ROOT_DIR, "libocfd_b200.so")
+BUILD_DIR = os.path.join(ROOT_DIR, "_build")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
+
+UNITS = [
+    ("setup.cu", ["--fmad=false"]),
+    ("solver_fp64.cu", ["--fmad=false"]),
+    ("solver_mixed.cu", []),
+    ("capi.cu", []),
+]
+
+
+def sources():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))] + [
+        os.path.join(os.path.dirname(ROOT_DIR), "include", "ocfd_ec_gpu.h")]
+
+
+def up_to_date():
+    if not os.path.exists(LIB_PATH):
+        return False
+    t = os.path.getmtime(LIB_PATH)
+    return all(os.path.getmtime(s) <= t for s in sources())
+
+
+def build(force=False, verbose=False, extra=()):
+    if not force and up_to_date():
+        return LIB_PATH
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    objs = []
+    procs = []
+    for src, flags in UNITS:
+        obj = os.path.join(BUILD_DIR, src.replace(".cu", ".o"))
+        cmd = [NVCC] + ARCH + COMMON + list(flags) + list(extra) + ["-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        objs.append(obj)
+    failed = []
+    for src, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            failed.append((src, out.decode(errors="replace")))
+        elif verbose and out:
+            print(out.decode(errors="replace"), file=sys.stderr)
+    if failed:
+        msg = "\n".join("---- %s\n%s" % f for f in failed)
+        raise RuntimeError("nvcc failed:\n" + msg)
+    tmp = LIB_PATH + ".tmp"
+    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
+    subprocess.check_call(cmd)
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(LIB_PATH)

@@ -1,0 +1,162 @@
+"""ctypes binding of libocfd_b200.so (C-ABI in include/ocfd_ec_gpu.h).
+
+There is no CPU fallback: if the library is missing or fails to load, every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import ROOT_DIR
+from .params import OcfdParams
+
+LIB_PATH = os.path.join(ROOT_DIR, "libocfd_b200.so")
+_lib = None
+
+OCFD_OK, OCFD_ERR_ARG, OCFD_ERR_CUDA, OCFD_ERR_OOM, OCFD_ERR_NAN, OCFD_ERR_TIMEOUT, OCFD_ERR_UNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
+
+EXPORTED = [
+    "ocfd_default_params", "ocfd_finalize_params", "ocfd_create", "ocfd_destroy", "ocfd_last_error", "ocfd_state_size",
+    "ocfd_set_state", "ocfd_get_state", "ocfd_init_flow", "ocfd_advance", "ocfd_residual", "ocfd_forces",
+    "ocfd_limiter_status", "ocfd_array_shape", "ocfd_get_array", "ocfd_version", "ocfd_compute_residual",
+]
+
+
+class OcfdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (code %d)" % (msg, code))
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OcfdError(-7, "libocfd_b200.so not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, dp, cp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.c_char_p
+        pp = ctypes.POINTER(OcfdParams)
+        L.ocfd_default_params.argtypes = [pp]
+        L.ocfd_finalize_params.argtypes = [pp]
+        L.ocfd_create.argtypes = [pp, ctypes.c_int, ip, ctypes.POINTER(dp), ip, ip, ctypes.POINTER(dp), ctypes.POINTER(vp)]
+        L.ocfd_destroy.argtypes = [vp]
+        L.ocfd_last_error.argtypes = [vp]
+        L.ocfd_last_error.restype = cp
+        L.ocfd_state_size.argtypes = [vp, ctypes.c_int]
+        L.ocfd_state_size.restype = ctypes.c_longlong
+        L.ocfd_set_state.argtypes = [vp, ctypes.c_int, dp]
+        L.ocfd_get_state.argtypes = [vp, ctypes.c_int, dp]
+        L.ocfd_init_flow.argtypes = [vp]
+        L.ocfd_compute_residual.argtypes = [vp, ctypes.c_int]
+        L.ocfd_advance.argtypes = [vp, ctypes.c_int, ip, dp]
+        L.ocfd_residual.argtypes = [vp, dp, dp]
+        L.ocfd_forces.argtypes = [vp, dp, dp, dp, dp]
+        L.ocfd_limiter_status.argtypes = [vp, ctypes.c_int, ip, ip]
+        L.ocfd_array_shape.argtypes = [vp, ctypes.c_int, cp, ip, ip, ip]
+        L.ocfd_get_array.argtypes = [vp, ctypes.c_int, cp, dp]
+        L.ocfd_version.restype = cp
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class Solver:
+    """One case resident on the current GPU, driven through the C-ABI."""
+
+    def __init__(self, params, case, dw=None):
+        L = lib()
+        self.case = case
+        self.params = params.copy()
+        nijk, xyz, nsub, inc = case.flat()
+        self._keep = (nijk, xyz, nsub, inc)
+        xyz_ptrs = (ctypes.POINTER(ctypes.c_double) * len(xyz))(*[_dp(a) for a in xyz])
+        dwp = None
+        if dw is not None:
+            self._dw = [np.ascontiguousarray(d, dtype=np.float64) for d in dw]
+            dwp = (ctypes.POINTER(ctypes.c_double) * len(dw))(*[_dp(a) for a in self._dw])
+        h = ctypes.c_void_p()
+        rc = L.ocfd_create(ctypes.byref(self.params), len(xyz), _ip(nijk), xyz_ptrs, _ip(nsub), _ip(inc), dwp, ctypes.byref(h))
+        if rc != 0:
+            raise OcfdError(rc, "ocfd_create failed")
+        self.h = h
+        self.nblk = len(xyz)
+        self.nvar = int(self.params.nvar)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ocfd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise OcfdError(rc, "%s: %s" % (what, lib().ocfd_last_error(self.h).decode()))
+
+    def advance(self, n=1):
+        ks, tt = ctypes.c_int(), ctypes.c_double()
+        self._check(lib().ocfd_advance(self.h, n, ctypes.byref(ks), ctypes.byref(tt)), "advance")
+        return ks.value, tt.value
+
+    def init_flow(self):
+        self._check(lib().ocfd_init_flow(self.h), "init_flow")
+
+    def compute_residual(self, lusgs=False):
+        self._check(lib().ocfd_compute_residual(self.h, int(lusgs)), "compute_residual")
+
+    def residual(self):
+        a, b = np.zeros(7), np.zeros(7)
+        rc = lib().ocfd_residual(self.h, _dp(a), _dp(b))
+        if rc == OCFD_ERR_NAN:
+            raise FloatingPointError(lib().ocfd_last_error(self.h).decode())
+        self._check(rc, "residual")
+        return a, b
+
+    def forces(self):
+        ft = np.zeros(9)
+        cl, cd, cs = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(lib().ocfd_forces(self.h, _dp(ft), ctypes.byref(cl), ctypes.byref(cd), ctypes.byref(cs)), "forces")
+        return ft, cl.value, cd.value, cs.value
+
+    def state_shape(self, b):
+        nx, ny, nz = self.case.dims[b]
+        return (nz + 7, ny + 7, nx + 7, self.nvar)
+
+    def get_state(self, b, out=None):
+        U = out if out is not None else np.empty(self.state_shape(b))
+        self._check(lib().ocfd_get_state(self.h, b, _dp(U)), "get_state")
+        return U
+
+    def set_state(self, b, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        self._check(lib().ocfd_set_state(self.h, b, _dp(U)), "set_state")
+
+    def limiter_status(self, b):
+        n, o = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().ocfd_limiter_status(self.h, b, ctypes.byref(n), ctypes.byref(o)), "limiter_status")
+        return n.value, o.value
+
+    def get_array(self, b, name):
+        lo, hi, nv = (ctypes.c_int * 3)(), (ctypes.c_int * 3)(), ctypes.c_int()
+        self._check(lib().ocfd_array_shape(self.h, b, name.encode(), lo, hi, ctypes.byref(nv)), "array_shape " + name)
+        shape = tuple(hi[d] - lo[d] + 1 for d in (2, 1, 0))
+        if nv.value > 1:
+            shape = shape + (nv.value,)
+        out = np.empty(shape)
+        self._check(lib().ocfd_get_array(self.h, b, name.encode(), _dp(out)), "get_array " + name)
+        return out, tuple(lo), tuple(hi)
+
+
+def version():
+    return lib().ocfd_version().decode()

@@ -1,0 +1,66 @@
+"""Benchmark and parity cases: mesh + flow parameters for each configuration.
+
+config1: plain FP64 Euler channel bump, 129x65x17, MUSCL3 (van Albada) + Roe, LU-SGS CFL 5, M 0.5.
+config2: plain FP64 RANS-SA swept wing, 8 uneven blocks, ~2.1M cells, WENO5 + Roe, LU-SGS,
+         M 0.8, AoA 3 deg, Re 1e7 per chord.
+config4: 2-D-extruded NACA 4-digit O-mesh airfoils (k = 3 nodes), SA, AUSMPW + MUSCL3, mixed.
+Small variants of each are the parity cases (sizes the CPU oracle finishes in seconds).
+"""
+import numpy as np
+
+from . import meshgen
+from .params import make_params
+
+
+def config1(scale=1.0, cuts_i=(), **over):
+    ni = int(round((129 - 1) * scale)) + 1
+    nj = int(round((65 - 1) * scale)) + 1
+    nk = max(3, int(round((17 - 1) * scale)) + 1)
+    case = meshgen.channel_bump(ni, nj, nk, cuts_i=cuts_i, name="config1_bump_%dx%dx%d" % (ni, nj, nk))
+    raw = dict(ma=0.5, aoa=0.0, if_viscous=0, iflag_scheme=5, iflag_flux=4, time_method=0, cfl=5.0, t_end=1.0e9)
+    raw.update(over)
+    raw.pop("t_end")
+    return make_params(**raw), case
+
+
+def config2(ni=257, nj=97, nk_wing=61, nk_tip=26, i_cut=49, **over):
+    case = meshgen.swept_wing(ni=ni, nj=nj, nk_wing=nk_wing, nk_tip=nk_tip, i_cut=i_cut,
+                              name="config2_wing_%dx%dx%d" % (ni, nj, nk_wing + nk_tip - 1))
+    raw = dict(ma=0.8, aoa=3.0, re=1.0e7, if_viscous=1, iflag_turbulence_model=2, iflag_scheme=7, iflag_flux=4,
+               time_method=0, cfl=5.0, ref_s=meshgen.wing_ref_area(), ref_l=1.0)
+    raw.update(over)
+    return make_params(**raw), case
+
+
+def config2_small(**over):
+    """A reduced swept wing (8 blocks) for oracle parity."""
+    return config2(ni=41, nj=17, nk_wing=9, nk_tip=6, i_cut=9, **over)
+
+
+def airfoil(ni=129, nj=33, m=0.02, p=0.4, t=0.12, ma=0.7, aoa=2.0, re=6.0e6, scheme=5, flux=6, turb=2, precision=0,
+            time_method=0, cfl=5.0, ds=2e-6, **over):
+    case = meshgen.airfoil_omesh(ni=ni, nj=nj, nk=3, m=m, p=p, t=t, ds=ds, name="naca_%dx%d" % (ni, nj))
+    raw = dict(ma=ma, aoa=aoa, re=re, if_viscous=1, iflag_turbulence_model=turb, iflag_scheme=scheme, iflag_flux=flux,
+               time_method=time_method, cfl=cfl, precision=precision, ref_s=case.xyz[0][2].max() - case.xyz[0][2].min())
+    raw.update(over)
+    return make_params(**raw), case
+
+
+def config4_batch(n=64, seed=1234, **over):
+    """64 airfoil solves: O-mesh sizes uniform in 129x33 .. 385x97 (odd ni), NACA 4-digit camber
+    U[0,0.04], thickness U[0.09,0.15], Mach U[0.3,0.85], AoA U[-2,6] deg, Re 6e6, SA, AUSMPW +
+    MUSCL3, mixed precision.  Returns a list of (params, case)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        ni = int(rng.integers(64, 193)) * 2 + 1      # 129..385, odd
+        nj = int(rng.integers(33, 98))
+        m = float(rng.uniform(0.0, 0.04))
+        p = 0.4
+        t = float(rng.uniform(0.09, 0.15))
+        ma = float(rng.uniform(0.3, 0.85))
+        aoa = float(rng.uniform(-2.0, 6.0))
+        raw = dict(precision=1)
+        raw.update(over)
+        out.append(airfoil(ni=ni, nj=nj, m=m, p=p, t=t, ma=ma, aoa=aoa, re=6.0e6, scheme=5, flux=6, turb=2, **raw))
+    return out

@@ -1,0 +1,305 @@
+#!/usr/bin/env python
+"""Benchmark of the OpenCFD-EC per-iteration hot path on B200.
+
+Workload (the headline configuration): the FP64 RANS-SA swept wing, 8 uneven blocks, ~2.1 M
+cells, WENO5 + Roe, LU-SGS, M 0.8, AoA 3 deg, Re 1e7 per chord (analytic O-H mesh; synthetic,
+seeded - no external mesh or dataset).  A step is one NS_Time_advance (residual + LU-SGS +
+update + limiter + BC + halo); the metric is cell-updates/s = cells x steps / device time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank solves its own copy of the case (independent solves at
+different angles of attack, no collective on the data path: "weak" scaling); the timed region is
+bracketed by barriers and the slowest rank's device time is used.  --impl reference times the CPU
+restatement of the reference algorithm (oracle/) on the host cores instead (rank 0 only).
+One JSON line is printed by rank 0.
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "opencfd-ec_b200"))
+
+# algorithmic bytes per cell-update (per-kernel data model: unique inputs + outputs once)
+#   residual: reads U + metrics, writes Res, dt, Lc, Lv;  LU-SGS lower: Res,U,dt,vol,Lc,Lv,S,n -> DU*;
+#   upper + update: DU*,U,dt,vol,Lc,Lv,S,n -> U
+BYTES = {
+    ("fp64", 5): {"residual": 248, "lusgs_lower": 256, "lusgs_upper": 256},
+    ("fp64", 6): {"residual": 584, "lusgs_lower": 304, "lusgs_upper": 304},
+    ("fp64", 7): {"residual": 600, "lusgs_lower": 328, "lusgs_upper": 328},
+    ("mixed", 5): {"residual": 148, "lusgs_lower": 176, "lusgs_upper": 176},
+    ("mixed", 6): {"residual": 356, "lusgs_lower": 192, "lusgs_upper": 192},
+    ("mixed", 7): {"residual": 364, "lusgs_lower": 216, "lusgs_upper": 216},
+}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock / throttle reasons through NVML while the timed region runs."""
+
+    def __init__(self, dev_index, period=0.01):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.period, self.stop_flag, self.th, self.h = period, False, None, None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            import torch
+            uuid = str(torch.cuda.get_device_properties(dev_index).uuid)
+            n = pynvml.nvmlDeviceGetCount()
+            for q in range(n):
+                hq = pynvml.nvmlDeviceGetHandleByIndex(q)
+                u = pynvml.nvmlDeviceGetUUID(hq)
+                u = u.decode() if isinstance(u, bytes) else u
+                if uuid in u or u.replace("GPU-", "") in uuid:
+                    self.h = hq
+            if self.h is None and n == 1:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(0)
+            self.nv = pynvml
+            if self.h is not None:
+                self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.h = None
+
+    def _run(self):
+        nv = self.nv
+        names = {
+            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
+        }
+        while not self.stop_flag:
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h) if hasattr(nv, "nvmlDeviceGetCurrentClocksEventReasons") else nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                for k, bit in names.items():
+                    if r & bit:
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.h is not None:
+            self.th = threading.Thread(target=self._run, daemon=True)
+            self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop_flag = True
+        if self.th:
+            self.th.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+def make_case(args, rank):
+    from ocfd_b200 import cases
+    prec = 1 if args.precision == "mixed" else 0
+    # independent solves per rank: the angle of attack varies with the rank
+    return cases.config2(precision=prec, aoa=3.0 + 0.25 * rank)
+
+
+def cpu_sample(args, min_seconds=10.0, max_steps=4):
+    """Times the CPU oracle (restatement of the reference algorithm, all host threads) on the same
+    workload: full mesh, one warm-up step, then steps until min_seconds of CPU work (at most
+    max_steps).  Returns (cell-updates/s, threads, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    p, case = make_case(args, 0)
+    o = oracle_py.OracleCase(p, case)
+    o.advance(1)
+    n, t0 = 0, time.time()
+    while True:
+        o.advance(1)
+        n += 1
+        el = time.time() - t0
+        if el >= min_seconds or n >= max_steps:
+            break
+    o.close()
+    threads = int(os.environ.get("OCFD_ORACLE_THREADS", os.cpu_count() or 1))
+    return case.ncells * n / el, threads, "%s, %d LU-SGS step(s) after 1 warm-up, %.1f s on %d host threads" % (case.name, n, el, threads)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    oracle_py.build()
+    p, case = make_case(args, 0)
+    o = oracle_py.OracleCase(p, case)
+    o.advance(args.warmup)
+    t0 = time.time()
+    o.advance(args.steps)
+    el = time.time() - t0
+    o.close()
+    threads = int(os.environ.get("OCFD_ORACLE_THREADS", os.cpu_count() or 1))
+    v = case.ncells * args.steps / el
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (analytic O-H swept-wing mesh, seeded)",
+        "config": {"workload": case.name + " RANS-SA WENO5+Roe LU-SGS", "cells": case.ncells, "blocks": len(case.dims),
+                   "precision": "fp64"},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                         "sample": "full workload, %d steps after %d warm-up on the CPU restatement (oracle/)" % (args.steps, args.warmup)},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    from ocfd_b200 import build, capi
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    if not os.path.exists(capi.LIB_PATH):
+        build.build()
+
+    p, case = make_case(args, rank)
+    s = capi.Solver(p, case)
+    stream = torch.cuda.ExternalStream(s.stream())
+    s.advance(args.warmup)
+    s.residual()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        s.advance(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    rmax, rrms = s.residual()
+    ncell = case.ncells
+    value = world * ncell * args.steps / (ms * 1e-3)
+
+    # roofline of the dominant kernel (per-phase device time measured with CUDA events)
+    ph = s.profile(3)
+    peak, peak_kind = peaks()
+    prec = args.precision
+    bmodel = BYTES[(prec, s.nvar)]
+    dom = max(bmodel, key=lambda k: ph[k])
+    t_dom = ph[dom] / 3.0 * 1e-3
+    achieved = bmodel[dom] * ncell / t_dom / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            with open(tfile) as f:
+                tj = json.load(f)
+            key = "%s/%s" % (prec, dom)
+            if key in tj:
+                traffic = tj[key]["bytes_per_cell"] * ncell
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": traffic, "bytes_per_cell": bmodel[dom],
+                "phase_ms_per_step": {k: v / 3.0 for k, v in ph.items()}}
+
+    # end to end through the C-ABI with host buffers: state H2D from pinned memory, then every
+    # step advance + residual norms + forces read back (the driver loop with Kstep_show = 1),
+    # state D2H at the end
+    host = [torch.empty(s.state_shape(b), dtype=torch.float64, pin_memory=True).numpy() for b in range(s.nblk)]
+    for b in range(s.nblk):
+        s.get_state(b, out=host[b])
+    e2e_steps = min(args.steps, 50)
+    barrier()
+    t0 = time.perf_counter()
+    for b in range(s.nblk):
+        s.set_state(b, host[b])
+    for _ in range(e2e_steps):
+        s.advance(1)
+        s.residual()
+        s.forces()
+    for b in range(s.nblk):
+        s.get_state(b, out=host[b])
+    t_e2e = time.perf_counter() - t0
+    state_bytes = sum(h.nbytes for h in host)
+    e2e = {"value": world * ncell * e2e_steps / t_e2e, "unit": "cell-updates/s", "steps": e2e_steps,
+           "h2d_bytes_per_step": state_bytes / e2e_steps, "d2h_bytes_per_step": state_bytes / e2e_steps + (14 + 9) * 8}
+    launches = s.launches_per_step() * args.steps
+    s.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            v, cores, desc = cpu_sample(args)
+            cpu = {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port", "sample": desc}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "port", "sample": "failed: %s" % e}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32/f64",
+            "data": "synthetic (analytic O-H swept-wing mesh, seeded)",
+            "config": {"workload": case.name + " RANS-SA WENO5+Roe LU-SGS", "cells": ncell, "blocks": len(case.dims),
+                       "precision": prec, "parallelism": "replicas x%d (independent solves, no collective)" % world,
+                       "l2": "working set %.1f GB > 126 MB L2 (no flush needed)" % (ncell * 1200 / 1e9)},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk.summary(), "residual_rms": rrms[: s.nvar].tolist(),
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

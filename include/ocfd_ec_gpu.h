@@ -192,6 +192,20 @@ int ocfd_get_array(ocfd_handle* h, int blk, const char* name, double* out);
 /* Library build/ABI information: "ocfd-b200 <abi> sm_100a ..." */
 const char* ocfd_version(void);
 
+/* ---- measurement (no counterpart in the reference, which only prints wall time per step at
+ *      opencfd_ec3d_v1.16a.f90:224-243) ----------------------------------------------------- */
+
+/* The cudaStream_t (as void*) all work of the handle is queued on, so a caller can time it with
+ * CUDA events or order its own work after it. */
+void* ocfd_stream(ocfd_handle* h);
+/* Runs nsteps steps phase by phase (outside the step graph) and accumulates the device time of
+ * each phase in ms: [0] residual (primitives, turbulence, fluxes, assembly, dt), [1] LU-SGS lower
+ * sweep, [2] LU-SGS upper sweep, [3] update + flow limiter + vt/k/w clamps, [4] BC + halo +
+ * corners, [5] whole step.  phase_ms must hold 8 doubles. */
+int ocfd_profile(ocfd_handle* h, int nsteps, double* phase_ms);
+/* Kernel launches queued by one ocfd_advance step (all of them this library's own kernels). */
+int ocfd_launches_per_step(ocfd_handle* h);
+
 #ifdef __cplusplus
 }
 #endif

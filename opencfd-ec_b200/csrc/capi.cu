@@ -17,6 +17,7 @@
 
 #include "../../include/ocfd_ec_gpu.h"
 #include "arena.h"
+#include "lusgs.cuh"
 #include "runner.h"
 #include "setup.h"
 
@@ -80,6 +81,9 @@ struct ocfd_handle {
   long long max_box_b = 0;
   Arena<double> A64;
   Arena<float> A32;
+  LuArgs lu{};
+  std::vector<LuTile> lu_tiles;
+  int* d_lu_err = nullptr;
   std::unique_ptr<Runner> run;
   cudaStream_t st = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -467,10 +471,49 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
     convert_to_float(h->d_dwd, h->d_dwf, tc, h->st);
   }
   if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "geometry sync"); }
+  // ---- LU-SGS wavefront tiles: TJ x TK columns per CTA (64 threads), ordered by J+K
+  {
+    int min_nzm = 1 << 30;
+    for (const BlkD& B : h->blk) min_nzm = std::min(min_nzm, B.nz - 1);
+    int TK = min_nzm <= 2 ? 2 : (min_nzm <= 4 ? 4 : 8);
+    int TJ = 64 / TK;
+    std::vector<int> tile_of(3 * nblk);
+    std::vector<std::pair<int, LuTile>> order;
+    int first = 0;
+    for (int b = 0; b < nblk; b++) {
+      const BlkD& B = h->blk[b];
+      int nJ = (B.ny - 1 + TJ - 1) / TJ, nK = (B.nz - 1 + TK - 1) / TK;
+      tile_of[3 * b] = first; tile_of[3 * b + 1] = nJ; tile_of[3 * b + 2] = nK;
+      for (int K = 0; K < nK; K++)
+        for (int J = 0; J < nJ; J++) order.push_back({J + K, LuTile{b, 1 + J * TJ, 1 + K * TK, 0}});
+      first += nJ * nK;
+    }
+    std::stable_sort(order.begin(), order.end(), [](const std::pair<int, LuTile>& a, const std::pair<int, LuTile>& b) { return a.first < b.first; });
+    for (auto& o : order) h->lu_tiles.push_back(o.second);
+    LuTile* d_tiles = M.alloc<LuTile>(h->lu_tiles.size(), e);
+    int* d_tile_of = M.alloc<int>(tile_of.size(), e);
+    int* d_counter = M.alloc<int>(2, e);
+    int* d_progress = M.alloc<int>(first, e);
+    h->d_lu_err = M.alloc<int>(1, e);
+    if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "lu tables"); }
+    cudaMemcpy(d_tiles, h->lu_tiles.data(), h->lu_tiles.size() * sizeof(LuTile), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_tile_of, tile_of.data(), tile_of.size() * sizeof(int), cudaMemcpyHostToDevice);
+    h->lu.tiles = d_tiles; h->lu.ntiles = first; h->lu.counter = d_counter; h->lu.progress = d_progress;
+    h->lu.tile_of = d_tile_of; h->lu.err = h->d_lu_err; h->lu.TJ = TJ; h->lu.TK = TK;
+    h->lu.spin_limit = 4000000;  // x ~64 ns: a few hundred ms before a stuck wait gives up
+  }
   // ---- runner
   RunInfo I;
   I.nvar = NV; I.time_method = p->time_method; I.viscous = p->if_viscous; I.turb = turb; I.max_plane = h->max_plane;
   I.ncchunk = (int)h->cchunk.size(); I.nwchunk = (int)h->wchunk.size();
+  I.lu_planes = std::getenv("OCFD_LUSGS_PLANES") ? 1 : 0;
+  I.lu = &h->lu;
+  {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    I.lu_grid = std::max(1, std::min(h->lu.ntiles, nsm * 8));
+  }
   if (h->prec == OCFD_PREC_MIXED) {
     fill_arena<float>(h, h->A32, h->d_Mf, h->d_volf, h->d_dtmf, h->d_dwf);
     h->run.reset(make_runner_mixed(h->A32, I));
@@ -601,6 +644,9 @@ extern "C" int ocfd_residual(ocfd_handle* h, double* rmax, double* rrms) {
     rmax[m] = m < h->nvar ? out[m] : 0.0;
     rrms[m] = m < h->nvar ? std::sqrt(out[7 + m] / (double)h->ncell) : 0.0;
   }
+  int lu_err = 0;
+  cudaMemcpy(&lu_err, h->d_lu_err, 4, cudaMemcpyDeviceToHost);
+  if (lu_err) return fail(h, OCFD_ERR_TIMEOUT, "LU-SGS wavefront: a bounded wait between tiles timed out");
   if (nan_at != ~0ULL) {
     long long g = (long long)(nan_at / 8);
     int m = (int)(nan_at % 8);
@@ -644,6 +690,31 @@ extern "C" int ocfd_forces(ocfd_handle* h, double* ft, double* cl, double* cd, d
   if (cl) *cl = L;
   if (cd) *cd = D;
   if (cs) *cs = S;
+  return OCFD_OK;
+}
+
+extern "C" void* ocfd_stream(ocfd_handle* h) { return h ? (void*)h->st : nullptr; }
+
+extern "C" int ocfd_launches_per_step(ocfd_handle* h) { return h ? h->run->launches_per_step() : 0; }
+
+extern "C" int ocfd_profile(ocfd_handle* h, int nsteps, double* phase_ms) {
+  if (!h || !phase_ms || nsteps < 1) return OCFD_ERR_ARG;
+  cudaEvent_t ev[6];
+  for (int q = 0; q < 6; q++) cudaEventCreate(&ev[q]);
+  for (int q = 0; q < 8; q++) phase_ms[q] = 0.0;
+  cudaError_t e = cudaSuccess;
+  for (int s = 0; s < nsteps && e == cudaSuccess; s++) {
+    h->run->step(h->st, ev);
+    e = cudaStreamSynchronize(h->st);
+    float ms[6] = {0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < 5 && e == cudaSuccess; q++) e = cudaEventElapsedTime(&ms[q], ev[q], ev[q + 1]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms[5], ev[0], ev[5]);
+    for (int q = 0; q < 6; q++) phase_ms[q] += ms[q];
+    h->tt = h->tt + h->P.dt_global;
+    h->kstep = h->kstep + 1;
+  }
+  for (int q = 0; q < 6; q++) cudaEventDestroy(ev[q]);
+  if (e != cudaSuccess) return cuda_fail(h, e, "profile");
   return OCFD_OK;
 }
 

@@ -1,0 +1,249 @@
+// LU-SGS sweeps (du_LU_SGS, sub_LU_SGS.f90:4-129) as one persistent pipelined-wavefront kernel
+// per sweep instead of one launch per hyperplane.
+//
+// The lower sweep needs DU(i-1,j,k), DU(i,j-1,k), DU(i,j,k-1) before DU(i,j,k); any order that
+// respects these dependencies gives bitwise the same DU as the reference's i+j+k = plane order,
+// because every cell evaluates the same expression from the same operands.
+//
+// Each block is cut into tiles of TJ x TK (j,k) columns.  A CTA of TJ*TK threads owns one tile
+// and marches along i with a skew: at local step t, thread (lj,lk) updates i = t - lj - lk.
+// Everything a cell's neighbours need from it (U, DU, the spectral radii of the shared face) is
+// handed over through shared memory or registers, so every cell's data is read from HBM once per
+// sweep, and the data of the next step is prefetched into registers while the current step's
+// dependent chain runs.  Across tile boundaries the neighbour tile publishes the number of steps
+// it has completed (st.release.gpu after a CTA barrier); the consumer waits (ld.acquire.gpu,
+// bounded spin) until the producer is far enough ahead and then reads the values through L2.
+//
+// Deadlock freedom: CTAs take tiles from a global counter in topological order (J+K ascending
+// for the lower sweep, descending for the upper), so every producer of a tile was handed out
+// earlier to a CTA that is already running and that itself depends only on earlier tiles.  Every
+// wait is bounded; a timeout sets an error flag and the CTA finishes its tile without waiting
+// (the host reports OCFD_ERR_TIMEOUT).
+#pragma once
+#include "solver.cuh"
+
+namespace ocfd {
+
+struct LuTile {
+  int blk, j0, k0, pad;  // first column (1-based j, k) of the tile
+};
+
+struct LuArgs {
+  const LuTile* tiles;  // lower-sweep order (J+K ascending); the upper sweep walks it backwards
+  int ntiles;
+  int* counter;         // [0] lower, [1] upper tile counters
+  int* progress;        // per tile: steps completed in the current sweep
+  int* tile_of;         // per block: first tile index, tiles per row (nJ), tiles per column (nK)
+  int* err;             // timeout flag
+  int TJ, TK;
+  long long spin_limit;
+};
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// wait until *p >= need; returns false on timeout
+__device__ __forceinline__ bool wait_ge(const int* p, int need, long long limit, int& seen) {
+  long long it = 0;
+  int v;
+  while ((v = ld_acquire(p)) < need) {
+    if (++it > limit) { seen = v; return false; }
+    if (it > 32) __nanosleep(32);
+  }
+  seen = v;
+  return true;
+}
+
+// data of one cell that the sweep reads from HBM
+template <int NV>
+struct LuCell {
+  double U[NV];    // conserved state (U6/U7 clamped as limit_vt leaves them)
+  double R[NV];    // lower sweep: Res; upper sweep: DU* of the lower sweep
+  double Lc[3], Lv[3];
+  double a0;       // vol/dt + w (Lci+Lcj+Lck)
+  double n[3][3];  // unit normals of the faces shared with the three upstream neighbours
+  double S[3];     // their areas
+};
+
+template <class T, int NV, bool UPPER>
+__device__ __forceinline__ void lu_load(const Arena<T>& A, const BlkD& B, int i, int j, int k, double w, LuCell<NV>& c) {
+  const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
+  const long long ci = cix(B, i, j, k), bi = bix(B, i, j, k);
+#pragma unroll
+  for (int m = 0; m < NV; m++) {
+    double u = A.U[m * tb + bi];
+    c.U[m] = m >= 5 ? clamp0(u) : u;
+    c.R[m] = UPPER ? A.DU[m * tc + ci] : (double)A.Res[m * tc + ci];
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++) { c.Lc[d] = A.Lc[d * tc + ci]; c.Lv[d] = A.Lv[d * tc + ci]; }
+  c.a0 = (double)A.vold[ci] / (double)A.dt[ci] + w * (c.Lc[0] + c.Lc[1] + c.Lc[2]);
+  const long long f = fix_(B, i, j, k);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    // normal of the cell's lower face in direction d; the area of the lower face (lower sweep)
+    // or of the upper face (upper sweep, the reference pairs n(i) with S(i+1), sub_LU_SGS.f90:96-97)
+    c.n[d][0] = A.M[(M_NI1 + 3 * d) * tf + f];
+    c.n[d][1] = A.M[(M_NI2 + 3 * d) * tf + f];
+    c.n[d][2] = A.M[(M_NI3 + 3 * d) * tf + f];
+    long long fs = f;
+    if (UPPER) fs = fix_(B, i + (d == 0), j + (d == 1), k + (d == 2));
+    c.S[d] = A.M[(M_SI + d) * tf + fs];
+  }
+}
+
+// what a cell hands to its downstream neighbours in j and k
+template <int NV>
+struct LuOut {
+  double U[NV], DU[NV];
+  double Lcj, Lck, Lvj, Lvk;
+};
+
+template <class T, int NV, bool UPPER>
+__global__ void __launch_bounds__(64) k_lusgs_wave(Arena<T> A, LuArgs L) {
+  __shared__ int s_tile;
+  __shared__ LuOut<NV> s_out[2][64];
+  const long long tb = A.tot_box, tc = A.tot_cell;
+  const int TJ = L.TJ, TK = L.TK;
+  const int lt = threadIdx.x, lj = lt % TJ, lk = lt / TJ;
+  for (;;) {
+    if (lt == 0) s_tile = atomicAdd(&L.counter[UPPER ? 1 : 0], 1);
+    __syncthreads();
+    const int q = s_tile;
+    if (q >= L.ntiles) break;
+    const LuTile tl = L.tiles[UPPER ? (L.ntiles - 1 - q) : q];
+    const BlkD& B = A.blk[tl.blk];
+    const SolveP& s = A.sp[B.solve];
+    const int nxm = B.nx - 1, nym = B.ny - 1, nzm = B.nz - 1;
+    const int j = UPPER ? (tl.j0 + TJ - 1 - lj) : (tl.j0 + lj);
+    const int k = UPPER ? (tl.k0 + TK - 1 - lk) : (tl.k0 + lk);
+    const bool active = j >= 1 && j <= nym && k >= 1 && k <= nzm;
+    const int* tb3 = L.tile_of + 3 * tl.blk;
+    const int first = tb3[0], nJ = tb3[1], nK = tb3[2];
+    const int J = (tl.j0 - 1) / TJ, K = (tl.k0 - 1) / TK;
+    int pj = -1, pk = -1;
+    if (!UPPER) {
+      if (J > 0) pj = first + (J - 1) + nJ * K;
+      if (K > 0) pk = first + J + nJ * (K - 1);
+    } else {
+      if (J < nJ - 1) pj = first + (J + 1) + nJ * K;
+      if (K < nK - 1) pk = first + J + nJ * (K + 1);
+    }
+    const int my = first + J + nJ * K;
+    const int nsteps = nxm + TJ + TK - 2;
+    const double w = s.w_lu, gamma = s.gamma;
+    const bool visc = s.viscous == 1;
+    const int off = UPPER ? 1 : -1;
+    // neighbour columns outside the tile (read through L2 from the producer tile)
+    const bool jx = (lj == 0) && (UPPER ? j != nym : j != 1);
+    const bool kx = (lk == 0) && (UPPER ? k != nzm : k != 1);
+    // the cell of step t is i(t); prefetch the first one
+    auto i_of = [&](int t) { int il = t - lj - lk; return UPPER ? (nxm - il) : (il + 1); };
+    auto on_at = [&](int t) { int il = t - lj - lk; return active && il >= 0 && il < nxm; };
+    LuCell<NV> cur, nxt;
+    if (on_at(0)) lu_load<T, NV, UPPER>(A, B, i_of(0), j, k, w, cur);
+    double prevU[NV], prevDU[NV], prevLci = 0.0, prevLvi = 0.0;  // the i-upstream cell (this thread's last one)
+#pragma unroll
+    for (int m = 0; m < NV; m++) { prevU[m] = 0.0; prevDU[m] = 0.0; }
+    int seen_j = 0, seen_k = 0;
+    for (int t = 0; t < nsteps; t++) {
+      const bool on = on_at(t);
+      const int i = i_of(t);
+      // prefetch the next step's cell while this step's chain runs
+      if (on_at(t + 1)) lu_load<T, NV, UPPER>(A, B, i_of(t + 1), j, k, w, nxt);
+      if (lt == 0) {
+        bool ok = true;
+        if (pj >= 0 && seen_j < min(t + TJ, nsteps)) ok &= wait_ge(L.progress + pj, min(t + TJ, nsteps), L.spin_limit, seen_j);
+        if (pk >= 0 && seen_k < min(t + TK, nsteps)) ok &= wait_ge(L.progress + pk, min(t + TK, nsteps), L.spin_limit, seen_k);
+        if (!ok) atomicExch(L.err, 1);
+      }
+      __syncthreads();
+      LuOut<NV> out;
+      if (on) {
+        double alfa[NV];
+#pragma unroll
+        for (int m = 0; m < NV; m++) alfa[m] = cur.a0;
+        if (visc) {
+          double lv = cur.Lv[0] + cur.Lv[1] + cur.Lv[2];
+#pragma unroll
+          for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + 2.0 * lv;
+          if (NV == 6) {
+            if (!UPPER) alfa[5] = alfa[5] + lv;
+            else alfa[5] = alfa[5] + cur.Lv[0] + cur.Lv[1] + cur.Lv[2];
+          }
+        }
+        double acc[3][NV];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const bool has = UPPER ? (d == 0 ? i != nxm : (d == 1 ? j != nym : k != nzm)) : (d == 0 ? i != 1 : (d == 1 ? j != 1 : k != 1));
+          if (!has) {
+#pragma unroll
+            for (int m = 0; m < NV; m++) acc[d][m] = 0.0;
+            continue;
+          }
+          double Un[NV], DUn[NV], Lcn, Lvn;
+          if (d == 0) {
+#pragma unroll
+            for (int m = 0; m < NV; m++) { Un[m] = prevU[m]; DUn[m] = prevDU[m]; }
+            Lcn = prevLci; Lvn = prevLvi;
+          } else if ((d == 1 && !jx) || (d == 2 && !kx)) {
+            const LuOut<NV>& o = s_out[(t + 1) & 1][d == 1 ? lt - 1 : lt - TJ];
+#pragma unroll
+            for (int m = 0; m < NV; m++) { Un[m] = o.U[m]; DUn[m] = o.DU[m]; }
+            Lcn = d == 1 ? o.Lcj : o.Lck;
+            Lvn = d == 1 ? o.Lvj : o.Lvk;
+          } else {
+            const int jj = j + (d == 1 ? off : 0), kk = k + (d == 2 ? off : 0);
+            const long long cn = cix(B, i, jj, kk), bn = bix(B, i, jj, kk);
+#pragma unroll
+            for (int m = 0; m < NV; m++) {
+              double u = A.U[m * tb + bn];
+              Un[m] = m >= 5 ? clamp0(u) : u;
+              DUn[m] = __ldcg(A.DU + m * tc + cn);
+            }
+            Lcn = A.Lc[d * tc + cn];
+            Lvn = A.Lv[d * tc + cn];
+          }
+          double DF[NV];
+          comput_DFn(NV, DF, Un, DUn, cur.n[d][0], cur.n[d][1], cur.n[d][2], gamma);
+#pragma unroll
+          for (int m = 0; m < NV; m++) {
+            double v;
+            if (!UPPER) v = 0.5 * (DF[m] * cur.S[d] + w * Lcn * DUn[m]);
+            else v = -(0.5 * (DF[m] * cur.S[d] - w * Lcn * DUn[m]));
+            if (visc) v = v + Lvn * DUn[m];
+            acc[d][m] = v;
+          }
+        }
+        const long long c = cix(B, i, j, k);
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          double r;
+          if (!UPPER) r = (cur.R[m] + acc[0][m] + acc[1][m] + acc[2][m]) / alfa[m];
+          else r = cur.R[m] + (acc[0][m] + acc[1][m] + acc[2][m]) / alfa[m];
+          A.DU[m * tc + c] = r;
+          out.DU[m] = r;
+          out.U[m] = cur.U[m];
+          prevU[m] = cur.U[m];
+          prevDU[m] = r;
+        }
+        out.Lcj = cur.Lc[1]; out.Lck = cur.Lc[2]; out.Lvj = cur.Lv[1]; out.Lvk = cur.Lv[2];
+        prevLci = cur.Lc[0];
+        prevLvi = cur.Lv[0];
+        s_out[t & 1][lt] = out;
+      }
+      __syncthreads();
+      if (lt == 0) st_release(L.progress + my, t + 1);
+      cur = nxt;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace ocfd

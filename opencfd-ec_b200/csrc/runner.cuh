@@ -1,5 +1,6 @@
 // Kernel sequencing of one time step, templated on the flux precision T and NVAR.
 #pragma once
+#include "lusgs.cuh"
 #include "runner.h"
 #include "solver.cuh"
 
@@ -31,7 +32,9 @@ __global__ void k_gather_state(Arena<T> A, int b, double* aos, long long box_b) 
 template <class T, int NV>
 class RunnerT : public Runner {
  public:
-  RunnerT(const Arena<T>& A, const RunInfo& I) : A_(A), I_(I) {}
+  RunnerT(const Arena<T>& A, const RunInfo& I) : A_(A), I_(I) {
+    if (I.lu) L_ = *I.lu;
+  }
 
   void residual(cudaStream_t st, bool lusgs) override {
     const Arena<T>& A = A_;
@@ -74,9 +77,26 @@ class RunnerT : public Runner {
     }
     k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
     if (lusgs) {
+      lusgs_sweep(st, false);
+      lusgs_sweep(st, true);
+    }
+  }
+
+  void lusgs_sweep(cudaStream_t st, bool upper) {
+    const Arena<T>& A = A_;
+    if (I_.lu_planes) {
       int gc = grid_of(A.tot_col, 128);
-      for (int p = 3; p <= I_.max_plane; p++) k_lusgs<T, NV, false><<<gc, 128, 0, st>>>(A, p);
-      for (int p = I_.max_plane; p >= 3; p--) k_lusgs<T, NV, true><<<gc, 128, 0, st>>>(A, p);
+      if (!upper) for (int p = 3; p <= I_.max_plane; p++) k_lusgs<T, NV, false><<<gc, 128, 0, st>>>(A, p);
+      else for (int p = I_.max_plane; p >= 3; p--) k_lusgs<T, NV, true><<<gc, 128, 0, st>>>(A, p);
+    } else {
+      if (!upper) {
+        cudaMemsetAsync(L_.counter, 0, 2 * sizeof(int), st);
+        cudaMemsetAsync(L_.progress, 0, sizeof(int) * L_.ntiles, st);
+        k_lusgs_wave<T, NV, false><<<I_.lu_grid, 64, 0, st>>>(A, L_);
+      } else {
+        cudaMemsetAsync(L_.progress, 0, sizeof(int) * L_.ntiles, st);
+        k_lusgs_wave<T, NV, true><<<I_.lu_grid, 64, 0, st>>>(A, L_);
+      }
     }
   }
 
@@ -97,13 +117,16 @@ class RunnerT : public Runner {
     }
   }
 
-  void step(cudaStream_t st) override {
+  void step(cudaStream_t st, cudaEvent_t* ev = nullptr) override {
     const Arena<T>& A = A_;
+    auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
+    rec(0);
     if (I_.time_method == 0) {
-      residual(st, true);
+      residual_phases(st, ev);
       cudaMemsetAsync(A.flags + A.nblk, 0, sizeof(int) * 2 * A.nblk, st);
       k_update<T, NV, 0><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
       limit(st);
+      rec(4);
       bc_halo(st);
     } else {
       k_copy_un<T, NV><<<grid_of((long long)NV * A.tot_box), 256, 0, st>>>(A);
@@ -116,8 +139,36 @@ class RunnerT : public Runner {
         limit(st);
         bc_halo(st);
       }
+      rec(1); rec(2); rec(3); rec(4);
     }
     if (NV >= 6) k_vtkw<T, NV><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+    rec(5);
+  }
+
+  // residual + LU-SGS with phase events (LU-SGS path)
+  void residual_phases(cudaStream_t st, cudaEvent_t* ev) {
+    residual(st, false);
+    if (ev) cudaEventRecord(ev[1], st);
+    lusgs_sweep(st, false);
+    if (ev) cudaEventRecord(ev[2], st);
+    lusgs_sweep(st, true);
+    if (ev) cudaEventRecord(ev[3], st);
+  }
+  int launches_per_step() const override {
+    int res = 1 + 4 /*inviscid*/ + 1 /*assemble*/;
+    if (I_.viscous) {
+      res += 1 + 3 + 1;  // mu, viscous fluxes, amut
+      if (I_.turb == 2) res += 6;
+      else if (I_.turb == 3) res += 11;
+    }
+    int lu = I_.lu_planes ? 2 * (I_.max_plane - 2) : 2;
+    int upd = 1 + 1 + (NV == 6 ? 3 : 0);
+    int bch = 2 + (A_.tot_halo > 0 ? 1 : 0);
+    int n;
+    if (I_.time_method == 0) n = res + lu + upd + bch;
+    else n = 1 + 3 * (res + upd + bch);
+    if (NV >= 6) n += 1;
+    return n;
   }
 
   void init_flow(cudaStream_t st) override {
@@ -144,6 +195,7 @@ class RunnerT : public Runner {
  private:
   Arena<T> A_;
   RunInfo I_;
+  LuArgs L_{};
 };
 
 template <class T>

@@ -7,17 +7,25 @@
 
 namespace ocfd {
 
+struct LuArgs;
+
 struct RunInfo {
   int nvar, time_method, viscous, turb;
   int max_plane;          // max over blocks of nx+ny+nz-3 (last LU-SGS hyperplane)
   int ncchunk, nwchunk;   // reduction chunk counts
+  int lu_planes;          // 1: one launch per hyperplane (reference order); 0: pipelined wavefront
+  const LuArgs* lu;       // wavefront tables (host copy of the kernel argument)
+  int lu_grid;            // CTAs of the wavefront kernel
 };
 
 class Runner {
  public:
   virtual ~Runner() {}
-  // one NS_Time_advance (sub_time_advance.f90:6-23) on stream st
-  virtual void step(cudaStream_t st) = 0;
+  // one NS_Time_advance (sub_time_advance.f90:6-23) on stream st; when ev is non-null, events
+  // ev[0..5] are recorded at the phase boundaries (see ocfd_profile)
+  virtual void step(cudaStream_t st, cudaEvent_t* ev = nullptr) = 0;
+  // kernel launches of one step
+  virtual int launches_per_step() const = 0;
   // residual only (Comput_Residual_one_mesh without LU-SGS), for parity checks
   virtual void residual(cudaStream_t st, bool lusgs) = 0;
   // freestream + BC + halo + corners (init_flow_zero, sub_init.f90:302-410)

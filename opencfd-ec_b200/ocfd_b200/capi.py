@@ -19,6 +19,7 @@ EXPORTED = [
     "ocfd_default_params", "ocfd_finalize_params", "ocfd_create", "ocfd_destroy", "ocfd_last_error", "ocfd_state_size",
     "ocfd_set_state", "ocfd_get_state", "ocfd_init_flow", "ocfd_advance", "ocfd_residual", "ocfd_forces",
     "ocfd_limiter_status", "ocfd_array_shape", "ocfd_get_array", "ocfd_version", "ocfd_compute_residual",
+    "ocfd_stream", "ocfd_profile", "ocfd_launches_per_step",
 ]
 
 
@@ -55,6 +56,10 @@ def lib():
         L.ocfd_array_shape.argtypes = [vp, ctypes.c_int, cp, ip, ip, ip]
         L.ocfd_get_array.argtypes = [vp, ctypes.c_int, cp, dp]
         L.ocfd_version.restype = cp
+        L.ocfd_stream.argtypes = [vp]
+        L.ocfd_stream.restype = vp
+        L.ocfd_profile.argtypes = [vp, ctypes.c_int, dp]
+        L.ocfd_launches_per_step.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -156,6 +161,22 @@ class Solver:
         out = np.empty(shape)
         self._check(lib().ocfd_get_array(self.h, b, name.encode(), _dp(out)), "get_array " + name)
         return out, tuple(lo), tuple(hi)
+
+
+    def stream(self):
+        """cudaStream_t (int) all of this handle's work is queued on."""
+        return lib().ocfd_stream(self.h)
+
+    PHASES = ("residual", "lusgs_lower", "lusgs_upper", "update_limit", "bc_halo", "step")
+
+    def profile(self, nsteps=3):
+        """Per-phase device ms accumulated over nsteps steps (dict)."""
+        ms = np.zeros(8)
+        self._check(lib().ocfd_profile(self.h, nsteps, _dp(ms)), "profile")
+        return dict(zip(self.PHASES, ms[:6].tolist()))
+
+    def launches_per_step(self):
+        return int(lib().ocfd_launches_per_step(self.h))
 
 
 def version():

@@ -501,6 +501,7 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
     h->lu.tiles = d_tiles; h->lu.ntiles = first; h->lu.counter = d_counter; h->lu.progress = d_progress;
     h->lu.tile_of = d_tile_of; h->lu.err = h->d_lu_err; h->lu.TJ = TJ; h->lu.TK = TK;
     h->lu.spin_limit = 4000000;  // x ~64 ns: a few hundred ms before a stuck wait gives up
+    if (const char* s = std::getenv("OCFD_LU_SPIN_LIMIT")) h->lu.spin_limit = std::max(0LL, std::atoll(s));
   }
   // ---- runner
   RunInfo I;
@@ -646,7 +647,10 @@ extern "C" int ocfd_residual(ocfd_handle* h, double* rmax, double* rrms) {
   }
   int lu_err = 0;
   cudaMemcpy(&lu_err, h->d_lu_err, 4, cudaMemcpyDeviceToHost);
-  if (lu_err) return fail(h, OCFD_ERR_TIMEOUT, "LU-SGS wavefront: a bounded wait between tiles timed out");
+  if (lu_err) {
+    cudaMemset(h->d_lu_err, 0, 4);
+    return fail(h, OCFD_ERR_TIMEOUT, "LU-SGS wavefront: a bounded wait between tiles timed out");
+  }
   if (nan_at != ~0ULL) {
     long long g = (long long)(nan_at / 8);
     int m = (int)(nan_at % 8);

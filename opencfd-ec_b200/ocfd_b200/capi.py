@@ -135,6 +135,8 @@ class Solver:
         return ft, cl.value, cd.value, cs.value
 
     def state_shape(self, b):
+        if not 0 <= b < self.nblk:
+            raise OcfdError(OCFD_ERR_ARG, "block %d out of range (%d blocks)" % (b, self.nblk))
         nx, ny, nz = self.case.dims[b]
         return (nz + 7, ny + 7, nx + 7, self.nvar)
 

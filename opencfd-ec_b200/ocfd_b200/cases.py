@@ -32,6 +32,12 @@ def config2(ni=257, nj=97, nk_wing=61, nk_tip=26, i_cut=49, **over):
     return make_params(**raw), case
 
 
+def config2_medium(**over):
+    """The swept wing at a quarter of the cells (~0.5 M, ~0.6 GB on the device): larger than L2,
+    small enough for multi-pass profiler captures."""
+    return config2(ni=129, nj=97, nk_wing=31, nk_tip=14, i_cut=25, **over)
+
+
 def config2_small(**over):
     """A reduced swept wing (8 blocks) for oracle parity."""
     return config2(ni=41, nj=17, nk_wing=9, nk_tip=6, i_cut=9, **over)

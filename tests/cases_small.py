@@ -1,0 +1,27 @@
+"""Small parity cases: every scheme, flux, turbulence model and time method the hot path has,
+on meshes the CPU oracle advances in well under a second per step."""
+from ocfd_b200 import cases
+
+SST_INF = dict(kt_inf=1e-8, wt_inf=1e-5)   # CFL3D-nondimensional k, omega far-field values
+
+
+def small_cases():
+    return {
+        "bump1": lambda: cases.config1(scale=0.25),
+        "bump2": lambda: cases.config1(scale=0.25, cuts_i=(12,)),
+        "foil_sa_weno5_roe": lambda: cases.airfoil(ni=65, nj=17, scheme=7, flux=4),
+        "foil_sa_muscl3_ausmpw": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=6),
+        "foil_lam_rk3_hllc": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=3, turb=0, time_method=3, cfl=1.0),
+        "foil_sst_lusgs_hllc": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=3, turb=3, **SST_INF),
+        "foil_sst_rk3_hllc": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=3, turb=3, time_method=3, cfl=1.5, **SST_INF),
+        "foil_sa_muscl2c_vl": lambda: cases.airfoil(ni=65, nj=17, scheme=4, flux=5, turb=2),
+        "foil_sa_weno7_sw": lambda: cases.airfoil(ni=65, nj=17, scheme=9, flux=1, turb=2),
+        "foil_sa_char_hll": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=2, turb=2, iflag_reconstruction=2),
+        "foil_sa_cons_omuscl2_roe": lambda: cases.airfoil(ni=65, nj=17, scheme=6, flux=4, turb=2, iflag_reconstruction=1),
+        "wing8": lambda: cases.config2_small(),
+    }
+
+
+# the subset whose golden fixtures are committed (tests/golden/)
+GOLDEN_CASES = ("bump2", "foil_sa_weno5_roe", "foil_lam_rk3_hllc", "foil_sst_lusgs_hllc", "wing8")
+GOLDEN_STEPS = 5

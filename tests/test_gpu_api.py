@@ -1,0 +1,114 @@
+"""C-ABI behaviour on the GPU: state round trips, re-initialisation, error codes, NaN reporting
+and the bounded LU-SGS waits (a wait that runs out returns OCFD_ERR_TIMEOUT, the context stays
+usable)."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def small():
+    from ocfd_b200 import cases
+    return cases.config1(scale=0.25, cuts_i=(12,))
+
+
+def test_state_roundtrip_and_init_flow(gpu):
+    p, case = small()
+    g = gpu.Solver(p, case)
+    U0 = [g.get_state(b) for b in range(g.nblk)]
+    g.advance(3)
+    U3 = [g.get_state(b) for b in range(g.nblk)]
+    assert any(not np.array_equal(a, b) for a, b in zip(U0, U3))
+    for b in range(g.nblk):
+        g.set_state(b, U3[b])
+        assert np.array_equal(g.get_state(b), U3[b])
+    g.init_flow()
+    for b in range(g.nblk):
+        assert np.array_equal(g.get_state(b), U0[b])
+    g.close()
+
+
+def test_set_state_restart_reproduces_run(gpu):
+    """Restart semantics: state written back after k steps continues exactly like the live run."""
+    p, case = small()
+    a, b = gpu.Solver(p, case), gpu.Solver(p, case)
+    a.advance(3)
+    for blk in range(a.nblk):
+        b.set_state(blk, a.get_state(blk))
+    a.advance(2)
+    b.advance(2)
+    assert np.array_equal(a.residual()[1], b.residual()[1])
+    a.close()
+    b.close()
+
+
+def test_bad_arguments(gpu):
+    p, case = small()
+    g = gpu.Solver(p, case)
+    with pytest.raises(gpu.OcfdError) as e:
+        g.get_state(7)
+    assert e.value.code == gpu.OCFD_ERR_ARG
+    with pytest.raises(gpu.OcfdError):
+        g.get_array(0, "no_such_array")
+    g.close()
+
+
+def test_nan_reported_with_location(gpu):
+    """A NaN in the state is reported by ocfd_residual as OCFD_ERR_NAN with block and cell,
+    replacing the reference's stop (sub_time_advance.f90:358-365)."""
+    p, case = small()
+    g = gpu.Solver(p, case)
+    U = g.get_state(1)
+    U[3 + 2, 3 + 5, 3 + 7, 0] = np.nan      # block 2, cell (i,j,k) = (7,5,2), density
+    g.set_state(1, U)
+    g.compute_residual(False)
+    with pytest.raises(FloatingPointError) as e:
+        g.residual()
+    assert "block 2" in str(e.value)
+    g.close()
+
+
+def test_lusgs_wait_bound_reports_timeout(gpu, oracle):
+    """With the LU-SGS wait bound at zero every cross-tile wait that is not already satisfied gives
+    up at once: the sweep finishes, the step reports OCFD_ERR_TIMEOUT, and a new handle on the
+    same context runs correctly."""
+    from ocfd_b200 import cases
+    p, case = cases.config2_small()
+    os.environ["OCFD_LU_SPIN_LIMIT"] = "0"
+    try:
+        g = gpu.Solver(p, case)
+    finally:
+        os.environ.pop("OCFD_LU_SPIN_LIMIT", None)
+    seen = False
+    for _ in range(3):
+        g.advance(1)
+        try:
+            g.residual()
+        except gpu.OcfdError as e:
+            assert e.code == gpu.OCFD_ERR_TIMEOUT
+            seen = True
+            break
+        except FloatingPointError:
+            seen = True   # stale neighbour data may also have produced a NaN first
+            break
+    g.close()
+    assert seen
+    h = gpu.Solver(p, case)
+    o = oracle.OracleCase(p, case)
+    h.advance(2)
+    o.advance(2)
+    np.testing.assert_allclose(h.residual()[1][:6], o.residual()[1][:6], rtol=1e-11)
+    h.close()
+    o.close()
+
+
+def test_profile_and_launch_count(gpu):
+    p, case = small()
+    g = gpu.Solver(p, case)
+    ph = g.profile(2)
+    assert set(ph) == set(g.PHASES) and all(v >= 0.0 for v in ph.values()) and ph["step"] > 0.0
+    assert 5 <= g.launches_per_step() <= 64
+    assert g.stream()
+    g.close()

@@ -51,8 +51,11 @@ class Pool {
   void set_threads(int n) {
     stop();
     if (n < 1) n = 1;
+    std::unique_lock<std::mutex> lk(m_);
     quit_ = false;
-    for (int t = 1; t < n; t++) workers_.emplace_back([this, t] { loop(t); });
+    // a worker starts at the current generation, so it only ever takes part in later runs
+    const unsigned g0 = gen_;
+    for (int t = 1; t < n; t++) workers_.emplace_back([this, t, g0] { loop(t, g0); });
   }
   template <class F>
   void run(int lo, int hi, F&& f) {
@@ -88,8 +91,7 @@ class Pool {
     for (auto& w : workers_) w.join();
     workers_.clear();
   }
-  void loop(int tid) {
-    unsigned seen = 0;
+  void loop(int tid, unsigned seen) {
     for (;;) {
       std::function<void(int)>* job;
       {
@@ -99,7 +101,8 @@ class Pool {
         if (quit_) return;
         job = job_;
       }
-      if (job) (*job)(tid);
+      if (!job) continue;
+      (*job)(tid);
       std::unique_lock<std::mutex> lk(m_);
       if (--pending_ == 0) done_.notify_one();
     }

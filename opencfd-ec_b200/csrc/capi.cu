@@ -471,12 +471,18 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
     convert_to_float(h->d_dwd, h->d_dwf, tc, h->st);
   }
   if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "geometry sync"); }
-  // ---- LU-SGS wavefront tiles: TJ x TK columns per CTA (64 threads), ordered by J+K
+  // ---- LU-SGS wavefront tiles: TJ x TK = TC columns per CTA, ordered by J+K
+  //      (version 3: 4*TC threads per CTA, TC = 32 by default; version 2: 64 threads, TC = 64)
+  const int lu_v2 = std::getenv("OCFD_LU_V2") ? 1 : 0;
+  int lu_tc = 32;
+  if (const char* e2 = std::getenv("OCFD_LU_TC")) lu_tc = std::atoi(e2) == 64 ? 64 : 32;
+  if (lu_v2) lu_tc = 64;
   {
     int min_nzm = 1 << 30;
     for (const BlkD& B : h->blk) min_nzm = std::min(min_nzm, B.nz - 1);
     int TK = min_nzm <= 2 ? 2 : (min_nzm <= 4 ? 4 : 8);
-    int TJ = 64 / TK;
+    if (lu_tc == 32 && TK == 8) TK = 4;
+    int TJ = lu_tc / TK;
     std::vector<int> tile_of(3 * nblk);
     std::vector<std::pair<int, LuTile>> order;
     int first = 0;
@@ -508,6 +514,8 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
   I.nvar = NV; I.time_method = p->time_method; I.viscous = p->if_viscous; I.turb = turb; I.max_plane = h->max_plane;
   I.ncchunk = (int)h->cchunk.size(); I.nwchunk = (int)h->wchunk.size();
   I.lu_planes = std::getenv("OCFD_LUSGS_PLANES") ? 1 : 0;
+  I.lu_version = lu_v2 ? 2 : 3;
+  I.lu_tc = lu_tc;
   I.lu = &h->lu;
   {
     int dev = 0, nsm = 148;

@@ -246,4 +246,255 @@ __global__ void __launch_bounds__(64) k_lusgs_wave(Arena<T> A, LuArgs L) {
   }
 }
 
+
+// ============================================================================================
+// Version 3: the work of one column split over four thread groups of TC threads each.
+//
+//   group d = 0, 1, 2 ("direction threads"): the flux-difference term of the upstream neighbour
+//                   in direction d (i, j, k): DF = F(U+DU)n - F(U)n, times S, plus the spectral
+//                   radius terms; the old-state half F(U)n is computed a step ahead, so only the
+//                   DU-dependent half sits on the dependency chain;
+//   group 3       ("owner"): sums Res + the three terms in the reference's order, divides by
+//                   the diagonal, writes DU and publishes (DU, p(U+DU)) for the downstream cells.
+//
+// Per step: barrier B1, direction threads compute their terms into shared memory while owners
+// load the next cell; barrier B2, owners finish the cell while direction threads prepare the
+// next step (old-state terms from prefetched data) and one thread polls the upstream tiles'
+// progress.  Every cell still evaluates the reference expression with the same operands in the
+// same order, so the bits equal the hyperplane order.
+// ============================================================================================
+template <int NV>
+struct LuDir {      // direction-thread data of one step (old state only)
+  double n1, n2, n3, S;
+  double Unb[NV];   // neighbour state (U6/U7 clamped as limit_vt leaves them)
+  double wLc, Lv;   // w * Lc and Lv of the neighbour in this direction
+};
+
+template <int NV>
+struct LuOwn {      // owner data of one step
+  double U[NV], R[NV];
+  double vol, dt, Lc[3], Lv[3];
+};
+
+__device__ __forceinline__ double ldro(const double* p) { return __ldg(p); }
+// CTA-wide barrier on a named barrier (warp-uniform callers; the owner and direction warps
+// reach it from different loops, each warp executing the same instruction in all its lanes)
+template <int NT>
+__device__ __forceinline__ void cta_bar() { asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory"); }
+__device__ __forceinline__ double ldro(const float* p) { return (double)__ldg(p); }
+
+template <class T, int NV, bool UPPER, int TC>
+__global__ void __launch_bounds__(4 * TC, 128 / TC) k_lusgs_wave3(Arena<T> A, LuArgs L) {
+  __shared__ int s_tile;
+  __shared__ double s_acc[3][NV][TC];    // direction terms of the current step
+  __shared__ double s_pub[NV + 1][TC];   // DU and p(U+DU) of each column's last cell
+  const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
+  const int TJ = L.TJ, TK = L.TK;
+  const int tid = threadIdx.x, grp = tid / TC, c = tid % TC;
+  const int lj = c % TJ, lk = c / TJ;
+  const bool owner = grp == 3;
+  const int d = grp;  // direction of a direction thread
+  for (;;) {
+    if (tid == 0) s_tile = atomicAdd(&L.counter[UPPER ? 1 : 0], 1);
+    __syncthreads();
+    const int q = s_tile;
+    if (q >= L.ntiles) break;
+    const LuTile tl = L.tiles[UPPER ? (L.ntiles - 1 - q) : q];
+    const BlkD& B = A.blk[tl.blk];
+    const SolveP& s = A.sp[B.solve];
+    const int nxm = B.nx - 1, nym = B.ny - 1, nzm = B.nz - 1;
+    const int j = UPPER ? (tl.j0 + TJ - 1 - lj) : (tl.j0 + lj);
+    const int k = UPPER ? (tl.k0 + TK - 1 - lk) : (tl.k0 + lk);
+    const bool active = j >= 1 && j <= nym && k >= 1 && k <= nzm;
+    const int* tb3 = L.tile_of + 3 * tl.blk;
+    const int first = tb3[0], nJ = tb3[1], nK = tb3[2];
+    const int J = (tl.j0 - 1) / TJ, K = (tl.k0 - 1) / TK;
+    int pj = -1, pk = -1;
+    if (!UPPER) {
+      if (J > 0) pj = first + (J - 1) + nJ * K;
+      if (K > 0) pk = first + J + nJ * (K - 1);
+    } else {
+      if (J < nJ - 1) pj = first + (J + 1) + nJ * K;
+      if (K < nK - 1) pk = first + J + nJ * (K + 1);
+    }
+    const int my = first + J + nJ * K;
+    const int nsteps = nxm + TJ + TK - 2;
+    const double w = s.w_lu, gamma = s.gamma;
+    const bool visc = s.viscous == 1;
+    const int off = UPPER ? 1 : -1;
+    auto i_of = [&](int t) { int il = t - lj - lk; return UPPER ? (nxm - il) : (il + 1); };
+    auto on_at = [&](int t) { int il = t - lj - lk; return active && il >= 0 && il < nxm; };
+    // does the cell of step t have an upstream neighbour in direction d inside the block?
+    auto has_at = [&](int t) {
+      const int i = i_of(t);
+      return UPPER ? (d == 0 ? i != nxm : (d == 1 ? j != nym : k != nzm)) : (d == 0 ? i != 1 : (d == 1 ? j != 1 : k != 1));
+    };
+    // a neighbour column in another tile: its DU comes through L2 after the progress wait
+    const bool xt = !owner && ((d == 1 && lj == 0) || (d == 2 && lk == 0));
+    const int pubcol = d == 0 ? c : (d == 1 ? c - 1 : c - TJ);
+
+    LuDir<NV> dn;  // prefetched direction data (raw) for the next step
+    LuOwn<NV> on;  // prefetched owner data (raw) for the next step
+    auto load_dir = [&](int t, LuDir<NV>& x) {
+      const int i = i_of(t);
+      const long long f = fix_(B, i, j, k);
+      x.n1 = ldro(A.M + (M_NI1 + 3 * d) * tf + f);
+      x.n2 = ldro(A.M + (M_NI2 + 3 * d) * tf + f);
+      x.n3 = ldro(A.M + (M_NI3 + 3 * d) * tf + f);
+      // the lower face's area (lower sweep) or the upper face's (upper sweep, sub_LU_SGS.f90:96-97)
+      const long long fs = UPPER ? fix_(B, i + (d == 0), j + (d == 1), k + (d == 2)) : f;
+      x.S = ldro(A.M + (M_SI + d) * tf + fs);
+      const int ii = i + (d == 0 ? off : 0), jj = j + (d == 1 ? off : 0), kk = k + (d == 2 ? off : 0);
+      const long long bn = bix(B, ii, jj, kk), cn = cix(B, ii, jj, kk);
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        double u = __ldg(A.U + m * tb + bn);
+        x.Unb[m] = m >= 5 ? clamp0(u) : u;
+      }
+      x.wLc = ldro(A.Lc + d * tc + cn);
+      x.Lv = ldro(A.Lv + d * tc + cn);
+    };
+    auto load_own = [&](int t, LuOwn<NV>& x) {
+      const int i = i_of(t);
+      const long long bi = bix(B, i, j, k), ci = cix(B, i, j, k);
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        double u = __ldg(A.U + m * tb + bi);
+        x.U[m] = m >= 5 ? clamp0(u) : u;
+        // upper sweep: R is DU* of the lower sweep, read before this thread overwrites it
+        x.R[m] = UPPER ? A.DU[m * tc + ci] : ldro(A.Res + m * tc + ci);
+      }
+      x.vol = __ldg(A.vold + ci);
+      x.dt = ldro(A.dt + ci);
+#pragma unroll
+      for (int q2 = 0; q2 < 3; q2++) { x.Lc[q2] = ldro(A.Lc + q2 * tc + ci); x.Lv[q2] = ldro(A.Lv + q2 * tc + ci); }
+    };
+
+    // direction thread state for the current step: old-state half of the flux difference
+    double un1 = 0.0, F1[NV], n1 = 0.0, n2 = 0.0, n3 = 0.0, S = 0.0, wLc = 0.0, Lvn = 0.0, Unb[NV];
+    bool has = false;
+    auto prep_dir = [&](int t, const LuDir<NV>& x) {  // comput_DFn's U terms (sub_LU_SGS.f90:135-157)
+      has = on_at(t) && has_at(t);
+      n1 = x.n1; n2 = x.n2; n3 = x.n3; S = x.S; Lvn = x.Lv;
+      wLc = w * x.wLc;
+#pragma unroll
+      for (int m = 0; m < NV; m++) Unb[m] = x.Unb[m];
+      if (!has) return;
+      un1 = (Unb[1] * n1 + Unb[2] * n2 + Unb[3] * n3) / Unb[0];
+      const double p1 = (gamma - 1.0) * (Unb[4] - 0.5 * (sq(Unb[1]) + sq(Unb[2]) + sq(Unb[3])) / Unb[0]);
+      F1[0] = Unb[0] * un1;
+      F1[1] = Unb[1] * un1 + p1 * n1;
+      F1[2] = Unb[2] * un1 + p1 * n2;
+      F1[3] = Unb[3] * un1 + p1 * n3;
+      F1[4] = (Unb[4] + p1) * un1;
+#pragma unroll
+      for (int m = 5; m < NV; m++) F1[m] = Unb[m] * un1;
+    };
+    // owner state for the current step
+    double oU[NV], oR[NV], alfa[NV];
+    auto prep_own = [&](const LuOwn<NV>& x) {  // diagonal (sub_LU_SGS.f90:50-62, 90-92)
+      const double a0 = x.vol / x.dt + w * (x.Lc[0] + x.Lc[1] + x.Lc[2]);
+#pragma unroll
+      for (int m = 0; m < NV; m++) { alfa[m] = a0; oU[m] = x.U[m]; oR[m] = x.R[m]; }
+      if (visc) {
+        const double lv = x.Lv[0] + x.Lv[1] + x.Lv[2];
+#pragma unroll
+        for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + 2.0 * lv;
+        if (NV == 6) {
+          if (!UPPER) alfa[5] = alfa[5] + lv;
+          else alfa[5] = alfa[5] + x.Lv[0] + x.Lv[1] + x.Lv[2];
+        }
+      }
+    };
+
+    int seen_j = 0, seen_k = 0;
+    auto poll = [&](int t) {  // upstream tiles far enough for step t
+      bool ok = true;
+      if (pj >= 0 && seen_j < min(t + TJ, nsteps)) ok &= wait_ge(L.progress + pj, min(t + TJ, nsteps), L.spin_limit, seen_j);
+      if (pk >= 0 && seen_k < min(t + TK, nsteps)) ok &= wait_ge(L.progress + pk, min(t + TK, nsteps), L.spin_limit, seen_k);
+      if (!ok) atomicExch(L.err, 1);
+    };
+
+    // The owner warps and the direction warps run separate loops (so each keeps only its own
+    // registers live); both take the same two CTA barriers per step.
+    if (owner) {
+      if (on_at(0)) { load_own(0, on); prep_own(on); }
+      for (int t = 0; t < nsteps; t++) {
+        cta_bar<4 * TC>();  // B1
+        if (on_at(t + 1)) load_own(t + 1, on);
+        cta_bar<4 * TC>();  // B2: the three direction terms of step t are in shared memory
+        if (on_at(t)) {
+          const long long ci = cix(B, i_of(t), j, k);
+          double U2[5];
+#pragma unroll
+          for (int m = 0; m < NV; m++) {
+            double r;
+            if (!UPPER) r = (oR[m] + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / alfa[m];
+            else r = oR[m] + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / alfa[m];
+            A.DU[m * tc + ci] = r;
+            s_pub[m][c] = r;
+            if (m < 5) U2[m] = oU[m] + r;
+          }
+          s_pub[NV][c] = (gamma - 1.0) * (U2[4] - 0.5 * (sq(U2[1]) + sq(U2[2]) + sq(U2[3])) / U2[0]);
+        }
+        if (on_at(t + 1)) prep_own(on);
+      }
+    } else {
+      if (on_at(0) && has_at(0)) load_dir(0, dn);
+      prep_dir(0, dn);
+      if (tid == 0) poll(0);
+      for (int t = 0; t < nsteps; t++) {
+        cta_bar<4 * TC>();  // B1: step t-1 finished (DU in s_pub and in HBM), upstream tiles ready
+        if (tid == 0 && t > 0) st_release(L.progress + my, t);
+        if (on_at(t + 1) && has_at(t + 1)) load_dir(t + 1, dn);
+        if (has) {
+          double DUn[NV], pp2;
+          if (!xt) {
+#pragma unroll
+            for (int m = 0; m < NV; m++) DUn[m] = s_pub[m][pubcol];
+            pp2 = s_pub[NV][pubcol];
+          } else {
+            const int i = i_of(t);
+            const long long cn = cix(B, i, j + (d == 1 ? off : 0), k + (d == 2 ? off : 0));
+#pragma unroll
+            for (int m = 0; m < NV; m++) DUn[m] = __ldcg(A.DU + m * tc + cn);
+            double V2[5];
+#pragma unroll
+            for (int m = 0; m < 5; m++) V2[m] = Unb[m] + DUn[m];
+            pp2 = (gamma - 1.0) * (V2[4] - 0.5 * (sq(V2[1]) + sq(V2[2]) + sq(V2[3])) / V2[0]);
+          }
+          double U2[NV];
+#pragma unroll
+          for (int m = 0; m < NV; m++) U2[m] = Unb[m] + DUn[m];
+          const double un2 = (U2[1] * n1 + U2[2] * n2 + U2[3] * n3) / U2[0];
+          double DF[NV];
+          DF[0] = U2[0] * un2 - F1[0];
+          DF[1] = (U2[1] * un2 + pp2 * n1) - F1[1];
+          DF[2] = (U2[2] * un2 + pp2 * n2) - F1[2];
+          DF[3] = (U2[3] * un2 + pp2 * n3) - F1[3];
+          DF[4] = (U2[4] + pp2) * un2 - F1[4];
+#pragma unroll
+          for (int m = 5; m < NV; m++) DF[m] = U2[m] * un2 - F1[m];
+#pragma unroll
+          for (int m = 0; m < NV; m++) {
+            double v;
+            if (!UPPER) v = 0.5 * (DF[m] * S + wLc * DUn[m]);
+            else v = -(0.5 * (DF[m] * S - wLc * DUn[m]));
+            if (visc) v = v + Lvn * DUn[m];
+            s_acc[d][m][c] = v;
+          }
+        } else if (on_at(t)) {
+#pragma unroll
+          for (int m = 0; m < NV; m++) s_acc[d][m][c] = 0.0;
+        }
+        cta_bar<4 * TC>();  // B2
+        prep_dir(t + 1, dn);
+        if (tid == 0 && t + 1 < nsteps) poll(t + 1);
+      }
+    }
+    __syncthreads();
+    if (tid == 0) st_release(L.progress + my, nsteps);
+  }
+}
+
 }  // namespace ocfd

@@ -89,13 +89,17 @@ class RunnerT : public Runner {
       if (!upper) for (int p = 3; p <= I_.max_plane; p++) k_lusgs<T, NV, false><<<gc, 128, 0, st>>>(A, p);
       else for (int p = I_.max_plane; p >= 3; p--) k_lusgs<T, NV, true><<<gc, 128, 0, st>>>(A, p);
     } else {
-      if (!upper) {
-        cudaMemsetAsync(L_.counter, 0, 2 * sizeof(int), st);
-        cudaMemsetAsync(L_.progress, 0, sizeof(int) * L_.ntiles, st);
-        k_lusgs_wave<T, NV, false><<<I_.lu_grid, 64, 0, st>>>(A, L_);
+      if (!upper) cudaMemsetAsync(L_.counter, 0, 2 * sizeof(int), st);
+      cudaMemsetAsync(L_.progress, 0, sizeof(int) * L_.ntiles, st);
+      if (I_.lu_version == 2) {
+        if (!upper) k_lusgs_wave<T, NV, false><<<I_.lu_grid, 64, 0, st>>>(A, L_);
+        else k_lusgs_wave<T, NV, true><<<I_.lu_grid, 64, 0, st>>>(A, L_);
+      } else if (I_.lu_tc == 64) {
+        if (!upper) k_lusgs_wave3<T, NV, false, 64><<<I_.lu_grid, 256, 0, st>>>(A, L_);
+        else k_lusgs_wave3<T, NV, true, 64><<<I_.lu_grid, 256, 0, st>>>(A, L_);
       } else {
-        cudaMemsetAsync(L_.progress, 0, sizeof(int) * L_.ntiles, st);
-        k_lusgs_wave<T, NV, true><<<I_.lu_grid, 64, 0, st>>>(A, L_);
+        if (!upper) k_lusgs_wave3<T, NV, false, 32><<<I_.lu_grid, 128, 0, st>>>(A, L_);
+        else k_lusgs_wave3<T, NV, true, 32><<<I_.lu_grid, 128, 0, st>>>(A, L_);
       }
     }
   }

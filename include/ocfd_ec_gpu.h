@@ -189,6 +189,40 @@ int ocfd_limiter_status(ocfd_handle* h, int blk, int* n_limited, int* overlimit)
 int ocfd_array_shape(const ocfd_handle* h, int blk, const char* name, int* lo, int* hi, int* nv);
 int ocfd_get_array(ocfd_handle* h, int blk, const char* name, double* out);
 
+/* ---- batches of independent solves (no counterpart in the reference, which runs one case per
+ *      MPI job; the batched form serves Mach/AoA sweeps and many meshes at once) ------------ */
+
+/*
+ * One handle holding nsolve independent cases: every kernel of a step covers the blocks of all
+ * of them, so a step of the batch is one graph launch of the same kernels as a single case.
+ *   ps[q]       parameters of solve q; all solves share NVAR (turbulence model), if_viscous,
+ *               time_method and precision (OCFD_ERR_ARG otherwise); Mach, angles, Re, CFL,
+ *               schemes, fluxes and limits may differ
+ *   nblk[q]     blocks of solve q; blocks are numbered globally in solve order for every other
+ *               argument and entry point (nijk, xyz, nsub, inc, dw, set/get_state, ...)
+ *   inc         partner block numbers (nb1) are 1-based WITHIN the solve, exactly as each
+ *               case's own .inc file has them
+ * Wall distance is taken over the walls of each block's own solve.  ocfd_create is this call
+ * with nsolve = 1.
+ */
+int ocfd_create_batch(const ocfd_params* ps, int nsolve, const int* nblk, const int* nijk,
+                      const double* const* xyz, const int* nsub, const int* inc,
+                      const double* const* dw, ocfd_handle** out);
+/* Number of solves of the handle. */
+int ocfd_nsolve(const ocfd_handle* h);
+/* ocfd_residual for every solve: res_max / res_rms hold 7*nsolve doubles (solve-major). */
+int ocfd_residual_all(ocfd_handle* h, double* res_max, double* res_rms);
+/* ocfd_forces for every solve: ft holds 9*nsolve doubles, cl / cd / cs nsolve each (may be
+ * NULL); each solve uses its own Ref_S, Ref_L, AoA and Cood_Y_UP. */
+int ocfd_forces_all(ocfd_handle* h, double* ft, double* cl, double* cd, double* cs);
+/* Upper estimate of the device bytes ocfd_create would allocate for these blocks and
+ * parameters (admission control by HBM footprint); -1 on bad arguments.  No device call. */
+long long ocfd_footprint(const ocfd_params* p, int nblk, const int* nijk);
+/* ocfd_advance only queues work on the handle's stream; this waits for it to finish.  Driving
+ * several handles from one host thread (advance each, then synchronize each) overlaps their
+ * work on the device. */
+int ocfd_synchronize(ocfd_handle* h);
+
 /* Library build/ABI information: "ocfd-b200 <abi> sm_100a ..." */
 const char* ocfd_version(void);
 

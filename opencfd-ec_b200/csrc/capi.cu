@@ -51,13 +51,16 @@ constexpr int LAPH = 4;
 }  // namespace
 
 struct ocfd_handle {
-  ocfd_params P;
+  ocfd_params P;                   // parameters of solve 0
+  std::vector<ocfd_params> Ps;     // per solve
+  std::vector<int> sblk0;          // first block of each solve (nsolve + 1 entries)
+  std::vector<long long> ncell_s;  // interior cells per solve
   int nvar = 5, prec = 0, nblk = 0, nsolve = 1;
   std::vector<BlkD> blk;
   std::vector<SubD> sub;
   std::vector<long long> pre_box, pre_cell, pre_face, pre_col, pre_subcell, pre_halo;
   std::vector<int4> cchunk, wchunk;
-  SolveP sp;
+  std::vector<SolveP> sps;
   long long tot_box = 0, tot_cell = 0, tot_face = 0, tot_node = 0, tot_col = 0, tot_subcell = 0, tot_halo = 0;
   long long ncell = 0;
   int max_plane = 3;
@@ -260,20 +263,45 @@ static cudaError_t up(T* d, const std::vector<T>& v) {
   return cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
 
-extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, const double* const* xyz, const int* nsub, const int* inc,
-                           const double* const* dw, ocfd_handle** out) {
-  if (!p || nblk <= 0 || !nijk || !xyz || !nsub || !inc || !out) return OCFD_ERR_ARG;
+// all solves of a handle share the model switches that select kernels; Mach, angles, Re, CFL,
+// schemes, fluxes and limits may differ per solve
+static int check_params(const ocfd_params* ps, int nsolve) {
+  const ocfd_params& p0 = ps[0];
+  for (int q = 0; q < nsolve; q++) {
+    const ocfd_params& p = ps[q];
+    int tm = p.if_viscous ? p.iflag_turbulence_model : 0;
+    if (tm != 0 && tm != 2 && tm != 3) return OCFD_ERR_UNSUPPORTED;
+    if (p.time_method != 0 && p.time_method != 3) return OCFD_ERR_UNSUPPORTED;
+    if (p.iflag_flux < 1 || p.iflag_flux > 6) return OCFD_ERR_ARG;
+    int tm0 = p0.if_viscous ? p0.iflag_turbulence_model : 0;
+    if (tm != tm0 || p.if_viscous != p0.if_viscous || p.time_method != p0.time_method || p.precision != p0.precision) return OCFD_ERR_ARG;
+  }
+  return OCFD_OK;
+}
+
+static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, const int* nijk, const double* const* xyz, const int* nsub,
+                       const int* inc, const double* const* dw, ocfd_handle** out) {
+  if (!ps || nsolve <= 0 || !nblk_s || !nijk || !xyz || !nsub || !inc || !out) return OCFD_ERR_ARG;
+  int nblk = 0;
+  for (int q = 0; q < nsolve; q++) {
+    if (nblk_s[q] <= 0) return OCFD_ERR_ARG;
+    nblk += nblk_s[q];
+  }
+  if (int rc = check_params(ps, nsolve)) return rc;
   std::unique_ptr<ocfd_handle> hp(new ocfd_handle());
   ocfd_handle* h = hp.get();
-  h->P = *p;
+  const ocfd_params* p = ps;
+  h->P = ps[0];
+  h->Ps.assign(ps, ps + nsolve);
+  h->nsolve = nsolve;
+  h->sblk0.assign(nsolve + 1, 0);
+  for (int q = 0; q < nsolve; q++) h->sblk0[q + 1] = h->sblk0[q] + nblk_s[q];
   int tm = p->if_viscous ? p->iflag_turbulence_model : 0;
   h->nvar = (tm == 2) ? 6 : (tm == 3 ? 7 : 5);
-  if (tm != 0 && tm != 2 && tm != 3) return OCFD_ERR_UNSUPPORTED;
-  if (p->time_method != 0 && p->time_method != 3) return OCFD_ERR_UNSUPPORTED;
-  if (p->iflag_flux < 1 || p->iflag_flux > 6) return OCFD_ERR_ARG;
   h->prec = p->precision;
   h->nblk = nblk;
-  fill_solve(*p, h->nvar, h->sp);
+  h->sps.resize(nsolve);
+  for (int q = 0; q < nsolve; q++) fill_solve(ps[q], h->nvar, h->sps[q]);
   // ---- tables
   h->blk.resize(nblk);
   h->pre_box.assign(nblk + 1, 0); h->pre_cell.assign(nblk + 1, 0); h->pre_face.assign(nblk + 1, 0); h->pre_col.assign(nblk + 1, 0);
@@ -285,7 +313,7 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
     if (B.nx < 2 || B.ny < 2 || B.nz < 2) return OCFD_ERR_ARG;
     B.NX = B.nx + 7; B.NY = B.ny + 7; B.NZ = B.nz + 7;
     B.NXn = B.nx + 2; B.NYn = B.ny + 2; B.NZn = B.nz + 2;
-    B.solve = 0;
+    B.solve = (int)(std::upper_bound(h->sblk0.begin(), h->sblk0.end(), b) - h->sblk0.begin()) - 1;
     B.obox = h->pre_box[b]; B.oface = h->pre_face[b]; B.ocell = h->pre_cell[b]; B.ocol = h->pre_col[b]; B.onode = onode;
     B.obci = obci; B.obcj = obcj; B.obck = obck;
     long long box = (long long)B.NX * B.NY * B.NZ;
@@ -307,7 +335,10 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
       S.ib1 = q[9]; S.ie1 = q[10]; S.jb1 = q[11]; S.je1 = q[12]; S.kb1 = q[13]; S.ke1 = q[14]; S.nb1 = q[15] - 1; S.face1 = q[16];
       S.f_no1 = q[17]; S.L1 = q[18]; S.L2 = q[19]; S.L3 = q[20];
       if (S.face < 1 || S.face > 6) return fail(nullptr, OCFD_ERR_ARG, "bad face");
-      if (S.bc < 0 && (S.nb1 < 0 || S.nb1 >= nblk)) return OCFD_ERR_ARG;
+      // partner block numbers are 1-based within the solve
+      const int sb0 = h->sblk0[B.solve], sbn = h->sblk0[B.solve + 1] - sb0;
+      if (S.bc < 0 && (S.nb1 < 0 || S.nb1 >= sbn)) return OCFD_ERR_ARG;
+      if (S.bc < 0) S.nb1 += sb0;
       if (S.bc > 0 && !(S.bc == 2 || S.bc == 3 || S.bc == 4 || S.bc == 5 || S.bc == 6 || S.bc == 401)) return OCFD_ERR_UNSUPPORTED;
       h->sub.push_back(S);
     }
@@ -315,6 +346,8 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
   h->tot_box = h->pre_box[nblk]; h->tot_face = h->pre_face[nblk]; h->tot_cell = h->pre_cell[nblk]; h->tot_col = h->pre_col[nblk];
   h->tot_node = onode;
   h->ncell = h->tot_cell;
+  h->ncell_s.assign(nsolve, 0);
+  for (int b = 0; b < nblk; b++) h->ncell_s[h->blk[b].solve] += h->pre_cell[b + 1] - h->pre_cell[b];
   int ns = (int)h->sub.size();
   h->pre_subcell.assign(ns + 1, 0); h->pre_halo.assign(ns + 1, 0);
   for (int s = 0; s < ns; s++) {
@@ -373,11 +406,13 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
     std::memcpy(&hz[B.onode], &X[b][2 * nn], nn * 8);
   }
   std::vector<double> Xw;
-  int turb = h->sp.turb;
+  std::vector<long long> wpre(nsolve + 1, 0);  // wall nodes of solve q: [wpre[q], wpre[q+1])
+  int turb = h->sps[0].turb;
   bool need_dw = turb != 0 && !(dw && dw[0]);
   if (need_dw) {
-    for (const SubD& S : h->sub) {
-      if (S.bc != 2) continue;
+    for (int sq_ = 0; sq_ < nsolve; sq_++) {
+     for (const SubD& S : h->sub) {
+      if (S.bc != 2 || h->blk[S.blk].solve != sq_) continue;
       const BlkD& B = h->blk[S.blk];
       for (int k = S.kb; k <= S.ke; k++)
         for (int j = S.jb; j <= S.je; j++)
@@ -386,6 +421,8 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
             size_t nn = (size_t)B.NXn * B.NYn * B.NZn;
             Xw.push_back(X[S.blk][o]); Xw.push_back(X[S.blk][nn + o]); Xw.push_back(X[S.blk][2 * nn + o]);
           }
+     }
+     wpre[sq_ + 1] = (long long)(Xw.size() / 3);
     }
   }
   X.clear();
@@ -397,7 +434,7 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
   const size_t ts = h->prec == OCFD_PREC_MIXED ? sizeof(float) : sizeof(double);
   h->d_blk = M.alloc<BlkD>(nblk, e);
   h->d_sub = M.alloc<SubD>(std::max(1, ns), e);
-  h->d_sp = M.alloc<SolveP>(1, e);
+  h->d_sp = M.alloc<SolveP>(nsolve, e);
   h->d_pre_box = M.alloc<long long>(nblk + 1, e); h->d_pre_cell = M.alloc<long long>(nblk + 1, e);
   h->d_pre_face = M.alloc<long long>(nblk + 1, e); h->d_pre_col = M.alloc<long long>(nblk + 1, e);
   h->d_pre_subcell = M.alloc<long long>(ns + 1, e); h->d_pre_halo = M.alloc<long long>(ns + 1, e);
@@ -432,10 +469,31 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
     h->d_volf = M.alloc<float>(tc, e); h->d_dtmf = M.alloc<float>(tc, e); h->d_dwf = M.alloc<float>(tc, e);
   }
   double* d_Xw = nullptr;
-  if (need_dw && !Xw.empty()) d_Xw = M.alloc<double>(Xw.size(), e);
+  long long* d_wpre = nullptr;
+  WallChunk* d_wch = nullptr;
+  int* d_wcpre = nullptr;
+  std::vector<WallChunk> wch;
+  std::vector<int> wcpre(nsolve + 1, 0);
+  if (need_dw) {
+    for (int q = 0; q < nsolve; q++) {
+      for (long long w0 = wpre[q]; w0 < wpre[q + 1]; w0 += 64) {
+        WallChunk C;
+        C.w0 = w0; C.w1 = std::min(w0 + 64, wpre[q + 1]);
+        for (int a = 0; a < 3; a++) { C.lo[a] = 1e300; C.hi[a] = -1e300; }
+        for (long long w = C.w0; w < C.w1; w++)
+          for (int a = 0; a < 3; a++) { C.lo[a] = std::min(C.lo[a], Xw[3 * w + a]); C.hi[a] = std::max(C.hi[a], Xw[3 * w + a]); }
+        wch.push_back(C);
+      }
+      wcpre[q + 1] = (int)wch.size();
+    }
+  }
+  if (need_dw && !Xw.empty()) {
+    d_Xw = M.alloc<double>(Xw.size(), e); d_wpre = M.alloc<long long>(nsolve + 1, e);
+    d_wch = M.alloc<WallChunk>(wch.size(), e); d_wcpre = M.alloc<int>(nsolve + 1, e);
+  }
   if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "allocation"); }
   // ---- uploads
-  if ((e = up(h->d_blk, h->blk)) || (e = up(h->d_sub, h->sub)) || (e = cudaMemcpy(h->d_sp, &h->sp, sizeof(SolveP), cudaMemcpyHostToDevice)) ||
+  if ((e = up(h->d_blk, h->blk)) || (e = up(h->d_sub, h->sub)) || (e = up(h->d_sp, h->sps)) ||
       (e = up(h->d_pre_box, h->pre_box)) || (e = up(h->d_pre_cell, h->pre_cell)) || (e = up(h->d_pre_face, h->pre_face)) ||
       (e = up(h->d_pre_col, h->pre_col)) || (e = up(h->d_pre_subcell, h->pre_subcell)) || (e = up(h->d_pre_halo, h->pre_halo)) ||
       (e = up(h->d_cchunk, h->cchunk)) || (e = up(h->d_wchunk, h->wchunk)) || (e = up(h->d_x, hx)) || (e = up(h->d_y, hy)) ||
@@ -443,17 +501,24 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
     M.release();
     return cuda_fail(nullptr, e, "upload");
   }
-  if (d_Xw) cudaMemcpy(d_Xw, Xw.data(), Xw.size() * 8, cudaMemcpyHostToDevice);
+  if (d_Xw) { cudaMemcpy(d_Xw, Xw.data(), Xw.size() * 8, cudaMemcpyHostToDevice); up(d_wpre, wpre); up(d_wch, wch); up(d_wcpre, wcpre); }
   if (dw && dw[0] && turb != 0) {
     std::vector<double> hdw(tc);
     for (int b = 0; b < nblk; b++) std::memcpy(&hdw[h->pre_cell[b]], dw[b], (h->pre_cell[b + 1] - h->pre_cell[b]) * 8);
     cudaMemcpy(h->d_dwd, hdw.data(), tc * 8, cudaMemcpyHostToDevice);
   }
-  // mu = 1/Re everywhere (allocate_mem_Blocks, sub_init.f90:507)
+  // mu = 1/Re everywhere (allocate_mem_Blocks, sub_init.f90:507), Re of each block's solve
   {
     size_t n = (size_t)tb;
-    if (h->prec == OCFD_PREC_MIXED) { std::vector<float> v(n, (float)(1.0 / p->re)); cudaMemcpy(h->d_mu, v.data(), n * 4, cudaMemcpyHostToDevice); }
-    else { std::vector<double> v(n, 1.0 / p->re); cudaMemcpy(h->d_mu, v.data(), n * 8, cudaMemcpyHostToDevice); }
+    std::vector<double> v(n);
+    for (int b = 0; b < nblk; b++)
+      std::fill(v.begin() + h->pre_box[b], v.begin() + h->pre_box[b + 1], 1.0 / ps[h->blk[b].solve].re);
+    if (h->prec == OCFD_PREC_MIXED) {
+      std::vector<float> vf(v.begin(), v.end());
+      cudaMemcpy(h->d_mu, vf.data(), n * 4, cudaMemcpyHostToDevice);
+    } else {
+      cudaMemcpy(h->d_mu, v.data(), n * 8, cudaMemcpyHostToDevice);
+    }
   }
   if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "stream"); }
   // ---- geometry on the device
@@ -462,7 +527,7 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
   G.tot_face = tf; G.tot_cell = tc; G.tot_box = tb; G.tot_node = onode;
   G.x = h->d_x; G.y = h->d_y; G.z = h->d_z; G.M = h->d_Md; G.scratch = (double*)h->d_Fi;
   G.vol = h->d_vold; G.dtm = h->d_dtmd; G.dw = h->d_dwd; G.xc = h->d_xc; G.yc = h->d_yc; G.zc = h->d_zc;
-  G.Xw = d_Xw; G.nwall = need_dw ? (long long)(Xw.size() / 3) : 0;
+  G.Xw = d_Xw; G.nwall = need_dw ? (long long)(Xw.size() / 3) : 0; G.wpre = d_wpre; G.wch = d_wch; G.wcpre = d_wcpre;
   if ((e = run_geometry(G, h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "geometry"); }
   if (h->prec == OCFD_PREC_MIXED) {
     convert_to_float(h->d_Md, h->d_Mf, (long long)M_COUNT * tf, h->st);
@@ -541,6 +606,50 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
   }
   if (bcerr) { M.release(); return OCFD_ERR_UNSUPPORTED; }
   *out = hp.release();
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, const double* const* xyz, const int* nsub, const int* inc,
+                           const double* const* dw, ocfd_handle** out) {
+  if (!p || nblk <= 0) return OCFD_ERR_ARG;
+  return create_impl(p, 1, &nblk, nijk, xyz, nsub, inc, dw, out);
+}
+
+extern "C" int ocfd_create_batch(const ocfd_params* ps, int nsolve, const int* nblk, const int* nijk, const double* const* xyz,
+                                 const int* nsub, const int* inc, const double* const* dw, ocfd_handle** out) {
+  return create_impl(ps, nsolve, nblk, nijk, xyz, nsub, inc, dw, out);
+}
+
+extern "C" int ocfd_nsolve(const ocfd_handle* h) { return h ? h->nsolve : 0; }
+
+extern "C" long long ocfd_footprint(const ocfd_params* p, int nblk, const int* nijk) {
+  if (!p || nblk <= 0 || !nijk) return -1;
+  long long tb = 0, tf = 0, tc = 0, tn = 0, maxbox = 0;
+  for (int b = 0; b < nblk; b++) {
+    long long nx = nijk[3 * b], ny = nijk[3 * b + 1], nz = nijk[3 * b + 2];
+    if (nx < 2 || ny < 2 || nz < 2) return -1;
+    long long box = (nx + 7) * (ny + 7) * (nz + 7);
+    tb += box; tf += nx * ny * nz; tc += (nx - 1) * (ny - 1) * (nz - 1); tn += (nx + 2) * (ny + 2) * (nz + 2);
+    maxbox = std::max(maxbox, box);
+  }
+  const int tm = p->if_viscous ? p->iflag_turbulence_model : 0;
+  const long long NV = tm == 2 ? 6 : (tm == 3 ? 7 : 5);
+  const long long ts = p->precision == OCFD_PREC_MIXED ? 4 : 8;
+  long long bytes = 0;
+  bytes += 3 * tn * 8 + M_COUNT * tf * 8 + 3 * tc * 8 + 3 * tb * 8;              // geometry (FP64)
+  bytes += NV * tb * 8 * (p->time_method == 3 ? 2 : 1) + std::max(NV, 5LL) * tc * 8;  // U, Un, DU
+  bytes += ts * (P_COUNT + 2) * tb + ts * (NV + 7) * tc;                          // P, mu, mut, Res, dt, Lc, Lv
+  bytes += std::max(ts * 15 * tf, 24 * tf) + (p->if_viscous ? ts * 12 * tf : 0) + (tm ? ts * 6 * tf : 0);
+  if (tm == 3) bytes += ts * (2 * tb + tf);
+  if (p->precision == OCFD_PREC_MIXED) bytes += 4 * (M_COUNT * tf + 3 * tc);
+  bytes += NV * maxbox * 8;                                                       // state staging
+  return bytes + bytes / 20 + (16LL << 20);                                       // tables, chunks, margin
+}
+
+extern "C" int ocfd_synchronize(ocfd_handle* h) {
+  if (!h) return OCFD_ERR_ARG;
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "synchronize");
   return OCFD_OK;
 }
 
@@ -638,21 +747,22 @@ extern "C" int ocfd_compute_residual(ocfd_handle* h, int with_lusgs) {
   return OCFD_OK;
 }
 
-extern "C" int ocfd_residual(ocfd_handle* h, double* rmax, double* rrms) {
-  if (!h || !rmax || !rrms) return OCFD_ERR_ARG;
+// norms of every solve (nout = 1: solve 0 only); NaN -> OCFD_ERR_NAN with the first location
+static int residual_impl(ocfd_handle* h, double* rmax, double* rrms, int nout) {
   unsigned long long init = ~0ULL;
   cudaMemcpyAsync(h->d_nan, &init, 8, cudaMemcpyHostToDevice, h->st);
   h->run->norms(h->st, h->d_norm_part, h->d_norm_out, h->d_nan);
-  double out[14];
+  std::vector<double> out(14 * (size_t)h->nsolve);
   unsigned long long nan_at = 0;
-  cudaMemcpyAsync(out, h->d_norm_out, sizeof(out), cudaMemcpyDeviceToHost, h->st);
+  cudaMemcpyAsync(out.data(), h->d_norm_out, out.size() * 8, cudaMemcpyDeviceToHost, h->st);
   cudaMemcpyAsync(&nan_at, h->d_nan, 8, cudaMemcpyDeviceToHost, h->st);
   cudaError_t e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "residual");
-  for (int m = 0; m < 7; m++) {
-    rmax[m] = m < h->nvar ? out[m] : 0.0;
-    rrms[m] = m < h->nvar ? std::sqrt(out[7 + m] / (double)h->ncell) : 0.0;
-  }
+  for (int q = 0; q < nout; q++)
+    for (int m = 0; m < 7; m++) {
+      rmax[7 * q + m] = m < h->nvar ? out[14 * q + m] : 0.0;
+      rrms[7 * q + m] = m < h->nvar ? std::sqrt(out[14 * q + 7 + m] / (double)h->ncell_s[q]) : 0.0;
+    }
   int lu_err = 0;
   cudaMemcpy(&lu_err, h->d_lu_err, 4, cudaMemcpyDeviceToHost);
   if (lu_err) {
@@ -666,15 +776,29 @@ extern "C" int ocfd_residual(ocfd_handle* h, double* rmax, double* rrms) {
     const BlkD& B = h->blk[b];
     long long l = g - h->pre_cell[b];
     int i = (int)(l % (B.nx - 1)) + 1, j = (int)((l / (B.nx - 1)) % (B.ny - 1)) + 1, k = (int)(l / ((long long)(B.nx - 1) * (B.ny - 1))) + 1;
-    char buf[160];
-    std::snprintf(buf, sizeof buf, "NaN in residual: block %d i,j,k,m = %d %d %d %d", b + 1, i, j, k, m + 1);
+    char buf[200];
+    if (h->nsolve > 1)
+      std::snprintf(buf, sizeof buf, "NaN in residual: solve %d block %d i,j,k,m = %d %d %d %d", B.solve, b - h->sblk0[B.solve] + 1, i, j, k, m + 1);
+    else
+      std::snprintf(buf, sizeof buf, "NaN in residual: block %d i,j,k,m = %d %d %d %d", b + 1, i, j, k, m + 1);
     return fail(h, OCFD_ERR_NAN, buf);
   }
   return OCFD_OK;
 }
 
-extern "C" int ocfd_forces(ocfd_handle* h, double* ft, double* cl, double* cd, double* cs) {
-  if (!h || !ft) return OCFD_ERR_ARG;
+extern "C" int ocfd_residual(ocfd_handle* h, double* rmax, double* rrms) {
+  if (!h || !rmax || !rrms) return OCFD_ERR_ARG;
+  return residual_impl(h, rmax, rrms, 1);
+}
+
+extern "C" int ocfd_residual_all(ocfd_handle* h, double* rmax, double* rrms) {
+  if (!h || !rmax || !rrms) return OCFD_ERR_ARG;
+  return residual_impl(h, rmax, rrms, h->nsolve);
+}
+
+// forces of every solve: partial sums per wall chunk, then per block in subface order, then over
+// the solve's blocks (sub_Post.f90:31-202)
+static int forces_impl(ocfd_handle* h, double* ft, double* cl, double* cd, double* cs, int nout) {
   size_t nw = h->wchunk.size();
   std::vector<double> part(9 * std::max<size_t>(nw, 1), 0.0);
   if (nw) {
@@ -683,26 +807,38 @@ extern "C" int ocfd_forces(ocfd_handle* h, double* ft, double* cl, double* cd, d
   }
   cudaError_t e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "forces");
-  // per block in subface order, then over blocks (sub_Post.f90:31-202)
-  double Ft[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<double> blk(9 * h->nblk, 0.0);
   for (size_t c = 0; c < nw; c++) {
     int b = h->sub[h->wchunk[c].x].blk;
     for (int q = 0; q < 9; q++) blk[9 * b + q] = blk[9 * b + q] + part[9 * c + q];
   }
-  for (int b = 0; b < h->nblk; b++)
-    for (int q = 0; q < 9; q++) Ft[q] = Ft[q] + blk[9 * b + q];
-  const ocfd_params& P = h->P;
-  for (int q = 0; q < 6; q++) ft[q] = 2.0 * Ft[q] / P.ref_s;
-  for (int q = 6; q < 9; q++) ft[q] = 2.0 * Ft[q] / (P.ref_s * P.ref_l);
-  double Fx = ft[0] + ft[3], Fy = ft[1] + ft[4], Fz = ft[2] + ft[5];
-  double L, D, S;
-  if (P.cood_y_up == 1) { L = Fy * std::cos(P.aoa) - Fx * std::sin(P.aoa); D = Fx * std::cos(P.aoa) + Fy * std::sin(P.aoa); S = Fz; }
-  else { L = Fz * std::cos(P.aoa) - Fx * std::sin(P.aoa); D = Fx * std::cos(P.aoa) + Fz * std::sin(P.aoa); S = Fy; }
-  if (cl) *cl = L;
-  if (cd) *cd = D;
-  if (cs) *cs = S;
+  for (int sv = 0; sv < nout; sv++) {
+    double Ft[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = h->sblk0[sv]; b < h->sblk0[sv + 1]; b++)
+      for (int q = 0; q < 9; q++) Ft[q] = Ft[q] + blk[9 * b + q];
+    const ocfd_params& P = h->Ps[sv];
+    double* f = ft + 9 * sv;
+    for (int q = 0; q < 6; q++) f[q] = 2.0 * Ft[q] / P.ref_s;
+    for (int q = 6; q < 9; q++) f[q] = 2.0 * Ft[q] / (P.ref_s * P.ref_l);
+    double Fx = f[0] + f[3], Fy = f[1] + f[4], Fz = f[2] + f[5];
+    double L, D, S;
+    if (P.cood_y_up == 1) { L = Fy * std::cos(P.aoa) - Fx * std::sin(P.aoa); D = Fx * std::cos(P.aoa) + Fy * std::sin(P.aoa); S = Fz; }
+    else { L = Fz * std::cos(P.aoa) - Fx * std::sin(P.aoa); D = Fx * std::cos(P.aoa) + Fz * std::sin(P.aoa); S = Fy; }
+    if (cl) cl[sv] = L;
+    if (cd) cd[sv] = D;
+    if (cs) cs[sv] = S;
+  }
   return OCFD_OK;
+}
+
+extern "C" int ocfd_forces(ocfd_handle* h, double* ft, double* cl, double* cd, double* cs) {
+  if (!h || !ft) return OCFD_ERR_ARG;
+  return forces_impl(h, ft, cl, cd, cs, 1);
+}
+
+extern "C" int ocfd_forces_all(ocfd_handle* h, double* ft, double* cl, double* cd, double* cs) {
+  if (!h || !ft) return OCFD_ERR_ARG;
+  return forces_impl(h, ft, cl, cd, cs, h->nsolve);
 }
 
 extern "C" void* ocfd_stream(ocfd_handle* h) { return h ? (void*)h->st : nullptr; }

@@ -282,8 +282,13 @@ __global__ void k_mesh_quality(GeoP G) {
   }
 }
 
-// wall distance: one thread per node, loop over all wall nodes, then cell average
-__global__ void k_wall_dist_nodes(GeoP G, const double* Xw, long long nw, double* dis) {
+// wall distance (comput_wall_dist, sub_comput_dw.f90:43-101): for every node the minimum of
+// sqrt(dx^2+dy^2+dz^2) over the wall nodes of its own solve, initial value 1e8.  The search is
+// pruned by the chunks' bounding boxes: a first pass bounds the minimum from above by the
+// farthest-corner distance of every box, the second evaluates only boxes whose nearest-point
+// distance can reach that bound.  The minimum is taken over squared distances and rooted once:
+// sqrt is monotone and correctly rounded, so this equals the minimum of the rooted values.
+__global__ void k_wall_dist_nodes(GeoP G, const double* Xw, const WallChunk* ch, const int* wcpre, double* dis) {
   GS(g, G.tot_face) {
     int b = sfind(G.pre_face, G.nblk, g);
     const BlkD& B = G.blk[b];
@@ -292,9 +297,33 @@ __global__ void k_wall_dist_nodes(GeoP G, const double* Xw, long long nw, double
     long long t = l / B.nx;
     int j = (int)(t % B.ny) + 1, k = (int)(t / B.ny) + 1;
     long long q = gn(B, i, j, k);
-    double px = G.x[q], py = G.y[q], pz = G.z[q], dmin = 1.e8;
-    for (long long w = 0; w < nw; w++) {
-      double d1 = sqrt(sq2(px - Xw[3 * w]) + sq2(py - Xw[3 * w + 1]) + sq2(pz - Xw[3 * w + 2]));
+    const double px = G.x[q], py = G.y[q], pz = G.z[q];
+    const int c0 = wcpre[B.solve], c1 = wcpre[B.solve + 1];
+    double ub = 1.0e300;
+    for (int c = c0; c < c1; c++) {
+      const WallChunk& C = ch[c];
+      double fx = fmax(fabs(px - C.lo[0]), fabs(px - C.hi[0]));
+      double fy = fmax(fabs(py - C.lo[1]), fabs(py - C.hi[1]));
+      double fz = fmax(fabs(pz - C.lo[2]), fabs(pz - C.hi[2]));
+      ub = fmin(ub, fx * fx + fy * fy + fz * fz);
+    }
+    ub = ub * (1.0 + 1.0e-12);
+    double best = 1.0e300;
+    for (int c = c0; c < c1; c++) {
+      const WallChunk& C = ch[c];
+      double ex = fmax(fmax(C.lo[0] - px, px - C.hi[0]), 0.0);
+      double ey = fmax(fmax(C.lo[1] - py, py - C.hi[1]), 0.0);
+      double ez = fmax(fmax(C.lo[2] - pz, pz - C.hi[2]), 0.0);
+      double lb = (ex * ex + ey * ey + ez * ez) * (1.0 - 1.0e-12);
+      if (lb > ub || lb > best) continue;
+      for (long long w = C.w0; w < C.w1; w++) {
+        double d2 = sq2(px - Xw[3 * w]) + sq2(py - Xw[3 * w + 1]) + sq2(pz - Xw[3 * w + 2]);
+        if (d2 < best) best = d2;
+      }
+    }
+    double dmin = 1.e8;
+    if (best < 1.0e300) {
+      double d1 = sqrt(best);
       if (d1 < dmin) dmin = d1;
     }
     dis[g] = dmin;
@@ -342,7 +371,7 @@ cudaError_t run_geometry(const GeoArgs& a, cudaStream_t st) {
   k_geom_jac<0><<<grid_for(a.tot_face), 256, 0, st>>>(G);
   k_mesh_quality<<<grid_for(a.tot_cell), 256, 0, st>>>(G);
   if (a.nwall > 0 && a.Xw) {
-    k_wall_dist_nodes<<<grid_for(a.tot_face), 128, 0, st>>>(G, a.Xw, a.nwall, a.scratch);
+    k_wall_dist_nodes<<<grid_for(a.tot_face), 128, 0, st>>>(G, a.Xw, a.wch, a.wcpre, a.scratch);
     k_wall_dist_cells<<<grid_for(a.tot_cell), 256, 0, st>>>(G, a.scratch);
   }
   return cudaGetLastError();

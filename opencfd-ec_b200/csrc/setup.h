@@ -16,8 +16,17 @@ struct GeoArgs {
   double* scratch;          // >= 3*tot_face doubles
   double *vol, *dtm, *dw;   // cell
   double *xc, *yc, *zc;     // box
-  const double* Xw;         // wall nodes (3 per node) or null
+  const double* Xw;         // wall nodes (3 per node) or null, grouped by solve
   long long nwall;
+  const long long* wpre;    // nsolve + 1: wall nodes of solve q are [wpre[q], wpre[q+1])
+  const struct WallChunk* wch;  // chunks of consecutive wall nodes with their bounding boxes
+  const int* wcpre;         // nsolve + 1: chunks of solve q are [wcpre[q], wcpre[q+1])
+};
+
+// a run of up to 64 consecutive wall nodes of one solve and its axis-aligned bounding box
+struct WallChunk {
+  double lo[3], hi[3];
+  long long w0, w1;
 };
 
 cudaError_t run_geometry(const GeoArgs& a, cudaStream_t st);

@@ -19,7 +19,8 @@ EXPORTED = [
     "ocfd_default_params", "ocfd_finalize_params", "ocfd_create", "ocfd_destroy", "ocfd_last_error", "ocfd_state_size",
     "ocfd_set_state", "ocfd_get_state", "ocfd_init_flow", "ocfd_advance", "ocfd_residual", "ocfd_forces",
     "ocfd_limiter_status", "ocfd_array_shape", "ocfd_get_array", "ocfd_version", "ocfd_compute_residual",
-    "ocfd_stream", "ocfd_profile", "ocfd_launches_per_step",
+    "ocfd_stream", "ocfd_profile", "ocfd_launches_per_step", "ocfd_create_batch", "ocfd_nsolve",
+    "ocfd_residual_all", "ocfd_forces_all", "ocfd_footprint", "ocfd_synchronize",
 ]
 
 
@@ -60,6 +61,13 @@ def lib():
         L.ocfd_stream.restype = vp
         L.ocfd_profile.argtypes = [vp, ctypes.c_int, dp]
         L.ocfd_launches_per_step.argtypes = [vp]
+        L.ocfd_create_batch.argtypes = [pp, ctypes.c_int, ip, ip, ctypes.POINTER(dp), ip, ip, ctypes.POINTER(dp), ctypes.POINTER(vp)]
+        L.ocfd_nsolve.argtypes = [vp]
+        L.ocfd_residual_all.argtypes = [vp, dp, dp]
+        L.ocfd_forces_all.argtypes = [vp, dp, dp, dp, dp]
+        L.ocfd_footprint.argtypes = [pp, ctypes.c_int, ip]
+        L.ocfd_footprint.restype = ctypes.c_longlong
+        L.ocfd_synchronize.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -72,26 +80,49 @@ def _ip(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
 
 
+def footprint(params, case):
+    """Device bytes a handle for this case would take (upper estimate, no device call)."""
+    nijk = np.array([v for d in case.dims for v in d], dtype=np.int32)
+    return int(lib().ocfd_footprint(ctypes.byref(params), len(case.dims), _ip(nijk)))
+
+
 class Solver:
     """One case resident on the current GPU, driven through the C-ABI."""
 
     def __init__(self, params, case, dw=None):
+        self._create([(params, case)], dw)
+
+    def _create(self, items, dw=None):
         L = lib()
-        self.case = case
-        self.params = params.copy()
-        nijk, xyz, nsub, inc = case.flat()
-        self._keep = (nijk, xyz, nsub, inc)
+        self.cases = [c for _, c in items]
+        self.case = self.cases[0]
+        self.params = items[0][0].copy()
+        self.params_list = [p.copy() for p, _ in items]
+        flats = [c.flat() for c in self.cases]
+        nijk = np.concatenate([f[0] for f in flats]).astype(np.int32)
+        xyz = [a for f in flats for a in f[1]]
+        nsub = np.concatenate([f[2] for f in flats]).astype(np.int32)
+        inc = np.concatenate([f[3] for f in flats]).astype(np.int32)
+        nblk_s = np.array([len(f[1]) for f in flats], dtype=np.int32)
+        self._keep = (nijk, xyz, nsub, inc, nblk_s)
         xyz_ptrs = (ctypes.POINTER(ctypes.c_double) * len(xyz))(*[_dp(a) for a in xyz])
         dwp = None
         if dw is not None:
             self._dw = [np.ascontiguousarray(d, dtype=np.float64) for d in dw]
             dwp = (ctypes.POINTER(ctypes.c_double) * len(dw))(*[_dp(a) for a in self._dw])
         h = ctypes.c_void_p()
-        rc = L.ocfd_create(ctypes.byref(self.params), len(xyz), _ip(nijk), xyz_ptrs, _ip(nsub), _ip(inc), dwp, ctypes.byref(h))
+        if len(items) == 1:
+            rc = L.ocfd_create(ctypes.byref(self.params), len(xyz), _ip(nijk), xyz_ptrs, _ip(nsub), _ip(inc), dwp, ctypes.byref(h))
+        else:
+            parr = (OcfdParams * len(items))(*self.params_list)
+            rc = L.ocfd_create_batch(parr, len(items), _ip(nblk_s), _ip(nijk), xyz_ptrs, _ip(nsub), _ip(inc), dwp, ctypes.byref(h))
         if rc != 0:
             raise OcfdError(rc, "ocfd_create failed")
         self.h = h
         self.nblk = len(xyz)
+        self.nsolve = len(items)
+        self.blk0 = np.concatenate([[0], np.cumsum(nblk_s)]).astype(int)
+        self.dims = [d for c in self.cases for d in c.dims]
         self.nvar = int(self.params.nvar)
 
     def close(self):
@@ -137,7 +168,7 @@ class Solver:
     def state_shape(self, b):
         if not 0 <= b < self.nblk:
             raise OcfdError(OCFD_ERR_ARG, "block %d out of range (%d blocks)" % (b, self.nblk))
-        nx, ny, nz = self.case.dims[b]
+        nx, ny, nz = self.dims[b]
         return (nz + 7, ny + 7, nx + 7, self.nvar)
 
     def get_state(self, b, out=None):
@@ -179,6 +210,33 @@ class Solver:
 
     def launches_per_step(self):
         return int(lib().ocfd_launches_per_step(self.h))
+
+    def synchronize(self):
+        self._check(lib().ocfd_synchronize(self.h), "synchronize")
+
+    def residual_all(self):
+        """(res_max, res_rms), each (nsolve, 7); NaN in a solve shows as NaN in its rms."""
+        a, b = np.zeros(7 * self.nsolve), np.zeros(7 * self.nsolve)
+        rc = lib().ocfd_residual_all(self.h, _dp(a), _dp(b))
+        if rc not in (0, OCFD_ERR_NAN):
+            self._check(rc, "residual_all")
+        return a.reshape(self.nsolve, 7), b.reshape(self.nsolve, 7)
+
+    def forces_all(self):
+        """(ft (nsolve, 9), cl, cd, cs (nsolve,))."""
+        n = self.nsolve
+        ft, cl, cd, cs = np.zeros(9 * n), np.zeros(n), np.zeros(n), np.zeros(n)
+        self._check(lib().ocfd_forces_all(self.h, _dp(ft), _dp(cl), _dp(cd), _dp(cs)), "forces_all")
+        return ft.reshape(n, 9), cl, cd, cs
+
+
+class Batch(Solver):
+    """Many independent cases in one handle: each step is one launch sequence over all blocks.
+    items: list of (params, case).  Blocks are numbered globally in item order; solve q owns
+    blocks blk0[q] .. blk0[q+1]-1."""
+
+    def __init__(self, items, dw=None):
+        self._create(list(items), dw)
 
 
 def version():

@@ -1,0 +1,161 @@
+"""Continuous-batching request loop over the C-ABI.
+
+Requests (a case + its parameters) arrive over time.  The loop admits a waiting request as soon
+as a slot is free and its device footprint (``ocfd_footprint``) fits in the HBM budget, keeps
+every admitted solve resident on the device, and advances all admitted solves together: each
+round queues ``chunk`` iterations on every handle's own stream (so the solves overlap on the
+GPU) and then reads back each solve's residual norms and forces.  A solve leaves as soon as it
+converges (density-residual RMS down by ``drop`` from its first iteration, or |dCL| below
+``dcl`` over the last ``dcl_window`` iterations) or reaches ``max_iters``; its memory is
+released for the next admission.
+
+The sequence of operations on one handle does not depend on the other solves in flight, so a
+request's result is the same alone and in the mix (bit for bit).  No counterpart in the
+reference, which runs one case per MPI job.
+"""
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import capi
+
+
+@dataclass
+class Request:
+    rid: int
+    params: object
+    case: object
+    arrival: float = 0.0            # seconds after the loop starts
+    max_iters: int = 5000
+
+
+@dataclass
+class Result:
+    rid: int
+    cells: int
+    arrival: float
+    admitted: float
+    finished: float
+    iters: int
+    converged: str                  # "residual", "cl", or "max_iters"
+    rms0: float
+    rms: np.ndarray
+    cl: float
+    cd: float
+    cl_hist: List[float] = field(default_factory=list)
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+
+class _Active:
+    def __init__(self, req, solver, admitted):
+        self.req, self.s, self.admitted = req, solver, admitted
+        self.iters = 0
+        self.rms0 = None
+        self.cl_hist = []    # (iteration, CL) at every read-back
+
+
+class Server:
+    def __init__(self, hbm_budget: Optional[int] = None, max_active: int = 32, chunk: int = 50, drop: float = 1e-6,
+                 dcl: float = 1e-4, dcl_window: int = 200, clock=time.perf_counter):
+        self.hbm_budget = hbm_budget
+        self.max_active = max_active
+        self.chunk = chunk
+        self.drop, self.dcl, self.dcl_window = drop, dcl, dcl_window
+        self.clock = clock
+
+    def _budget(self):
+        if self.hbm_budget is not None:
+            return self.hbm_budget
+        import torch
+        free, _ = torch.cuda.mem_get_info()
+        return int(free * 0.9)
+
+    def _done(self, a):
+        _, rms = a.s.residual()
+        _, cl, cd, _ = a.s.forces()
+        a.cl_hist.append((a.iters, cl))
+        if a.rms0 is None:
+            a.rms0 = rms[0]
+        if rms[0] <= self.drop * a.rms0:
+            return "residual", rms, cl, cd
+        old = [c for it, c in a.cl_hist if it <= a.iters - self.dcl_window]
+        if old and a.iters >= self.dcl_window and abs(cl - old[-1]) < self.dcl and \
+                all(abs(cl - c) < self.dcl for it, c in a.cl_hist if it >= a.iters - self.dcl_window):
+            return "cl", rms, cl, cd
+        if a.iters >= a.req.max_iters:
+            return "max_iters", rms, cl, cd
+        return None, rms, cl, cd
+
+    def run(self, requests: List[Request]) -> List[Result]:
+        pending = sorted(requests, key=lambda r: r.arrival)
+        queue, active, results = [], [], []
+        budget = self._budget()
+        used = 0
+        fp = {}
+        t0 = self.clock()
+        while pending or queue or active:
+            now = self.clock() - t0
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.pop(0))
+            # admission: FIFO, by free slot and device footprint
+            while queue and len(active) < self.max_active:
+                r = queue[0]
+                need = fp.setdefault(r.rid, capi.footprint(r.params, r.case))
+                if used + need > budget:
+                    if not active:
+                        raise MemoryError("request %d needs %d bytes, budget %d" % (r.rid, need, budget))
+                    break
+                queue.pop(0)
+                s = capi.Solver(r.params, r.case)
+                used += need
+                a = _Active(r, s, self.clock() - t0)
+                s.advance(1)
+                a.iters = 1
+                active.append(a)
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, min(0.05, pending[0].arrival - (self.clock() - t0))))
+                continue
+            # one round: queue work on every stream first, then read each solve back
+            for a in active:
+                if a.iters > 1 or a.rms0 is not None:
+                    n = min(self.chunk, a.req.max_iters - a.iters)
+                    if n > 0:
+                        a.s.advance(n)
+                        a.iters += n
+            still = []
+            for a in active:
+                why, rms, cl, cd = self._done(a)
+                if why is None:
+                    still.append(a)
+                    continue
+                fin = self.clock() - t0
+                results.append(Result(a.req.rid, a.req.case.ncells, a.req.arrival, a.admitted, fin, a.iters, why,
+                                      float(a.rms0), rms.copy(), cl, cd, [c for _, c in a.cl_hist]))
+                a.s.close()
+                used -= fp[a.req.rid]
+            active = still
+        return sorted(results, key=lambda r: r.rid)
+
+
+def poisson_requests(items, rate=2.0, seed=2024, max_iters=5000):
+    """Requests for the given (params, case) items with exponential inter-arrival times."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for q, (p, case) in enumerate(items):
+        t += float(rng.exponential(1.0 / rate))
+        out.append(Request(q, p, case, t, max_iters))
+    return out
+
+
+def summarize(results, wall_s):
+    lat = np.array([r.latency for r in results])
+    cells = sum(r.cells * r.iters for r in results)
+    return {"requests": len(results), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "cell_updates_per_s": cells / wall_s, "wall_s": wall_s,
+            "converged": {k: sum(1 for r in results if r.converged == k) for k in ("residual", "cl", "max_iters")}}

@@ -1,0 +1,84 @@
+"""Batches of independent solves in one handle (ocfd_create_batch): every solve of a batch gives
+bit for bit the result it gives alone (same kernels, per-block arithmetic, per-solve reductions
+in a fixed order), for uneven mesh sizes and different flow conditions."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def items(precision=0):
+    from ocfd_b200 import cases
+    return [
+        cases.airfoil(ni=65, nj=17, m=0.02, t=0.12, ma=0.7, aoa=2.0, precision=precision),
+        cases.airfoil(ni=81, nj=25, m=0.0, t=0.10, ma=0.5, aoa=-1.0, precision=precision),
+        cases.airfoil(ni=49, nj=21, m=0.04, t=0.15, ma=0.8, aoa=4.0, precision=precision),
+    ]
+
+
+def run(s, steps):
+    s.advance(steps)
+    return s
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_equals_alone(gpu, precision):
+    its = items(precision)
+    batch = run(gpu.Batch(its), 6)
+    rmax, rrms = batch.residual_all()
+    ft, cl, cd, cs = batch.forces_all()
+    for q, (p, case) in enumerate(its):
+        alone = run(gpu.Solver(p, case), 6)
+        am, ar = alone.residual()
+        aft, acl, acd, acs = alone.forces()
+        assert np.array_equal(ar, rrms[q]) and np.array_equal(am, rmax[q]), q
+        assert np.array_equal(aft, ft[q]) and acl == cl[q] and acd == cd[q], q
+        for b in range(len(case.dims)):
+            assert np.array_equal(alone.get_state(b), batch.get_state(batch.blk0[q] + b)), (q, b)
+        alone.close()
+    batch.close()
+
+
+def test_batch_matches_oracle(gpu, oracle):
+    """Each solve of an FP64 batch against the oracle run of that case alone."""
+    its = items(0)
+    batch = run(gpu.Batch(its), 4)
+    _, rrms = batch.residual_all()
+    _, cl, cd, _ = batch.forces_all()
+    for q, (p, case) in enumerate(its):
+        o = oracle.OracleCase(p, case)
+        o.advance(4)
+        np.testing.assert_allclose(rrms[q][:6], o.residual()[1][:6], rtol=1e-11)
+        _, ocl, ocd, _ = o.forces()
+        assert abs(cl[q] - ocl) <= 1e-10 * abs(ocl) and abs(cd[q] - ocd) <= 1e-10 * abs(ocd)
+        o.close()
+    batch.close()
+
+
+def test_footprint_bounds_allocation(gpu):
+    import torch
+    from ocfd_b200 import cases
+    p, case = cases.config2_medium()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    s = gpu.Solver(p, case)
+    s.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    used = free0 - free1
+    est = gpu.footprint(p, case)
+    assert used <= est <= 2 * used + (64 << 20), (used, est)
+    s.close()
+
+
+def test_config4_batch_runs(gpu):
+    """The 64-airfoil batch (uneven 129x33 .. 385x97 O-meshes, SA, AUSMPW + MUSCL3, mixed) in
+    one handle: one graph launch per step for all 64 solves, finite residuals and forces."""
+    from ocfd_b200 import cases
+    its = cases.config4_batch(n=64)
+    b = gpu.Batch(its)
+    assert b.nsolve == 64
+    b.advance(20)
+    _, rrms = b.residual_all()
+    _, cl, cd, _ = b.forces_all()
+    assert np.all(np.isfinite(rrms)) and np.all(np.isfinite(cl)) and np.all(np.isfinite(cd))
+    b.close()

@@ -266,8 +266,8 @@ __global__ void __launch_bounds__(64) k_lusgs_wave(Arena<T> A, LuArgs L) {
 template <int NV>
 struct LuDir {      // direction-thread data of one step (old state only)
   double n1, n2, n3, S;
-  double Unb[NV];   // neighbour state (U6/U7 clamped as limit_vt leaves them)
-  double wLc, Lv;   // w * Lc and Lv of the neighbour in this direction
+  double Unb[NV];   // neighbour state, U6/U7 clamped as limit_vt leaves them (cross-tile only)
+  double wLc, Lv;   // Lc and Lv of the neighbour in this direction (cross-tile only)
 };
 
 template <int NV>
@@ -284,10 +284,11 @@ __device__ __forceinline__ void cta_bar() { asm volatile("bar.sync 1, %0;" ::"n"
 __device__ __forceinline__ double ldro(const float* p) { return (double)__ldg(p); }
 
 template <class T, int NV, bool UPPER, int TC>
-__global__ void __launch_bounds__(4 * TC, 128 / TC) k_lusgs_wave3(Arena<T> A, LuArgs L) {
+__global__ void __launch_bounds__(4 * TC, 64 / TC) k_lusgs_wave3(Arena<T> A, LuArgs L) {
   __shared__ int s_tile;
-  __shared__ double s_acc[3][NV][TC];    // direction terms of the current step
-  __shared__ double s_pub[NV + 1][TC];   // DU and p(U+DU) of each column's last cell
+  __shared__ double s_acc[3][NV][TC];      // direction terms of the current step
+  __shared__ double s_pub[NV + 1][TC];     // DU and p(U+DU) of each column's last cell
+  __shared__ double s_old[2][NV + 6][TC];  // old state U, Lc(3), Lv(3) of each column's cell, by step parity
   const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
   const int TJ = L.TJ, TK = L.TK;
   const int tid = threadIdx.x, grp = tid / TC, c = tid % TC;
@@ -344,6 +345,7 @@ __global__ void __launch_bounds__(4 * TC, 128 / TC) k_lusgs_wave3(Arena<T> A, Lu
       // the lower face's area (lower sweep) or the upper face's (upper sweep, sub_LU_SGS.f90:96-97)
       const long long fs = UPPER ? fix_(B, i + (d == 0), j + (d == 1), k + (d == 2)) : f;
       x.S = ldro(A.M + (M_SI + d) * tf + fs);
+      if (!xt) return;  // in-tile neighbours publish their old state in shared memory
       const int ii = i + (d == 0 ? off : 0), jj = j + (d == 1 ? off : 0), kk = k + (d == 2 ? off : 0);
       const long long bn = bix(B, ii, jj, kk), cn = cix(B, ii, jj, kk);
 #pragma unroll
@@ -373,13 +375,24 @@ __global__ void __launch_bounds__(4 * TC, 128 / TC) k_lusgs_wave3(Arena<T> A, Lu
     // direction thread state for the current step: old-state half of the flux difference
     double un1 = 0.0, F1[NV], n1 = 0.0, n2 = 0.0, n3 = 0.0, S = 0.0, wLc = 0.0, Lvn = 0.0, Unb[NV];
     bool has = false;
-    auto prep_dir = [&](int t, const LuDir<NV>& x) {  // comput_DFn's U terms (sub_LU_SGS.f90:135-157)
+    // comput_DFn's U terms (sub_LU_SGS.f90:135-157) of step t; in-tile neighbours' old state is
+    // read from s_old[(t-1)&1], published by their owners during step t-1
+    auto prep_dir = [&](int t, const LuDir<NV>& x) {
       has = on_at(t) && has_at(t);
-      n1 = x.n1; n2 = x.n2; n3 = x.n3; S = x.S; Lvn = x.Lv;
-      wLc = w * x.wLc;
-#pragma unroll
-      for (int m = 0; m < NV; m++) Unb[m] = x.Unb[m];
       if (!has) return;
+      n1 = x.n1; n2 = x.n2; n3 = x.n3; S = x.S;
+      if (xt) {
+        Lvn = x.Lv;
+        wLc = w * x.wLc;
+#pragma unroll
+        for (int m = 0; m < NV; m++) Unb[m] = x.Unb[m];
+      } else {
+        const int pb = (t - 1) & 1;
+        Lvn = s_old[pb][NV + 3 + d][pubcol];
+        wLc = w * s_old[pb][NV + d][pubcol];
+#pragma unroll
+        for (int m = 0; m < NV; m++) Unb[m] = s_old[pb][m][pubcol];
+      }
       un1 = (Unb[1] * n1 + Unb[2] * n2 + Unb[3] * n3) / Unb[0];
       const double p1 = (gamma - 1.0) * (Unb[4] - 0.5 * (sq(Unb[1]) + sq(Unb[2]) + sq(Unb[3])) / Unb[0]);
       F1[0] = Unb[0] * un1;
@@ -391,11 +404,13 @@ __global__ void __launch_bounds__(4 * TC, 128 / TC) k_lusgs_wave3(Arena<T> A, Lu
       for (int m = 5; m < NV; m++) F1[m] = Unb[m] * un1;
     };
     // owner state for the current step
-    double oU[NV], oR[NV], alfa[NV];
+    double oU[NV], oR[NV], alfa[NV], oL[6];
     auto prep_own = [&](const LuOwn<NV>& x) {  // diagonal (sub_LU_SGS.f90:50-62, 90-92)
       const double a0 = x.vol / x.dt + w * (x.Lc[0] + x.Lc[1] + x.Lc[2]);
 #pragma unroll
       for (int m = 0; m < NV; m++) { alfa[m] = a0; oU[m] = x.U[m]; oR[m] = x.R[m]; }
+#pragma unroll
+      for (int q2 = 0; q2 < 3; q2++) { oL[q2] = x.Lc[q2]; oL[3 + q2] = x.Lv[q2]; }
       if (visc) {
         const double lv = x.Lv[0] + x.Lv[1] + x.Lv[2];
 #pragma unroll
@@ -421,6 +436,12 @@ __global__ void __launch_bounds__(4 * TC, 128 / TC) k_lusgs_wave3(Arena<T> A, Lu
       if (on_at(0)) { load_own(0, on); prep_own(on); }
       for (int t = 0; t < nsteps; t++) {
         cta_bar<4 * TC>();  // B1
+        if (on_at(t)) {  // publish this step's old state for the downstream cells' next step
+#pragma unroll
+          for (int m = 0; m < NV; m++) s_old[t & 1][m][c] = oU[m];
+#pragma unroll
+          for (int q2 = 0; q2 < 6; q2++) s_old[t & 1][NV + q2][c] = oL[q2];
+        }
         if (on_at(t + 1)) load_own(t + 1, on);
         cta_bar<4 * TC>();  // B2: the three direction terms of step t are in shared memory
         if (on_at(t)) {

@@ -71,8 +71,11 @@ struct Arena {
   int nsub;
   const long long* pre_subcell;  // nsub+1 prefix sums of face cells per subface (transverse ranges b..e-1)
   const long long* pre_halo;     // nsub+1 prefix sums of halo target cells per inner subface (LAP deep)
-  const int4* cchunk;            // norm chunks (blk, first local cell, count, -)
+  const int4* cchunk;            // norm chunks (blk, first local cell, count, -), in block order
   int ncchunk;
+  const int* cspre;              // nsolve+1: chunks of solve q are [cspre[q], cspre[q+1])
+  const int* bc_ent;             // boundary work list: subface of each entry, grouped in rounds
+  const long long* bc_pre;       // prefix sums of the entries' cells (per round, from 0)
   const int4* wchunk;            // force chunks (subface, first local face cell, count, -)
   int nwchunk;
   const SolveP* sp;

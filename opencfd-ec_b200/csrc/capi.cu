@@ -71,6 +71,12 @@ struct ocfd_handle {
   SolveP* d_sp = nullptr;
   long long *d_pre_box = nullptr, *d_pre_cell = nullptr, *d_pre_face = nullptr, *d_pre_col = nullptr, *d_pre_subcell = nullptr, *d_pre_halo = nullptr;
   int4 *d_cchunk = nullptr, *d_wchunk = nullptr;
+  int* d_cspre = nullptr;
+  std::vector<int> cspre;
+  std::vector<int> bc_ent, bc_rounds;   // boundary work list (entries grouped by round)
+  std::vector<long long> bc_pre;
+  int* d_bc_ent = nullptr;
+  long long* d_bc_pre = nullptr;
   double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr, *d_Md = nullptr, *d_vold = nullptr, *d_dtmd = nullptr, *d_dwd = nullptr;
   double *d_xc = nullptr, *d_yc = nullptr, *d_zc = nullptr;
   float *d_Mf = nullptr, *d_volf = nullptr, *d_dtmf = nullptr, *d_dwf = nullptr;
@@ -243,7 +249,8 @@ static void fill_arena(ocfd_handle* h, Arena<T>& A, const T* M, const T* vol, co
   A.pre_box = h->d_pre_box; A.pre_cell = h->d_pre_cell; A.pre_face = h->d_pre_face; A.pre_col = h->d_pre_col;
   A.sub = h->d_sub; A.nsub = (int)h->sub.size();
   A.pre_subcell = h->d_pre_subcell; A.pre_halo = h->d_pre_halo;
-  A.cchunk = h->d_cchunk; A.ncchunk = (int)h->cchunk.size();
+  A.cchunk = h->d_cchunk; A.ncchunk = (int)h->cchunk.size(); A.cspre = h->d_cspre;
+  A.bc_ent = h->d_bc_ent; A.bc_pre = h->d_bc_pre;
   A.wchunk = h->d_wchunk; A.nwchunk = (int)h->wchunk.size();
   A.sp = h->d_sp; A.nsolve = h->nsolve;
   A.tot_box = h->tot_box; A.tot_cell = h->tot_cell; A.tot_face = h->tot_face; A.tot_node = h->tot_node; A.tot_col = h->tot_col;
@@ -364,14 +371,45 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     h->pre_halo[s + 1] = h->pre_halo[s] + nh;
   }
   h->tot_subcell = h->pre_subcell[ns]; h->tot_halo = h->pre_halo[ns];
+  h->cspre.assign(nsolve + 1, 0);
   for (int b = 0; b < nblk; b++) {
     long long n = h->pre_cell[b + 1] - h->pre_cell[b];
     for (long long s0 = 0; s0 < n; s0 += 8192) h->cchunk.push_back(make_int4(b, (int)s0, (int)std::min<long long>(8192, n - s0), 0));
+    h->cspre[h->blk[b].solve + 1] = (int)h->cchunk.size();
   }
   for (int s = 0; s < ns; s++) {
     if (h->sub[s].bc != 2) continue;
     long long n = subcell_count(h->sub[s]);
     for (long long s0 = 0; s0 < n; s0 += 4096) h->wchunk.push_back(make_int4(s, (int)s0, (int)std::min<long long>(4096, n - s0), 0));
+  }
+  // boundary rounds: round r holds the r-th subface of every block (physical subfaces only); the
+  // cells of an entry are the subface's face cells (walls, symmetry) or its inclusive node range
+  // (far field, inflow, outflow, extrapolation), as the boundary kernels iterate them
+  {
+    int maxsub = 0;
+    for (const BlkD& B : h->blk) maxsub = std::max(maxsub, B.nsub);
+    for (int r = 0; r < maxsub; r++) {
+      int e0 = (int)h->bc_ent.size();
+      long long cells = 0;
+      for (int b = 0; b < nblk; b++) {
+        const BlkD& B = h->blk[b];
+        if (r >= B.nsub) continue;
+        const SubD& S = h->sub[B.sub0 + r];
+        if (S.bc <= 0) continue;
+        long long n;
+        if (S.bc == 4 || S.bc == 5 || S.bc == 6 || S.bc == 401)
+          n = (long long)(S.ie - S.ib + 1) * (S.je - S.jb + 1) * (S.ke - S.kb + 1);
+        else
+          n = subcell_count(S);
+        if (n <= 0) continue;
+        h->bc_pre.push_back(cells);
+        h->bc_ent.push_back(B.sub0 + r);
+        cells += n;
+      }
+      h->bc_pre.push_back(cells);  // closing entry of the round
+      h->bc_ent.push_back(-1);
+      h->bc_rounds.push_back(e0); h->bc_rounds.push_back((int)h->bc_ent.size() - 1); h->bc_rounds.push_back((int)cells);
+    }
   }
   // physical-face flags (set_BcK, sub_init.f90:545-577)
   std::vector<unsigned char> bci(obci, 0), bcj(obcj, 0), bck(obck, 0);
@@ -438,6 +476,9 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   h->d_pre_box = M.alloc<long long>(nblk + 1, e); h->d_pre_cell = M.alloc<long long>(nblk + 1, e);
   h->d_pre_face = M.alloc<long long>(nblk + 1, e); h->d_pre_col = M.alloc<long long>(nblk + 1, e);
   h->d_pre_subcell = M.alloc<long long>(ns + 1, e); h->d_pre_halo = M.alloc<long long>(ns + 1, e);
+  h->d_cspre = M.alloc<int>(nsolve + 1, e);
+  h->d_bc_ent = M.alloc<int>(std::max<size_t>(1, h->bc_ent.size()), e);
+  h->d_bc_pre = M.alloc<long long>(std::max<size_t>(1, h->bc_pre.size()), e);
   h->d_cchunk = M.alloc<int4>(h->cchunk.size(), e); h->d_wchunk = M.alloc<int4>(std::max<size_t>(1, h->wchunk.size()), e);
   h->d_x = M.alloc<double>(onode, e); h->d_y = M.alloc<double>(onode, e); h->d_z = M.alloc<double>(onode, e);
   h->d_Md = M.alloc<double>((size_t)M_COUNT * tf, e);
@@ -496,7 +537,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   if ((e = up(h->d_blk, h->blk)) || (e = up(h->d_sub, h->sub)) || (e = up(h->d_sp, h->sps)) ||
       (e = up(h->d_pre_box, h->pre_box)) || (e = up(h->d_pre_cell, h->pre_cell)) || (e = up(h->d_pre_face, h->pre_face)) ||
       (e = up(h->d_pre_col, h->pre_col)) || (e = up(h->d_pre_subcell, h->pre_subcell)) || (e = up(h->d_pre_halo, h->pre_halo)) ||
-      (e = up(h->d_cchunk, h->cchunk)) || (e = up(h->d_wchunk, h->wchunk)) || (e = up(h->d_x, hx)) || (e = up(h->d_y, hy)) ||
+      (e = up(h->d_cchunk, h->cchunk)) || (e = up(h->d_cspre, h->cspre)) || (e = up(h->d_bc_ent, h->bc_ent)) || (e = up(h->d_bc_pre, h->bc_pre)) || (e = up(h->d_wchunk, h->wchunk)) || (e = up(h->d_x, hx)) || (e = up(h->d_y, hy)) ||
       (e = up(h->d_z, hz)) || (e = up(h->d_bci, bci)) || (e = up(h->d_bcj, bcj)) || (e = up(h->d_bck, bck))) {
     M.release();
     return cuda_fail(nullptr, e, "upload");
@@ -580,6 +621,9 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   I.ncchunk = (int)h->cchunk.size(); I.nwchunk = (int)h->wchunk.size();
   I.lu_planes = std::getenv("OCFD_LUSGS_PLANES") ? 1 : 0;
   I.lu_version = lu_v2 ? 2 : 3;
+  I.bc_rounds = h->bc_rounds.data(); I.nround = (int)(h->bc_rounds.size() / 3);
+  I.recon_prim = 1;
+  for (int q = 0; q < nsolve; q++) if (ps[q].iflag_reconstruction != 0) I.recon_prim = 0;
   I.lu_tc = lu_tc;
   I.lu = &h->lu;
   {
@@ -843,7 +887,26 @@ extern "C" int ocfd_forces_all(ocfd_handle* h, double* ft, double* cl, double* c
 
 extern "C" void* ocfd_stream(ocfd_handle* h) { return h ? (void*)h->st : nullptr; }
 
-extern "C" int ocfd_launches_per_step(ocfd_handle* h) { return h ? h->run->launches_per_step() : 0; }
+// kernel nodes of the captured step graph (memset nodes excluded); without a graph, the count
+// the runner derives from its launch sequence
+extern "C" int ocfd_launches_per_step(ocfd_handle* h) {
+  if (!h) return 0;
+  if (ensure_graph(h) == OCFD_OK && h->graph) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(h->graph, nullptr, &n) == cudaSuccess && n > 0) {
+      std::vector<cudaGraphNode_t> nodes(n);
+      if (cudaGraphGetNodes(h->graph, nodes.data(), &n) == cudaSuccess) {
+        int k = 0;
+        for (size_t q = 0; q < n; q++) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+        }
+        return k;
+      }
+    }
+  }
+  return h->run->launches_per_step();
+}
 
 extern "C" int ocfd_profile(ocfd_handle* h, int nsteps, double* phase_ms) {
   if (!h || !phase_ms || nsteps < 1) return OCFD_ERR_ARG;

@@ -66,9 +66,15 @@ class RunnerT : public Runner {
       }
       k_amut<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
     }
-    k_inv_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
-    k_inv_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
-    k_inv_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+    if (I_.recon_prim) {
+      k_inv_flux<T, 0, true><<<grid_of(tf), 256, 0, st>>>(A);
+      k_inv_flux<T, 1, true><<<grid_of(tf), 256, 0, st>>>(A);
+      k_inv_flux<T, 2, true><<<grid_of(tf), 256, 0, st>>>(A);
+    } else {
+      k_inv_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
+      k_inv_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
+      k_inv_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+    }
     k_inv_kbc<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
     if (I_.viscous) {
       k_visc_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
@@ -106,7 +112,10 @@ class RunnerT : public Runner {
 
   void bc_halo(cudaStream_t st) override {
     const Arena<T>& A = A_;
-    k_bc<T, NV><<<A.nblk, 256, 0, st>>>(A);
+    for (int r = 0; r < I_.nround; r++) {
+      const int* R = I_.bc_rounds + 3 * r;
+      if (R[2] > 0) k_bc_round<T, NV><<<grid_of(R[2]), 256, 0, st>>>(A, R[0], R[1], (long long)R[2]);
+    }
     if (A.tot_halo > 0) k_halo<T, NV><<<grid_of(A.tot_halo), 256, 0, st>>>(A);
     k_corner<T, NV><<<A.nblk, 256, 0, st>>>(A);
   }
@@ -167,7 +176,9 @@ class RunnerT : public Runner {
     }
     int lu = I_.lu_planes ? 2 * (I_.max_plane - 2) : 2;
     int upd = 1 + 1 + (NV == 6 ? 3 : 0);
-    int bch = 2 + (A_.tot_halo > 0 ? 1 : 0);
+    int nbc = 0;
+    for (int r = 0; r < I_.nround; r++) nbc += I_.bc_rounds[3 * r + 2] > 0;
+    int bch = nbc + 1 + (A_.tot_halo > 0 ? 1 : 0);
     int n;
     if (I_.time_method == 0) n = res + lu + upd + bch;
     else n = 1 + 3 * (res + upd + bch);
@@ -182,7 +193,7 @@ class RunnerT : public Runner {
 
   void norms(cudaStream_t st, double* part, double* out, unsigned long long* nan_at) override {
     k_norms<T, NV><<<A_.ncchunk, 256, 0, st>>>(A_, part, nan_at);
-    k_norms_combine<T><<<(A_.nsolve + 63) / 64, 64, 0, st>>>(A_, part, out);
+    k_norms_combine<T><<<A_.nsolve, 128, 0, st>>>(A_, part, out);
   }
 
   void forces(cudaStream_t st, double* part) override {

@@ -18,6 +18,9 @@ struct RunInfo {
   int lu_grid;            // CTAs of the wavefront kernel
   int lu_version;         // 2: one thread per column; 3: four thread groups per column
   int lu_tc;              // columns per tile (32 or 64)
+  int recon_prim;         // 1: every solve reconstructs primitive variables
+  const int* bc_rounds;   // per boundary round: first entry, end entry, cells
+  int nround;
 };
 
 class Runner {

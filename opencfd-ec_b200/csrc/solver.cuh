@@ -474,11 +474,20 @@ __global__ void k_amut(Arena<T> A) {
   }
 }
 
+#ifndef INV_FLUX_MIXED_MINB
+#define INV_FLUX_MIXED_MINB 3
+#endif
 // ============================================================================================
 // inviscid fluxes (flux_inviscous_i/j/k, sub_Residual.f90:182-705)
 // ============================================================================================
-template <class T, int DIR>
-__global__ void k_inv_flux(Arena<T> A) {
+// FP64: at most 128 registers so two 256-thread CTAs share an SM (the kernel is bound by FP64
+// latency, not by memory); FP32: the compiler's choice
+template <class T>
+struct InvFluxOcc { static constexpr int value = sizeof(T) == 8 ? 2 : INV_FLUX_MIXED_MINB; };
+// PRIM: every solve of the handle reconstructs the primitive variables (IFlag_Reconstruction = 0),
+// so the conservative / characteristic branches are compiled out
+template <class T, int DIR, bool PRIM = false>
+__global__ void __launch_bounds__(256, InvFluxOcc<T>::value) k_inv_flux(Arena<T> A) {
   const long long tb = A.tot_box, tf = A.tot_face;
   OCFD_GRID_STRIDE(g, tf) {
     int b = find_blk(A.pre_face, A.nblk, g);
@@ -503,7 +512,7 @@ __global__ void k_inv_flux(Arena<T> A) {
     long long c0 = bix(B, i - 4 * di, j - 4 * dj, k - 4 * dk);
     const long long st = DIR == 0 ? 1 : (DIR == 1 ? (long long)B.NX : (long long)B.NX * B.NY);
     T UL[5], UR[5];
-    if (s.recon == 0) {
+    if (PRIM || s.recon == 0) {
       T u[8];
 #pragma unroll
       for (int m = 0; m < 5; m++) {
@@ -1083,105 +1092,102 @@ __device__ void wall_bound_d(const SolveP& s, double* U, long long tb, long long
   for (int m = 0; m < NV; m++) U[m * tb + c2] = Ug[m];
 }
 
+// Physical boundary conditions.  The reference applies the subfaces of a block one after the
+// other (ghost cells on edges are written by more than one subface, and far-field loops read
+// ghost cells written by earlier subfaces), so the work is issued in rounds: round r applies the
+// r-th subface of every block, all blocks and all cells of a subface in parallel, and the rounds
+// run in order.
 template <class T, int NV>
-__global__ void k_bc(Arena<T> A) {
-  const int b = blockIdx.x;
-  if (b >= A.nblk) return;
-  const BlkD& B = A.blk[b];
-  const SolveP& s = A.sp[B.solve];
+__device__ __forceinline__ void bc_cell(Arena<T>& A, const SubD& S, const BlkD& B, const SolveP& s, long long l) {
   const long long tb = A.tot_box, tf = A.tot_face;
   double* U = A.U;
-  for (int q = 0; q < B.nsub; q++) {
-    const SubD S = A.sub[B.sub0 + q];
-    if (S.bc <= 0) continue;
-    const int f = S.face;
-    if ((S.bc == 2 && s.viscous == 1)) {  // boundary_wall (87-147)
-      long long n = A.pre_subcell[B.sub0 + q + 1] - A.pre_subcell[B.sub0 + q];
-      for (long long l = threadIdx.x; l < n; l += blockDim.x) {
-        int i, j, k, gi, gj, gk;
-        subcell_ijk(S, l, i, j, k);
-        ghost_of(S, i, j, k, gi, gj, gk);
-        long long c1 = bix(B, i, j, k);
-        double dwv = NV == 7 ? (double)A.dwd[cix(B, i, j, k)] : 0.0;
-        wall_bound_d<NV>(s, U, tb, c1, bix(B, gi, gj, gk), (double)A.mu[c1], dwv);
-      }
-    } else if (S.bc == 4 || S.bc == 5 || S.bc == 6 || S.bc == 401) {  // far field / inflow / outflow / extrapolate (152-283, 458-504)
-      const int Flag = S.bc == 5 ? 2 : (S.bc == 6 ? 1 : 0);
-      int ni = S.ie - S.ib + 1, nj = S.je - S.jb + 1, nk = S.ke - S.kb + 1;
-      long long n = (long long)ni * nj * nk;
-      for (long long l = threadIdx.x; l < n; l += blockDim.x) {
-        int i = S.ib + (int)(l % ni), j = S.jb + (int)((l / ni) % nj), k = S.kb + (int)(l / ((long long)ni * nj));
-        int i1 = i, j1 = j, k1 = k, i2 = i, j2 = j, k2 = k;
-        double n1, n2, n3, sg = (f <= 3) ? -1.0 : 1.0;
-        if (f == 1) i2 = i - 1; else if (f == 2) j2 = j - 1; else if (f == 3) k2 = k - 1;
-        else if (f == 4) i1 = i - 1; else if (f == 5) j1 = j - 1; else k1 = k - 1;
-        int d = (f - 1) % 3;
-        long long fi = fix_(B, i, j, k);
-        n1 = A.Md[(M_NI1 + 3 * d) * tf + fi]; n2 = A.Md[(M_NI2 + 3 * d) * tf + fi]; n3 = A.Md[(M_NI3 + 3 * d) * tf + fi];
-        if (sg < 0) { n1 = -n1; n2 = -n2; n3 = -n3; }
-        long long c1 = bix(B, i1, j1, k1), c2 = bix(B, i2, j2, k2);
-        if (S.bc == 401) {
-          for (int m = 0; m < NV; m++) U[m * tb + c2] = U[m * tb + c1];
-          continue;
-        }
-        double gamma = s.gamma;
-        double d1 = U[c1], u1 = U[tb + c1] / d1, v1 = U[2 * tb + c1] / d1, w1 = U[3 * tb + c1] / d1;
-        double p1 = (U[4 * tb + c1] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1)) * (gamma - 1.0);
-        double c1s = sqrt(gamma * p1 / d1);
-        double d2, u2, v2, w2, p2, Ma_n = 0.0;
-        double d_inf = s.d_inf, u_inf = s.u_inf, v_inf = s.v_inf, w_inf = s.w_inf, p_inf = s.p_inf;
-        if (Flag == 1) { d2 = d1; u2 = u1; v2 = v1; w2 = w1; p2 = p1; }
-        else if (Flag == 2) { d2 = d_inf; u2 = u_inf; v2 = v_inf; w2 = w_inf; p2 = p_inf; }
-        else {
-          if (s.p_outlet <= -1.0) Ma_n = (u_inf * n1 + v_inf * n2 + w_inf * n3) * s.ma;
-          else Ma_n = (u1 * n1 + v1 * n2 + w1 * n3) / c1s;
-          if (Ma_n > 1.0) { d2 = d1; u2 = u1; v2 = v1; w2 = w1; p2 = p1; }
-          else if (Ma_n > -1.e-6) {
-            if (s.p_outlet > 0.0) {
-              double pb = s.p_outlet, db = d1 + (pb - p1) / (c1s * c1s);
-              double ub = u1 + (p1 - pb) / (d1 * c1s) * n1, vb = v1 + (p1 - pb) / (d1 * c1s) * n2, wb = w1 + (p1 - pb) / (d1 * c1s) * n3;
-              p2 = 2.0 * pb - p1; d2 = 2.0 * db - d1; u2 = 2.0 * ub - u1; v2 = 2.0 * vb - v1; w2 = 2.0 * wb - w1;
-            } else { d2 = d1; u2 = u1; v2 = v1; w2 = w1; p2 = p1; }
-          } else if (Ma_n > -1.0) {
-            double pb = 0.5 * (p1 + p_inf - d1 * c1s * ((u_inf - u1) * n1 + (v_inf - v1) * n2 + (w_inf - w1) * n3));
-            double db = d_inf + (pb - p_inf) / (c1s * c1s);
-            double ub = u_inf - (p_inf - pb) / (d1 * c1s) * n1, vb = v_inf - (p_inf - pb) / (d1 * c1s) * n2, wb = w_inf - (p_inf - pb) / (d1 * c1s) * n3;
-            p2 = 2.0 * pb - p1; d2 = 2.0 * db - d1; u2 = 2.0 * ub - u1; v2 = 2.0 * vb - v1; w2 = 2.0 * wb - w1;
-          } else { d2 = d_inf; u2 = u_inf; v2 = v_inf; w2 = w_inf; p2 = p_inf; }
-        }
-        U[c2] = d2; U[tb + c2] = d2 * u2; U[2 * tb + c2] = d2 * v2; U[3 * tb + c2] = d2 * w2;
-        U[4 * tb + c2] = p2 / (gamma - 1.0) + 0.5 * d2 * (u2 * u2 + v2 * v2 + w2 * w2);
-        if (Ma_n > 0.0 || Flag == 1) {
-          if (NV >= 6) U[5 * tb + c2] = U[5 * tb + c1];
-          if (NV == 7) U[6 * tb + c2] = U[6 * tb + c1];
-        } else {
-          if (NV == 6) U[5 * tb + c2] = 5.0;
-          if (NV == 7) { U[5 * tb + c2] = d_inf * s.kt_inf; U[6 * tb + c2] = d_inf * s.wt_inf; }
-        }
-      }
-    } else if (S.bc == 3 || S.bc == 2) {  // symmetry / slip wall (291-373)
-      long long n = A.pre_subcell[B.sub0 + q + 1] - A.pre_subcell[B.sub0 + q];
-      int d = (f - 1) % 3;
-      for (long long l = threadIdx.x; l < n; l += blockDim.x) {
-        int i, j, k, gi, gj, gk;
-        subcell_ijk(S, l, i, j, k);
-        ghost_of(S, i, j, k, gi, gj, gk);
-        // the normal is taken at the boundary node plane (i=ib or ie, ...)
-        int ni_ = i, nj_ = j, nk_ = k;
-        if (f == 4) ni_ = S.ie; else if (f == 5) nj_ = S.je; else if (f == 6) nk_ = S.ke;
-        long long fi = fix_(B, ni_, nj_, nk_);
-        double n1 = A.Md[(M_NI1 + 3 * d) * tf + fi], n2 = A.Md[(M_NI2 + 3 * d) * tf + fi], n3 = A.Md[(M_NI3 + 3 * d) * tf + fi];
-        long long c1 = bix(B, i, j, k), c2 = bix(B, gi, gj, gk);
-        for (int m = 0; m < NV; m++) U[m * tb + c2] = U[m * tb + c1];
-        double Vn = U[tb + c1] * n1 + U[2 * tb + c1] * n2 + U[3 * tb + c1] * n3;
-        U[tb + c2] = U[tb + c2] - 2.0 * Vn * n1;
-        U[2 * tb + c2] = U[2 * tb + c2] - 2.0 * Vn * n2;
-        U[3 * tb + c2] = U[3 * tb + c2] - 2.0 * Vn * n3;
-      }
-    } else {
-      if (threadIdx.x == 0) atomicOr(&A.flags[3 * A.nblk + b], 1);  // unsupported boundary type
+  const int f = S.face;
+  if ((S.bc == 2 && s.viscous == 1)) {  // boundary_wall (87-147)
+    int i, j, k, gi, gj, gk;
+    subcell_ijk(S, l, i, j, k);
+    ghost_of(S, i, j, k, gi, gj, gk);
+    long long c1 = bix(B, i, j, k);
+    double dwv = NV == 7 ? (double)A.dwd[cix(B, i, j, k)] : 0.0;
+    wall_bound_d<NV>(s, U, tb, c1, bix(B, gi, gj, gk), (double)A.mu[c1], dwv);
+  } else if (S.bc == 4 || S.bc == 5 || S.bc == 6 || S.bc == 401) {  // far field / inflow / outflow / extrapolate (152-283, 458-504)
+    const int Flag = S.bc == 5 ? 2 : (S.bc == 6 ? 1 : 0);
+    int ni = S.ie - S.ib + 1, nj = S.je - S.jb + 1;
+    int i = S.ib + (int)(l % ni), j = S.jb + (int)((l / ni) % nj), k = S.kb + (int)(l / ((long long)ni * nj));
+    int i1 = i, j1 = j, k1 = k, i2 = i, j2 = j, k2 = k;
+    double n1, n2, n3, sg = (f <= 3) ? -1.0 : 1.0;
+    if (f == 1) i2 = i - 1; else if (f == 2) j2 = j - 1; else if (f == 3) k2 = k - 1;
+    else if (f == 4) i1 = i - 1; else if (f == 5) j1 = j - 1; else k1 = k - 1;
+    int d = (f - 1) % 3;
+    long long fi = fix_(B, i, j, k);
+    n1 = A.Md[(M_NI1 + 3 * d) * tf + fi]; n2 = A.Md[(M_NI2 + 3 * d) * tf + fi]; n3 = A.Md[(M_NI3 + 3 * d) * tf + fi];
+    if (sg < 0) { n1 = -n1; n2 = -n2; n3 = -n3; }
+    long long c1 = bix(B, i1, j1, k1), c2 = bix(B, i2, j2, k2);
+    if (S.bc == 401) {
+      for (int m = 0; m < NV; m++) U[m * tb + c2] = U[m * tb + c1];
+      return;
     }
-    __syncthreads();
+    double gamma = s.gamma;
+    double d1 = U[c1], u1 = U[tb + c1] / d1, v1 = U[2 * tb + c1] / d1, w1 = U[3 * tb + c1] / d1;
+    double p1 = (U[4 * tb + c1] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1)) * (gamma - 1.0);
+    double c1s = sqrt(gamma * p1 / d1);
+    double d2, u2, v2, w2, p2, Ma_n = 0.0;
+    double d_inf = s.d_inf, u_inf = s.u_inf, v_inf = s.v_inf, w_inf = s.w_inf, p_inf = s.p_inf;
+    if (Flag == 1) { d2 = d1; u2 = u1; v2 = v1; w2 = w1; p2 = p1; }
+    else if (Flag == 2) { d2 = d_inf; u2 = u_inf; v2 = v_inf; w2 = w_inf; p2 = p_inf; }
+    else {
+      if (s.p_outlet <= -1.0) Ma_n = (u_inf * n1 + v_inf * n2 + w_inf * n3) * s.ma;
+      else Ma_n = (u1 * n1 + v1 * n2 + w1 * n3) / c1s;
+      if (Ma_n > 1.0) { d2 = d1; u2 = u1; v2 = v1; w2 = w1; p2 = p1; }
+      else if (Ma_n > -1.e-6) {
+        if (s.p_outlet > 0.0) {
+          double pb = s.p_outlet, db = d1 + (pb - p1) / (c1s * c1s);
+          double ub = u1 + (p1 - pb) / (d1 * c1s) * n1, vb = v1 + (p1 - pb) / (d1 * c1s) * n2, wb = w1 + (p1 - pb) / (d1 * c1s) * n3;
+          p2 = 2.0 * pb - p1; d2 = 2.0 * db - d1; u2 = 2.0 * ub - u1; v2 = 2.0 * vb - v1; w2 = 2.0 * wb - w1;
+        } else { d2 = d1; u2 = u1; v2 = v1; w2 = w1; p2 = p1; }
+      } else if (Ma_n > -1.0) {
+        double pb = 0.5 * (p1 + p_inf - d1 * c1s * ((u_inf - u1) * n1 + (v_inf - v1) * n2 + (w_inf - w1) * n3));
+        double db = d_inf + (pb - p_inf) / (c1s * c1s);
+        double ub = u_inf - (p_inf - pb) / (d1 * c1s) * n1, vb = v_inf - (p_inf - pb) / (d1 * c1s) * n2, wb = w_inf - (p_inf - pb) / (d1 * c1s) * n3;
+        p2 = 2.0 * pb - p1; d2 = 2.0 * db - d1; u2 = 2.0 * ub - u1; v2 = 2.0 * vb - v1; w2 = 2.0 * wb - w1;
+      } else { d2 = d_inf; u2 = u_inf; v2 = v_inf; w2 = w_inf; p2 = p_inf; }
+    }
+    U[c2] = d2; U[tb + c2] = d2 * u2; U[2 * tb + c2] = d2 * v2; U[3 * tb + c2] = d2 * w2;
+    U[4 * tb + c2] = p2 / (gamma - 1.0) + 0.5 * d2 * (u2 * u2 + v2 * v2 + w2 * w2);
+    if (Ma_n > 0.0 || Flag == 1) {
+      if (NV >= 6) U[5 * tb + c2] = U[5 * tb + c1];
+      if (NV == 7) U[6 * tb + c2] = U[6 * tb + c1];
+    } else {
+      if (NV == 6) U[5 * tb + c2] = 5.0;
+      if (NV == 7) { U[5 * tb + c2] = d_inf * s.kt_inf; U[6 * tb + c2] = d_inf * s.wt_inf; }
+    }
+  } else {  // symmetry / slip wall (291-373)
+    int d = (f - 1) % 3;
+    int i, j, k, gi, gj, gk;
+    subcell_ijk(S, l, i, j, k);
+    ghost_of(S, i, j, k, gi, gj, gk);
+    // the normal is taken at the boundary node plane (i=ib or ie, ...)
+    int ni_ = i, nj_ = j, nk_ = k;
+    if (f == 4) ni_ = S.ie; else if (f == 5) nj_ = S.je; else if (f == 6) nk_ = S.ke;
+    long long fi = fix_(B, ni_, nj_, nk_);
+    double n1 = A.Md[(M_NI1 + 3 * d) * tf + fi], n2 = A.Md[(M_NI2 + 3 * d) * tf + fi], n3 = A.Md[(M_NI3 + 3 * d) * tf + fi];
+    long long c1 = bix(B, i, j, k), c2 = bix(B, gi, gj, gk);
+    for (int m = 0; m < NV; m++) U[m * tb + c2] = U[m * tb + c1];
+    double Vn = U[tb + c1] * n1 + U[2 * tb + c1] * n2 + U[3 * tb + c1] * n3;
+    U[tb + c2] = U[tb + c2] - 2.0 * Vn * n1;
+    U[2 * tb + c2] = U[2 * tb + c2] - 2.0 * Vn * n2;
+    U[3 * tb + c2] = U[3 * tb + c2] - 2.0 * Vn * n3;
+  }
+}
+
+// one round: entries e0..e1-1 of the boundary work list (subface, cells), ncell cells in total
+template <class T, int NV>
+__global__ void k_bc_round(Arena<T> A, int e0, int e1, long long ncell) {
+  OCFD_GRID_STRIDE(g, ncell) {
+    const long long gg = A.bc_pre[e0] + g;
+    const int e = e0 + find_blk(A.bc_pre + e0, e1 - e0, gg);
+    const SubD S = A.sub[A.bc_ent[e]];
+    const BlkD& B = A.blk[S.blk];
+    bc_cell<T, NV>(A, S, B, A.sp[B.solve], gg - A.bc_pre[e]);
   }
 }
 
@@ -1307,17 +1313,29 @@ __global__ void k_norms(Arena<T> A, double* part, unsigned long long* nan_at) {
     part[(long long)blockIdx.x * 14 + 7 + threadIdx.x] = ssum[threadIdx.x][0];
   }
 }
-// per solve: max / sum over chunks in chunk order
+// per solve (one CTA each): every thread folds a fixed stride of the solve's chunks in order,
+// then a fixed tree over the threads -- the same order whatever else the handle holds
 template <class T>
 __global__ void k_norms_combine(Arena<T> A, const double* part, double* out) {
-  int sv = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sv >= A.nsolve) return;
+  __shared__ double smx[7][128], ssm[7][128];
+  const int sv = blockIdx.x, c0 = A.cspre[sv], c1 = A.cspre[sv + 1];
   double mx[7] = {0, 0, 0, 0, 0, 0, 0}, sm[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int c = 0; c < A.ncchunk; c++) {
-    if (A.blk[A.cchunk[c].x].solve != sv) continue;
+  for (int c = c0 + (int)threadIdx.x; c < c1; c += blockDim.x)
+#pragma unroll
     for (int m = 0; m < 7; m++) { mx[m] = fmax(mx[m], part[c * 14 + m]); sm[m] = sm[m] + part[c * 14 + 7 + m]; }
+#pragma unroll
+  for (int m = 0; m < 7; m++) { smx[m][threadIdx.x] = mx[m]; ssm[m][threadIdx.x] = sm[m]; }
+  __syncthreads();
+  for (int w = 64; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+#pragma unroll
+      for (int m = 0; m < 7; m++) {
+        smx[m][threadIdx.x] = fmax(smx[m][threadIdx.x], smx[m][threadIdx.x + w]);
+        ssm[m][threadIdx.x] = ssm[m][threadIdx.x] + ssm[m][threadIdx.x + w];
+      }
+    __syncthreads();
   }
-  for (int m = 0; m < 7; m++) { out[sv * 14 + m] = mx[m]; out[sv * 14 + 7 + m] = sm[m]; }
+  if (threadIdx.x < 7) { out[sv * 14 + threadIdx.x] = smx[threadIdx.x][0]; out[sv * 14 + 7 + threadIdx.x] = ssm[threadIdx.x][0]; }
 }
 
 // ============================================================================================

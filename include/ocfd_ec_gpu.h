@@ -223,6 +223,22 @@ long long ocfd_footprint(const ocfd_params* p, int nblk, const int* nijk);
  * work on the device. */
 int ocfd_synchronize(ocfd_handle* h);
 
+/* ---- allocation-free monitoring (no counterpart in the reference) ------------------------ */
+
+/*
+ * ocfd_residual for solve 0 that allocates nothing, neither device nor host heap memory: for
+ * callers that must not allocate inside their iteration loop (a driver whose device memory is
+ * fully committed to resident solves, or a monitor that must not touch an allocator while the
+ * solver runs).  Its scratch is one static device area per device, shared by all handles of the
+ * process: at most 33,554,432 interior cells (4096 chunks of 8192) and 256 solves per handle;
+ * larger handles get OCFD_ERR_ARG with a message (use ocfd_residual).  The first call on a device
+ * looks the area up (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture.  Calls that overlap in time (other threads, other handles on the same
+ * device) race on the shared area and must be serialised by the caller.  On a NaN it returns
+ * OCFD_ERR_NAN without the cell location (ocfd_residual reports it).
+ */
+int ocfd_residual_static(ocfd_handle* h, double* res_max, double* res_rms);
+
 /* Library build/ABI information: "ocfd-b200 <abi> sm_100a ..." */
 const char* ocfd_version(void);
 

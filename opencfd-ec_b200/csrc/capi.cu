@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -297,6 +298,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   if (int rc = check_params(ps, nsolve)) return rc;
   std::unique_ptr<ocfd_handle> hp(new ocfd_handle());
   ocfd_handle* h = hp.get();
+  h->err.reserve(512);
   const ocfd_params* p = ps;
   h->P = ps[0];
   h->Ps.assign(ps, ps + nsolve);
@@ -838,6 +840,80 @@ extern "C" int ocfd_residual(ocfd_handle* h, double* rmax, double* rrms) {
 extern "C" int ocfd_residual_all(ocfd_handle* h, double* rmax, double* rrms) {
   if (!h || !rmax || !rrms) return OCFD_ERR_ARG;
   return residual_impl(h, rmax, rrms, h->nsolve);
+}
+
+// ---- residual norms without any allocation --------------------------------------------------
+// ocfd_residual_static uses one statically sized device area per device, shared by every handle
+// of the process: per-chunk partial max / sum of squares, per-solve totals, and the NaN location.
+// Each call overwrites all partials and totals it reads; only the NaN location must start at its
+// sentinel (all ones), which the call resets on the handle's stream before the norm kernels.
+constexpr int kStaticNormChunks = 4096;  // 8192 cells per chunk: up to 33,554,432 interior cells
+constexpr int kStaticNormSolves = 256;
+static __device__ __align__(256) double g_static_norm[(kStaticNormChunks + kStaticNormSolves) * 14];
+static __device__ __align__(256) unsigned long long g_static_nan;
+
+__global__ void k_static_nan_reset(unsigned long long* nan_at) { *nan_at = ~0ULL; }
+
+namespace {
+struct StaticNormArea {
+  double* part = nullptr;
+  double* out = nullptr;
+  unsigned long long* nan = nullptr;
+};
+constexpr int kMaxDevices = 64;
+StaticNormArea g_static_area[kMaxDevices];
+std::mutex g_static_mu;
+}  // namespace
+
+// device addresses of the static area on the current device (looked up once per device)
+static int static_norm_area(ocfd_handle* h, StaticNormArea& a) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(h, e, "residual_static: cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(h, OCFD_ERR_ARG, "residual_static: device ordinal beyond 63");
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  StaticNormArea& c = g_static_area[dev];
+  if (!c.part) {
+    void* p = nullptr;
+    void* n = nullptr;
+    if ((e = cudaGetSymbolAddress(&p, g_static_norm)) != cudaSuccess) return cuda_fail(h, e, "residual_static: cudaGetSymbolAddress");
+    if ((e = cudaGetSymbolAddress(&n, g_static_nan)) != cudaSuccess) return cuda_fail(h, e, "residual_static: cudaGetSymbolAddress");
+    c.part = (double*)p;
+    c.out = (double*)p + (size_t)kStaticNormChunks * 14;
+    c.nan = (unsigned long long*)n;
+  }
+  a = c;
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_residual_static(ocfd_handle* h, double* rmax, double* rrms) {
+  if (!h || !rmax || !rrms) return OCFD_ERR_ARG;
+  if ((long long)h->cchunk.size() > kStaticNormChunks)
+    return fail(h, OCFD_ERR_ARG, "residual_static: the handle has more than 33,554,432 interior cells (4096 chunks); use ocfd_residual");
+  if (h->nsolve > kStaticNormSolves) return fail(h, OCFD_ERR_ARG, "residual_static: the handle has more than 256 solves; use ocfd_residual");
+  StaticNormArea a;
+  if (int rc = static_norm_area(h, a)) return rc;
+  k_static_nan_reset<<<1, 1, 0, h->st>>>(a.nan);
+  h->run->norms(h->st, a.part, a.out, a.nan);
+  double out[14];
+  unsigned long long nan_at = 0;
+  int lu_err = 0;
+  cudaMemcpyAsync(out, a.out, sizeof(out), cudaMemcpyDeviceToHost, h->st);
+  cudaMemcpyAsync(&nan_at, a.nan, 8, cudaMemcpyDeviceToHost, h->st);
+  cudaMemcpyAsync(&lu_err, h->d_lu_err, 4, cudaMemcpyDeviceToHost, h->st);
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "residual_static");
+  for (int m = 0; m < 7; m++) {
+    rmax[m] = m < h->nvar ? out[m] : 0.0;
+    rrms[m] = m < h->nvar ? std::sqrt(out[7 + m] / (double)h->ncell_s[0]) : 0.0;
+  }
+  if (lu_err) {
+    cudaMemsetAsync(h->d_lu_err, 0, 4, h->st);
+    cudaStreamSynchronize(h->st);
+    return fail(h, OCFD_ERR_TIMEOUT, "LU-SGS wavefront: a bounded wait between tiles timed out");
+  }
+  if (nan_at != ~0ULL) return fail(h, OCFD_ERR_NAN, "NaN in residual (location: ocfd_residual)");
+  return OCFD_OK;
 }
 
 // forces of every solve: partial sums per wall chunk, then per block in subface order, then over

@@ -20,7 +20,7 @@ EXPORTED = [
     "ocfd_set_state", "ocfd_get_state", "ocfd_init_flow", "ocfd_advance", "ocfd_residual", "ocfd_forces",
     "ocfd_limiter_status", "ocfd_array_shape", "ocfd_get_array", "ocfd_version", "ocfd_compute_residual",
     "ocfd_stream", "ocfd_profile", "ocfd_launches_per_step", "ocfd_create_batch", "ocfd_nsolve",
-    "ocfd_residual_all", "ocfd_forces_all", "ocfd_footprint", "ocfd_synchronize",
+    "ocfd_residual_all", "ocfd_forces_all", "ocfd_footprint", "ocfd_synchronize", "ocfd_residual_static",
 ]
 
 
@@ -68,6 +68,7 @@ def lib():
         L.ocfd_footprint.argtypes = [pp, ctypes.c_int, ip]
         L.ocfd_footprint.restype = ctypes.c_longlong
         L.ocfd_synchronize.argtypes = [vp]
+        L.ocfd_residual_static.argtypes = [vp, dp, dp]
         _lib = L
     return _lib
 
@@ -157,6 +158,15 @@ class Solver:
         if rc == OCFD_ERR_NAN:
             raise FloatingPointError(lib().ocfd_last_error(self.h).decode())
         self._check(rc, "residual")
+        return a, b
+
+    def residual_static(self):
+        """ocfd_residual without any allocation (static device scratch, see the header)."""
+        a, b = np.zeros(7), np.zeros(7)
+        rc = lib().ocfd_residual_static(self.h, _dp(a), _dp(b))
+        if rc == OCFD_ERR_NAN:
+            raise FloatingPointError(lib().ocfd_last_error(self.h).decode())
+        self._check(rc, "residual_static")
         return a, b
 
     def forces(self):

@@ -168,6 +168,74 @@ def cpu_sample(args, min_seconds=10.0, max_steps=50):
     return case.ncells * n / el, threads, "%s, %d LU-SGS step(s) after 1 warm-up, %.1f s on %d host threads" % (case.name, n, el, threads)
 
 
+def event_ms(s, nsteps):
+    """Device time (ms) of nsteps steps of handle s, CUDA events on the handle's stream."""
+    import torch
+    st = torch.cuda.ExternalStream(s.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    s.advance(nsteps)
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def mixed_leg(args, rank, cl64, cd64):
+    """The same workload in mixed precision (FP32 reconstruction / fluxes / sources / metrics, FP64
+    state, LU-SGS diagonal, norms, forces): rate and CL / CD error against the FP64 run after the
+    same number of steps (1 count = 1e-4)."""
+    from ocfd_b200 import capi, cases
+    p, case = getattr(cases, args.workload)(precision=1, aoa=rank_aoa(rank))
+    s = capi.Solver(p, case)
+    s.advance(args.warmup)
+    s.synchronize()
+    ms = event_ms(s, args.steps)
+    _, cl, cd, _ = s.forces()
+    s.close()
+    return {"value": case.ncells * args.steps / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms / args.steps,
+            "dCL_counts": abs(cl - cl64) * 1e4, "dCD_counts": abs(cd - cd64) * 1e4, "steps": args.warmup + args.steps}
+
+
+def batch_leg(args, nsteps=100):
+    """Config 4: 64 independent 2-D-extruded airfoil solves (O-meshes 129x33 .. 385x97, SA,
+    AUSMPW + MUSCL3, mixed precision) in one handle: one step graph covers all 64."""
+    from ocfd_b200 import capi, cases
+    items = cases.config4_batch(n=64)
+    cells = sum(c.ncells for _, c in items)
+    b = capi.Batch(items)
+    b.advance(args.warmup)
+    b.synchronize()
+    n = min(args.steps, nsteps)
+    ms = event_ms(b, n)
+    launches = b.launches_per_step()
+    b.close()
+    return {"workload": "config4: 64 NACA 4-digit O-mesh airfoils (k=3), SA, AUSMPW+MUSCL3, mixed, seed 1234",
+            "cells": cells, "value": cells * n / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms / n,
+            "steps": n, "launches_per_step": launches}
+
+
+def serving_leg(max_iters=1500, n=14, rate=2.0):
+    """Continuous batching: Poisson arrivals (rate/s) of seeded airfoil solves (config 4 sizes) and
+    reduced swept wings, run to a 1e-6 residual drop or |dCL| < 1e-4 over 200 iterations (at most
+    max_iters); p50 / p99 time from arrival to convergence, beside the same requests run one at a
+    time in plain FP64."""
+    from ocfd_b200 import cases, serve
+    def items(precision):
+        its = cases.config4_batch(n=n - 2, seed=77, precision=precision)
+        its.append(cases.config2_medium(precision=precision, aoa=2.0))
+        its.append(cases.config2_small(precision=precision, aoa=4.0))
+        return its
+    out = {}
+    for name, prec, max_active in (("mixed_continuous", 1, 32), ("fp64_one_at_a_time", 0, 1)):
+        reqs = serve.poisson_requests(items(prec), rate=rate, seed=2024, max_iters=max_iters)
+        t0 = time.perf_counter()
+        res = serve.Server(max_active=max_active, chunk=50).run(reqs)
+        out[name] = serve.summarize(res, time.perf_counter() - t0)
+    out["workload"] = "%d requests, Poisson %.1f/s: %d config-4 airfoils + config2_medium + config2_small wings, max %d iterations" % (
+        n, rate, n - 2, max_iters)
+    return out
+
+
 def run_reference(args, budget_s=150.0):
     """The reference arm: the CPU restatement of the reference algorithm (oracle/, FP64, all host
     threads) on the same workload, rank 0 only.  Times args.steps full steps, or as many as fit
@@ -215,6 +283,7 @@ def main():
                     help="config2 (the headline case); the others are for profiler captures")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-extra", action="store_true", help="skip the mixed-precision, batch and serving legs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -259,6 +328,7 @@ def main():
     barrier()
     ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
     rmax, rrms = s.residual()
+    _, cl64, cd64, _ = s.forces()
     ncell = case.ncells
     value = aggregate_rate(world, ncell * args.steps, ms)
 
@@ -315,6 +385,14 @@ def main():
     launches = s.launches_per_step() * args.steps
     s.close()
 
+    extra = {}
+    if not args.no_extra and args.precision == "fp64":
+        extra["mixed"] = mixed_leg(args, rank, cl64, cd64)
+        extra["mixed"]["speedup_vs_fp64"] = (ms / args.steps) / extra["mixed"]["ms_per_step"]
+        if world == 1:
+            extra["batch"] = batch_leg(args)
+            extra["serving"] = serving_leg()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -336,8 +414,9 @@ def main():
                        "precision": prec, "parallelism": "replicas x%d (independent solves, no collective)" % world,
                        "l2": "working set %.1f GB > 126 MB L2 (no flush needed)" % (ncell * 1200 / 1e9)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk.summary(), "residual_rms": rrms[: s.nvar].tolist(),
+            "clocks": clk.summary(), "residual_rms": rrms[: s.nvar].tolist(), "cl": cl64, "cd": cd64,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     return 0
 

@@ -44,6 +44,12 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
   asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -283,15 +289,22 @@ template <int NT>
 __device__ __forceinline__ void cta_bar() { asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory"); }
 __device__ __forceinline__ double ldro(const float* p) { return (double)__ldg(p); }
 
+#ifndef OCFD_LU_MINB
+#define OCFD_LU_MINB (64 / TC)
+#endif
 template <class T, int NV, bool UPPER, int TC>
-__global__ void __launch_bounds__(4 * TC, 64 / TC) k_lusgs_wave3(Arena<T> A, LuArgs L) {
+__global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena<T> A, LuArgs L) {
   __shared__ int s_tile;
   __shared__ double s_acc[3][NV][TC];      // direction terms of the current step
-  __shared__ double s_pub[NV + 1][TC];     // DU and p(U+DU) of each column's last cell
+  __shared__ double s_pub[NV][TC];         // DU of each column's last cell
   __shared__ double s_old[2][NV + 6][TC];  // old state U, Lc(3), Lv(3) of each column's cell, by step parity
+  __shared__ double s_diag[NV + 2][TC];    // R (NV) and the diagonal (all variables; the SA variable's) of the current step
   const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
   const int TJ = L.TJ, TK = L.TK;
-  const int tid = threadIdx.x, grp = tid / TC, c = tid % TC;
+  // thread groups: 0..2 direction threads, 3 owner (TC threads each), 4 the poller warp (lane 0
+  // publishes this tile's progress and waits for the upstream tiles')
+  constexpr int NT = 4 * TC + 32;
+  const int tid = threadIdx.x, grp = tid < 4 * TC ? tid / TC : 4, c = tid % TC;
   const int lj = c % TJ, lk = c / TJ;
   const bool owner = grp == 3;
   const int d = grp;  // direction of a direction thread
@@ -432,62 +445,72 @@ __global__ void __launch_bounds__(4 * TC, 64 / TC) k_lusgs_wave3(Arena<T> A, LuA
 
     // The owner warps and the direction warps run separate loops (so each keeps only its own
     // registers live); both take the same two CTA barriers per step.
-    if (owner) {
-      if (on_at(0)) { load_own(0, on); prep_own(on); }
+    //   phase A (after B1): direction threads evaluate their flux-difference term (the dependency
+    //     chain); the owner prepares the cell's diagonal and R (off the chain) and prefetches.
+    //   phase B (after B2): the final divisions are shared: direction thread d computes DU of
+    //     variable d, the owner the variables 3..NV-1; direction threads then prepare the next
+    //     step's old-state terms, and thread 0 completes the poll of the upstream tiles.
+    auto diag_of = [&](int m) { return (NV == 6 && m == 5) ? s_diag[NV + 1][c] : s_diag[NV][c]; };
+    auto finish = [&](int m, long long ci) {  // sub_LU_SGS.f90:63-72 (lower), 108-117 (upper)
+      double r;
+      if (!UPPER) r = (s_diag[m][c] + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      else r = s_diag[m][c] + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      A.DU[m * tc + ci] = r;
+      s_pub[m][c] = r;
+    };
+    if (grp == 4) {
+      // poller warp: its flag traffic (release of this tile's progress after B1, acquire of the
+      // upstream tiles' progress) never sits on the compute warps' paths
+      if (tid == 4 * TC) poll(0);
       for (int t = 0; t < nsteps; t++) {
-        cta_bar<4 * TC>();  // B1
-        if (on_at(t)) {  // publish this step's old state for the downstream cells' next step
+        cta_bar<NT>();  // B1
+        if (tid == 4 * TC && t > 0) st_release(L.progress + my, t);
+        cta_bar<NT>();  // B2
+        if (tid == 4 * TC && t + 1 < nsteps) poll(t + 1);
+      }
+    } else if (owner) {
+      if (on_at(0)) load_own(0, on);
+      for (int t = 0; t < nsteps; t++) {
+        cta_bar<NT>();  // B1
+        if (on_at(t)) {
+          prep_own(on);
 #pragma unroll
-          for (int m = 0; m < NV; m++) s_old[t & 1][m][c] = oU[m];
+          for (int m = 0; m < NV; m++) { s_old[t & 1][m][c] = oU[m]; s_diag[m][c] = oR[m]; }
 #pragma unroll
           for (int q2 = 0; q2 < 6; q2++) s_old[t & 1][NV + q2][c] = oL[q2];
+          s_diag[NV][c] = alfa[0];
+          s_diag[NV + 1][c] = alfa[NV - 1];
         }
         if (on_at(t + 1)) load_own(t + 1, on);
-        cta_bar<4 * TC>();  // B2: the three direction terms of step t are in shared memory
+        cta_bar<NT>();  // B2: the three direction terms of step t are in shared memory
         if (on_at(t)) {
           const long long ci = cix(B, i_of(t), j, k);
-          double U2[5];
 #pragma unroll
-          for (int m = 0; m < NV; m++) {
-            double r;
-            if (!UPPER) r = (oR[m] + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / alfa[m];
-            else r = oR[m] + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / alfa[m];
-            A.DU[m * tc + ci] = r;
-            s_pub[m][c] = r;
-            if (m < 5) U2[m] = oU[m] + r;
-          }
-          s_pub[NV][c] = (gamma - 1.0) * (U2[4] - 0.5 * (sq(U2[1]) + sq(U2[2]) + sq(U2[3])) / U2[0]);
+          for (int m = 3; m < NV; m++) finish(m, ci);
         }
-        if (on_at(t + 1)) prep_own(on);
       }
     } else {
       if (on_at(0) && has_at(0)) load_dir(0, dn);
       prep_dir(0, dn);
-      if (tid == 0) poll(0);
       for (int t = 0; t < nsteps; t++) {
-        cta_bar<4 * TC>();  // B1: step t-1 finished (DU in s_pub and in HBM), upstream tiles ready
-        if (tid == 0 && t > 0) st_release(L.progress + my, t);
+        cta_bar<NT>();  // B1: step t-1 finished (DU in s_pub and in HBM), upstream tiles ready
         if (on_at(t + 1) && has_at(t + 1)) load_dir(t + 1, dn);
         if (has) {
-          double DUn[NV], pp2;
+          double DUn[NV];
           if (!xt) {
 #pragma unroll
             for (int m = 0; m < NV; m++) DUn[m] = s_pub[m][pubcol];
-            pp2 = s_pub[NV][pubcol];
           } else {
             const int i = i_of(t);
             const long long cn = cix(B, i, j + (d == 1 ? off : 0), k + (d == 2 ? off : 0));
 #pragma unroll
             for (int m = 0; m < NV; m++) DUn[m] = __ldcg(A.DU + m * tc + cn);
-            double V2[5];
-#pragma unroll
-            for (int m = 0; m < 5; m++) V2[m] = Unb[m] + DUn[m];
-            pp2 = (gamma - 1.0) * (V2[4] - 0.5 * (sq(V2[1]) + sq(V2[2]) + sq(V2[3])) / V2[0]);
           }
           double U2[NV];
 #pragma unroll
           for (int m = 0; m < NV; m++) U2[m] = Unb[m] + DUn[m];
           const double un2 = (U2[1] * n1 + U2[2] * n2 + U2[3] * n3) / U2[0];
+          const double pp2 = (gamma - 1.0) * (U2[4] - 0.5 * (sq(U2[1]) + sq(U2[2]) + sq(U2[3])) / U2[0]);
           double DF[NV];
           DF[0] = U2[0] * un2 - F1[0];
           DF[1] = (U2[1] * un2 + pp2 * n1) - F1[1];
@@ -508,9 +531,9 @@ __global__ void __launch_bounds__(4 * TC, 64 / TC) k_lusgs_wave3(Arena<T> A, LuA
 #pragma unroll
           for (int m = 0; m < NV; m++) s_acc[d][m][c] = 0.0;
         }
-        cta_bar<4 * TC>();  // B2
+        cta_bar<NT>();  // B2
+        if (on_at(t)) finish(d, cix(B, i_of(t), j, k));
         prep_dir(t + 1, dn);
-        if (tid == 0 && t + 1 < nsteps) poll(t + 1);
       }
     }
     __syncthreads();

@@ -101,11 +101,11 @@ class RunnerT : public Runner {
         if (!upper) k_lusgs_wave<T, NV, false><<<I_.lu_grid, 64, 0, st>>>(A, L_);
         else k_lusgs_wave<T, NV, true><<<I_.lu_grid, 64, 0, st>>>(A, L_);
       } else if (I_.lu_tc == 64) {
-        if (!upper) k_lusgs_wave3<T, NV, false, 64><<<I_.lu_grid, 256, 0, st>>>(A, L_);
-        else k_lusgs_wave3<T, NV, true, 64><<<I_.lu_grid, 256, 0, st>>>(A, L_);
+        if (!upper) k_lusgs_wave3<T, NV, false, 64><<<I_.lu_grid, 4 * 64 + 32, 0, st>>>(A, L_);
+        else k_lusgs_wave3<T, NV, true, 64><<<I_.lu_grid, 4 * 64 + 32, 0, st>>>(A, L_);
       } else {
-        if (!upper) k_lusgs_wave3<T, NV, false, 32><<<I_.lu_grid, 128, 0, st>>>(A, L_);
-        else k_lusgs_wave3<T, NV, true, 32><<<I_.lu_grid, 128, 0, st>>>(A, L_);
+        if (!upper) k_lusgs_wave3<T, NV, false, 32><<<I_.lu_grid, 4 * 32 + 32, 0, st>>>(A, L_);
+        else k_lusgs_wave3<T, NV, true, 32><<<I_.lu_grid, 4 * 32 + 32, 0, st>>>(A, L_);
       }
     }
   }

@@ -214,6 +214,30 @@ def batch_leg(args, nsteps=100):
             "steps": n, "launches_per_step": launches}
 
 
+def config3_leg(args, nsteps=20):
+    """Config 3 stand-in (SST swept wing, 24 uneven blocks, ~7.8 M cells, MUSCL3 + Roe): FP64 and
+    mixed LU-SGS rates over the same steps, CL / CD error of mixed against FP64 in counts, and the
+    RK3 variant's rate (CFL 0.5)."""
+    from ocfd_b200 import capi, cases
+    out, forces = {}, {}
+    for name, over in (("fp64", dict(precision=0)), ("mixed", dict(precision=1)), ("rk3_mixed", dict(precision=1, time_method=3, cfl=0.5))):
+        p, case = cases.config3(**over)
+        s = capi.Solver(p, case)
+        s.advance(args.warmup)
+        s.synchronize()
+        ms = event_ms(s, nsteps)
+        _, cl, cd, _ = s.forces()
+        forces[name] = (cl, cd)
+        out[name] = {"value": case.ncells * nsteps / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms / nsteps}
+        s.close()
+    out["workload"] = "%s RANS-SST MUSCL3+Roe, %d blocks, %d cells, %d steps after %d warm-up" % (
+        case.name, len(case.dims), case.ncells, nsteps, args.warmup)
+    out["mixed"]["dCL_counts"] = abs(forces["mixed"][0] - forces["fp64"][0]) * 1e4
+    out["mixed"]["dCD_counts"] = abs(forces["mixed"][1] - forces["fp64"][1]) * 1e4
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
+
+
 def serving_leg(max_iters=1500, n=14, rate=2.0):
     """Continuous batching: Poisson arrivals (rate/s) of seeded airfoil solves (config 4 sizes) and
     reduced swept wings, run to a 1e-6 residual drop or |dCL| < 1e-4 over 200 iterations (at most
@@ -391,6 +415,7 @@ def main():
         extra["mixed"]["speedup_vs_fp64"] = (ms / args.steps) / extra["mixed"]["ms_per_step"]
         if world == 1:
             extra["batch"] = batch_leg(args)
+            extra["config3"] = config3_leg(args)
             extra["serving"] = serving_leg()
 
     cpu = None

@@ -193,7 +193,7 @@ def airfoil_omesh(ni=129, nj=33, nk=3, m=0.0, p=0.0, t=0.12, radius=20.0, ds=2e-
 
 
 def swept_wing(ni=257, nj=97, nk_wing=61, nk_tip=26, i_cut=49, sweep_deg=30.0, taper=0.56,
-               semi_span=1.5, radius=20.0, ds=4.5e-6, tip_far=15.0, name="wing"):
+               semi_span=1.5, radius=20.0, ds=4.5e-6, tip_far=15.0, name="wing", j_cuts=()):
     """Config 2 stand-in: O-H mesh around a swept, tapered NACA 0012 wing.
 
     i runs around each spanwise section (O-type, periodic trailing-edge seam), j from the wall
@@ -202,7 +202,8 @@ def swept_wing(ni=257, nj=97, nk_wing=61, nk_tip=26, i_cut=49, sweep_deg=30.0, t
     and on to a far field `tip_far` chords beyond the tip (nk_tip nodes).  Beyond the tip the
     section collapses to its chord line and the j=1 surface becomes a sheet joining the lower and
     upper sides (an inner boundary i <-> ni+1-i).  Blocks: i cut at i_cut, the leading edge and
-    ni+1-i_cut; k cut at the tip -> 8 uneven blocks.
+    ni+1-i_cut; k cut at the tip -> 8 uneven blocks; optional wall-normal cuts at the node
+    indices j_cuts multiply that by len(j_cuts)+1.
     """
     assert ni % 2 == 1
     mid = (ni + 1) // 2
@@ -236,51 +237,65 @@ def swept_wing(ni=257, nj=97, nk_wing=61, nk_tip=26, i_cut=49, sweep_deg=30.0, t
         X[2, k] = z[k]
     kt = nk_wing  # node index of the tip plane
     ibnd = [1, i_cut, mid, ni + 1 - i_cut, ni]
+    jbnd = [1] + list(j_cuts) + [nj]
     kbnd = [1, kt, nk]
+    njb = len(jbnd) - 1
     xyz, inp = [], []
     bid = {}
     for kb in range(2):
-        for ib in range(4):
-            bid[(ib, kb)] = len(xyz) + 1
-            i0, i1 = ibnd[ib], ibnd[ib + 1]
-            k0, k1 = kbnd[kb], kbnd[kb + 1]
-            xyz.append(np.ascontiguousarray(X[:, k0 - 1:k1, :, i0 - 1:i1]))
-            inp.append(InpBlock(i1 - i0 + 1, nj, k1 - k0 + 1))
+        for jb in range(njb):
+            for ib in range(4):
+                bid[(ib, jb, kb)] = len(xyz) + 1
+                i0, i1 = ibnd[ib], ibnd[ib + 1]
+                j0, j1 = jbnd[jb], jbnd[jb + 1]
+                k0, k1 = kbnd[kb], kbnd[kb + 1]
+                xyz.append(np.ascontiguousarray(X[:, k0 - 1:k1, j0 - 1:j1, i0 - 1:i1]))
+                inp.append(InpBlock(i1 - i0 + 1, j1 - j0 + 1, k1 - k0 + 1))
     for kb in range(2):
-        for ib in range(4):
-            b = bid[(ib, kb)]
-            B = inp[b - 1]
-            nx, ny, nzb = B.nx, B.ny, B.nz
-            # i faces
-            if ib == 0:  # TE seam: i=1 of block ib0 <-> i=ni of block ib3
-                sA, sB = interface(b, ((1, 1), (1, ny), (1, nzb)), bid[(3, kb)], lambda i, j, k, n3=inp[bid[(3, kb)] - 1].nx: (n3, j, k))
-                B.subs.append(sA)
-                inp[bid[(3, kb)] - 1].subs.append(sB)
-            if ib < 3:
-                nb = bid[(ib + 1, kb)]
-                sA, sB = interface(b, ((nx, nx), (1, ny), (1, nzb)), nb, lambda i, j, k: (1, j, k))
-                B.subs.append(sA)
-                inp[nb - 1].subs.append(sB)
-            # j faces
-            if kb == 0:
-                B.subs.append(InpSub((1, nx, 1, 1, 1, nzb), BC_WALL))
-            elif ib < 2:  # sheet beyond the tip: block ib <-> block 3-ib with i reversed
-                ob = bid[(3 - ib, kb)]
-                i0 = ibnd[ib]
-                o0 = ibnd[3 - ib]
-                sA, sB = interface(b, ((1, nx), (1, 1), (1, nzb)), ob, lambda i, j, k, i0=i0, o0=o0: ((ni + 1 - (i0 + i - 1)) - o0 + 1, 1, k))
-                B.subs.append(sA)
-                inp[ob - 1].subs.append(sB)
-            B.subs.append(InpSub((1, nx, ny, ny, 1, nzb), BC_FARFIELD))
-            # k faces
-            if kb == 0:
-                B.subs.append(InpSub((1, nx, 1, ny, 1, 1), BC_SYMMETRY))
-                nb = bid[(ib, 1)]
-                sA, sB = interface(b, ((1, nx), (1, ny), (nzb, nzb)), nb, lambda i, j, k: (i, j, 1))
-                B.subs.append(sA)
-                inp[nb - 1].subs.append(sB)
-            else:
-                B.subs.append(InpSub((1, nx, 1, ny, nzb, nzb), BC_FARFIELD))
+        for jb in range(njb):
+            for ib in range(4):
+                b = bid[(ib, jb, kb)]
+                B = inp[b - 1]
+                nx, ny, nzb = B.nx, B.ny, B.nz
+                # i faces
+                if ib == 0:  # TE seam: i=1 of block ib0 <-> i=ni of block ib3
+                    o = bid[(3, jb, kb)]
+                    sA, sB = interface(b, ((1, 1), (1, ny), (1, nzb)), o, lambda i, j, k, n3=inp[o - 1].nx: (n3, j, k))
+                    B.subs.append(sA)
+                    inp[o - 1].subs.append(sB)
+                if ib < 3:
+                    nb = bid[(ib + 1, jb, kb)]
+                    sA, sB = interface(b, ((nx, nx), (1, ny), (1, nzb)), nb, lambda i, j, k: (1, j, k))
+                    B.subs.append(sA)
+                    inp[nb - 1].subs.append(sB)
+                # j faces
+                if jb == 0:
+                    if kb == 0:
+                        B.subs.append(InpSub((1, nx, 1, 1, 1, nzb), BC_WALL))
+                    elif ib < 2:  # sheet beyond the tip: block ib <-> block 3-ib with i reversed
+                        ob = bid[(3 - ib, jb, kb)]
+                        i0 = ibnd[ib]
+                        o0 = ibnd[3 - ib]
+                        sA, sB = interface(b, ((1, nx), (1, 1), (1, nzb)), ob,
+                                           lambda i, j, k, i0=i0, o0=o0: ((ni + 1 - (i0 + i - 1)) - o0 + 1, 1, k))
+                        B.subs.append(sA)
+                        inp[ob - 1].subs.append(sB)
+                if jb == njb - 1:
+                    B.subs.append(InpSub((1, nx, ny, ny, 1, nzb), BC_FARFIELD))
+                else:  # wall-normal cut: top face of this block <-> bottom face of the next
+                    nb = bid[(ib, jb + 1, kb)]
+                    sA, sB = interface(b, ((1, nx), (ny, ny), (1, nzb)), nb, lambda i, j, k: (i, 1, k))
+                    B.subs.append(sA)
+                    inp[nb - 1].subs.append(sB)
+                # k faces
+                if kb == 0:
+                    B.subs.append(InpSub((1, nx, 1, ny, 1, 1), BC_SYMMETRY))
+                    nb = bid[(ib, jb, 1)]
+                    sA, sB = interface(b, ((1, nx), (1, ny), (nzb, nzb)), nb, lambda i, j, k: (i, j, 1))
+                    B.subs.append(sA)
+                    inp[nb - 1].subs.append(sB)
+                else:
+                    B.subs.append(InpSub((1, nx, 1, ny, nzb, nzb), BC_FARFIELD))
     return Case(name, xyz, inp, meta=dict(kind="wing", ni=ni, nj=nj, nk=nk, nk_wing=nk_wing, ref_s=None))
 
 

@@ -19,6 +19,8 @@ def small_cases():
         "foil_sa_char_hll": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=2, turb=2, iflag_reconstruction=2),
         "foil_sa_cons_omuscl2_roe": lambda: cases.airfoil(ni=65, nj=17, scheme=6, flux=4, turb=2, iflag_reconstruction=1),
         "wing8": lambda: cases.config2_small(),
+        "wing24_sst_roe": lambda: cases.config3_small(),
+        "wing24_sst_rk3": lambda: cases.config3_small(time_method=3, cfl=0.5),
     }
 
 

@@ -138,3 +138,27 @@ def test_mixed_vs_fp64_forces_config2(gpu):
     (_, cl0, cd0, _), (_, cl1, cd1, _) = out
     assert abs(cl1 - cl0) <= 1e-3 * abs(cl0)
     assert abs(cd1 - cd0) <= 1e-3 * abs(cd0)
+
+
+def test_config3_full_mixed_vs_fp64(gpu):
+    """Config 3 stand-in: SST swept wing, 24 uneven blocks, 7,798,784 cells.  Mixed precision
+    against FP64 after 20 LU-SGS steps: finite, CL / CD within 0.5 count (5e-5); the RK3 variant
+    (CFL 0.5) advances 3 steps without NaN."""
+    from ocfd_b200 import cases
+    out = []
+    for prec in (0, 1):
+        p, case = cases.config3(precision=prec)
+        assert len(case.dims) == 24 and case.ncells == 7798784
+        g = gpu.Solver(p, case)
+        g.advance(20)
+        _, rms = g.residual()
+        assert np.all(np.isfinite(rms))
+        out.append(g.forces())
+        g.close()
+    (_, cl0, cd0, _), (_, cl1, cd1, _) = out
+    assert abs(cl1 - cl0) <= 5e-5 and abs(cd1 - cd0) <= 5e-5, (cl0, cl1, cd0, cd1)
+    p, case = cases.config3(time_method=3, cfl=0.5)
+    g = gpu.Solver(p, case)
+    g.advance(3)
+    assert np.all(np.isfinite(g.residual()[1]))
+    g.close()

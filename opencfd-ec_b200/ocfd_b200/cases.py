@@ -39,13 +39,15 @@ def config3(ni=449, nj=129, nk_wing=97, nk_tip=41, i_cut=86, j_cuts=(33, 73), **
     the ellipsoidal fuselage is not modelled (only the wing, root on a symmetry plane), and the
     flux is Roe: HLLC as the reference implements it (the right star state carries v into the
     w-momentum, sub_flux_split.f90:67) diverges within 5 steps on this 3-D wing, in the CPU
-    restatement as on the GPU; iflag_flux=3 selects it.  The RK3 variant (time_method=3) runs at
+    restatement as on the GPU; iflag_flux=3 selects it.  LU-SGS runs at CFL 1 (at 2 and above the
+    wall cell at the root trailing edge diverges within 15 steps at this resolution with SST).
+    The RK3 variant (time_method=3) runs at
     CFL 0.5: at the configuration's 1.5, explicit RK3 with the SST sources diverges in the first
     steps on this mesh (wall spacing 4.5e-6 chord), again in both implementations."""
     case = meshgen.swept_wing(ni=ni, nj=nj, nk_wing=nk_wing, nk_tip=nk_tip, i_cut=i_cut, j_cuts=j_cuts,
                               name="config3_wing_%dx%dx%d_24blk" % (ni, nj, nk_wing + nk_tip - 1))
     raw = dict(ma=0.75, aoa=2.0, re=3.0e6, if_viscous=1, iflag_turbulence_model=3, iflag_scheme=5, iflag_flux=4,
-               time_method=0, cfl=5.0, precision=1, kt_inf=1e-8, wt_inf=1e-5, ref_s=meshgen.wing_ref_area(), ref_l=1.0)
+               time_method=0, cfl=1.0, precision=1, kt_inf=1e-8, wt_inf=1e-5, ref_s=meshgen.wing_ref_area(), ref_l=1.0)
     raw.update(over)
     return make_params(**raw), case
 

@@ -112,3 +112,28 @@ def test_profile_and_launch_count(gpu):
     assert 5 <= g.launches_per_step() <= 64
     assert g.stream()
     g.close()
+
+
+def test_restart_from_reference_flow_files(gpu, oracle, tmp_path):
+    """output_flow after 3 steps, then a restart from those files (read_flow_data semantics:
+    cells 0..n from the files, outer ghosts at the allocation values) on the GPU and on the
+    oracle: both continue identically to 1e-11."""
+    from ocfd_b200 import cases
+    from ocfd_b200.formats import read_flow, write_flow
+    p, case = cases.config2_small()
+    g = gpu.Solver(p, case)
+    k, tt = g.advance(3)
+    write_flow(str(tmp_path), [g.get_state(b) for b in range(g.nblk)], p, kstep=k, tt=tt)
+    g.close()
+    boxes, kstep, _ = read_flow(str(tmp_path), case.dims, p)
+    assert kstep == 3
+    h, o = gpu.Solver(p, case), oracle.OracleCase(p, case)
+    for b, U in enumerate(boxes):
+        h.set_state(b, U)
+        o.set_state(b, U)
+    for _ in range(2):
+        h.advance(1)
+        o.advance(1)
+        np.testing.assert_allclose(h.residual()[1][:6], o.residual()[1][:6], rtol=1e-11)
+    h.close()
+    o.close()

@@ -255,6 +255,10 @@ void* ocfd_stream(ocfd_handle* h);
 int ocfd_profile(ocfd_handle* h, int nsteps, double* phase_ms);
 /* Kernel launches queued by one ocfd_advance step (all of them this library's own kernels). */
 int ocfd_launches_per_step(ocfd_handle* h);
+/* Columns per CTA tile (32 or 64) of the LU-SGS wavefront sweeps.  ocfd_create times both on the
+ * new case (a few steps from freestream, before the state is initialised; the result does not
+ * depend on the choice) and keeps the faster; OCFD_LU_TC=32|64 or OCFD_NO_AUTOTUNE=1 skip that. */
+int ocfd_lu_tile_width(const ocfd_handle* h);
 
 #ifdef __cplusplus
 }

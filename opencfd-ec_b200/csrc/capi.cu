@@ -92,7 +92,10 @@ struct ocfd_handle {
   Arena<double> A64;
   Arena<float> A32;
   LuArgs lu{};
-  std::vector<LuTile> lu_tiles;
+  LuArgs lu_var[2]{};          // LU-SGS tile tables for TC = 32, 64
+  int lu_tc = 32;              // the tile width in use
+  RunInfo info{};
+  int nsm = 148;
   int* d_lu_err = nullptr;
   std::unique_ptr<Runner> run;
   cudaStream_t st = nullptr;
@@ -270,6 +273,88 @@ static cudaError_t up(T* d, const std::vector<T>& v) {
   if (v.empty()) return cudaSuccess;
   return cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
+
+// mu = 1/Re everywhere (allocate_mem_Blocks, sub_init.f90:507), Re of each block's solve
+static void reset_mu(ocfd_handle* h) {
+  size_t n = (size_t)h->tot_box;
+  std::vector<double> v(n);
+  for (int b = 0; b < h->nblk; b++)
+    std::fill(v.begin() + h->pre_box[b], v.begin() + h->pre_box[b + 1], 1.0 / h->Ps[h->blk[b].solve].re);
+  if (h->prec == OCFD_PREC_MIXED) {
+    std::vector<float> vf(v.begin(), v.end());
+    cudaMemcpy(h->d_mu, vf.data(), n * 4, cudaMemcpyHostToDevice);
+  } else {
+    cudaMemcpy(h->d_mu, v.data(), n * 8, cudaMemcpyHostToDevice);
+  }
+}
+
+// every work array back to its state right after allocation (zeros; mu = 1/Re), so that steps
+// run before the caller's first step leave no trace (edge ghosts of mu and mu_t are never
+// recomputed and carry history, sub_turbulence_SA.f90:37-45)
+static void reset_work(ocfd_handle* h) {
+  const long long tb = h->tot_box, tf = h->tot_face, tc = h->tot_cell;
+  const size_t ts = h->prec == OCFD_PREC_MIXED ? sizeof(float) : sizeof(double);
+  const int NV = h->nvar;
+  cudaDeviceSynchronize();
+  cudaMemset(h->d_P, 0, ts * P_COUNT * tb);
+  cudaMemset(h->d_mut, 0, ts * tb);
+  if (h->d_Kt) { cudaMemset(h->d_Kt, 0, ts * tb); cudaMemset(h->d_Wt, 0, ts * tb); cudaMemset(h->d_f1, 0, ts * tf); }
+  cudaMemset(h->d_Res, 0, ts * NV * tc);
+  cudaMemset(h->d_dt, 0, ts * tc);
+  cudaMemset(h->d_Lc, 0, ts * 3 * tc);
+  cudaMemset(h->d_Lv, 0, ts * 3 * tc);
+  cudaMemset(h->d_DU, 0, sizeof(double) * std::max(NV, 5) * tc);
+  if (h->d_Fv) cudaMemset(h->d_Fv, 0, ts * 12 * tf);
+  if (h->d_Ft) cudaMemset(h->d_Ft, 0, ts * 6 * tf);
+  if (h->d_Un) cudaMemset(h->d_Un, 0, sizeof(double) * NV * tb);
+  cudaMemset(h->d_flags, 0, sizeof(int) * 4 * h->nblk);
+  cudaMemset(h->d_lu_err, 0, sizeof(int));
+  reset_mu(h);
+}
+
+// (re)builds the runner for LU-SGS tile table v (0: TC = 32, 1: TC = 64); drops a captured graph
+static void select_lu(ocfd_handle* h, int v) {
+  h->lu = h->lu_var[v];
+  h->lu_tc = v == 0 ? 32 : 64;
+  h->info.lu = &h->lu;
+  h->info.lu_tc = h->lu_tc;
+  h->info.lu_grid = std::max(1, std::min(h->lu.ntiles, h->nsm * 8));
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  if (h->prec == OCFD_PREC_MIXED) h->run.reset(make_runner_mixed(h->A32, h->info));
+  else h->run.reset(make_runner_fp64(h->A64, h->info));
+}
+
+// Tile-width autotuner: both tile tables sweep the freshly initialised case (two warm-up and three
+// timed steps each, CUDA events around the two sweeps); the faster is kept.  The state is
+// re-initialised afterwards by the caller, and the choice does not change any result (every
+// tiling gives the hyperplane-order bits).
+static void autotune_lu(ocfd_handle* h) {
+  cudaEvent_t ev[6];
+  for (int q = 0; q < 6; q++) cudaEventCreate(&ev[q]);
+  float best = 1e30f;
+  int bestv = 0;
+  for (int v = 0; v < 2; v++) {
+    select_lu(h, v);
+    h->run->init_flow(h->st);
+    for (int s = 0; s < 2; s++) h->run->step(h->st);
+    float tot = 0.0f;
+    for (int s = 0; s < 3; s++) {
+      h->run->step(h->st, ev);
+      cudaEventSynchronize(ev[5]);
+      float a = 0.0f, b2 = 0.0f;
+      cudaEventElapsedTime(&a, ev[1], ev[2]);
+      cudaEventElapsedTime(&b2, ev[2], ev[3]);
+      tot += a + b2;
+    }
+    if (cudaGetLastError() == cudaSuccess && tot < best) { best = tot; bestv = v; }
+  }
+  for (int q = 0; q < 6; q++) cudaEventDestroy(ev[q]);
+  reset_work(h);
+  select_lu(h, bestv);
+}
+
+extern "C" int ocfd_lu_tile_width(const ocfd_handle* h) { return h ? h->lu_tc : 0; }
 
 // all solves of a handle share the model switches that select kernels; Mach, angles, Re, CFL,
 // schemes, fluxes and limits may differ per solve
@@ -550,19 +635,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     for (int b = 0; b < nblk; b++) std::memcpy(&hdw[h->pre_cell[b]], dw[b], (h->pre_cell[b + 1] - h->pre_cell[b]) * 8);
     cudaMemcpy(h->d_dwd, hdw.data(), tc * 8, cudaMemcpyHostToDevice);
   }
-  // mu = 1/Re everywhere (allocate_mem_Blocks, sub_init.f90:507), Re of each block's solve
-  {
-    size_t n = (size_t)tb;
-    std::vector<double> v(n);
-    for (int b = 0; b < nblk; b++)
-      std::fill(v.begin() + h->pre_box[b], v.begin() + h->pre_box[b + 1], 1.0 / ps[h->blk[b].solve].re);
-    if (h->prec == OCFD_PREC_MIXED) {
-      std::vector<float> vf(v.begin(), v.end());
-      cudaMemcpy(h->d_mu, vf.data(), n * 4, cudaMemcpyHostToDevice);
-    } else {
-      cudaMemcpy(h->d_mu, v.data(), n * 8, cudaMemcpyHostToDevice);
-    }
-  }
+  reset_mu(h);
   if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "stream"); }
   // ---- geometry on the device
   GeoArgs G;
@@ -579,20 +652,25 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     convert_to_float(h->d_dwd, h->d_dwf, tc, h->st);
   }
   if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "geometry sync"); }
-  // ---- LU-SGS wavefront tiles: TJ x TK = TC columns per CTA, ordered by J+K
-  //      (version 3: 4*TC threads per CTA, TC = 32 by default; version 2: 64 threads, TC = 64)
+  // ---- LU-SGS wavefront tiles: TJ x TK = TC columns per CTA, ordered by J+K.  Tables are built
+  //      for both tile widths (TC = 32 and 64); the faster one on this case is picked at the end
+  //      of creation (OCFD_LU_TC=32|64 fixes it; the one-thread-per-column form uses TC = 64)
   const int lu_v2 = std::getenv("OCFD_LU_V2") ? 1 : 0;
-  int lu_tc = 32;
-  if (const char* e2 = std::getenv("OCFD_LU_TC")) lu_tc = std::atoi(e2) == 64 ? 64 : 32;
-  if (lu_v2) lu_tc = 64;
-  {
+  int lu_force = 0;
+  if (const char* e2 = std::getenv("OCFD_LU_TC")) lu_force = std::atoi(e2) == 64 ? 64 : 32;
+  if (lu_v2) lu_force = 64;
+  h->d_lu_err = M.alloc<int>(1, e);
+  int* d_counter = M.alloc<int>(2, e);
+  for (int v = 0; v < 2; v++) {
+    const int tcv = v == 0 ? 32 : 64;
     int min_nzm = 1 << 30;
     for (const BlkD& B : h->blk) min_nzm = std::min(min_nzm, B.nz - 1);
     int TK = min_nzm <= 2 ? 2 : (min_nzm <= 4 ? 4 : 8);
-    if (lu_tc == 32 && TK == 8) TK = 4;
-    int TJ = lu_tc / TK;
+    if (tcv == 32 && TK == 8) TK = 4;
+    int TJ = tcv / TK;
     std::vector<int> tile_of(3 * nblk);
     std::vector<std::pair<int, LuTile>> order;
+    std::vector<LuTile> tiles;
     int first = 0;
     for (int b = 0; b < nblk; b++) {
       const BlkD& B = h->blk[b];
@@ -603,45 +681,38 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
       first += nJ * nK;
     }
     std::stable_sort(order.begin(), order.end(), [](const std::pair<int, LuTile>& a, const std::pair<int, LuTile>& b) { return a.first < b.first; });
-    for (auto& o : order) h->lu_tiles.push_back(o.second);
-    LuTile* d_tiles = M.alloc<LuTile>(h->lu_tiles.size(), e);
+    for (auto& o : order) tiles.push_back(o.second);
+    LuTile* d_tiles = M.alloc<LuTile>(tiles.size(), e);
     int* d_tile_of = M.alloc<int>(tile_of.size(), e);
-    int* d_counter = M.alloc<int>(2, e);
     int* d_progress = M.alloc<int>(first, e);
-    h->d_lu_err = M.alloc<int>(1, e);
     if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "lu tables"); }
-    cudaMemcpy(d_tiles, h->lu_tiles.data(), h->lu_tiles.size() * sizeof(LuTile), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_tiles, tiles.data(), tiles.size() * sizeof(LuTile), cudaMemcpyHostToDevice);
     cudaMemcpy(d_tile_of, tile_of.data(), tile_of.size() * sizeof(int), cudaMemcpyHostToDevice);
-    h->lu.tiles = d_tiles; h->lu.ntiles = first; h->lu.counter = d_counter; h->lu.progress = d_progress;
-    h->lu.tile_of = d_tile_of; h->lu.err = h->d_lu_err; h->lu.TJ = TJ; h->lu.TK = TK;
-    h->lu.spin_limit = 4000000;  // x ~64 ns: a few hundred ms before a stuck wait gives up
-    if (const char* s = std::getenv("OCFD_LU_SPIN_LIMIT")) h->lu.spin_limit = std::max(0LL, std::atoll(s));
+    LuArgs& L = h->lu_var[v];
+    L.tiles = d_tiles; L.ntiles = first; L.counter = d_counter; L.progress = d_progress;
+    L.tile_of = d_tile_of; L.err = h->d_lu_err; L.TJ = TJ; L.TK = TK;
+    L.spin_limit = 4000000;  // x ~64 ns: a few hundred ms before a stuck wait gives up
+    if (const char* sl = std::getenv("OCFD_LU_SPIN_LIMIT")) L.spin_limit = std::max(0LL, std::atoll(sl));
   }
   // ---- runner
-  RunInfo I;
-  I.nvar = NV; I.time_method = p->time_method; I.viscous = p->if_viscous; I.turb = turb; I.max_plane = h->max_plane;
-  I.ncchunk = (int)h->cchunk.size(); I.nwchunk = (int)h->wchunk.size();
-  I.lu_planes = std::getenv("OCFD_LUSGS_PLANES") ? 1 : 0;
-  I.lu_version = lu_v2 ? 2 : 3;
-  I.bc_rounds = h->bc_rounds.data(); I.nround = (int)(h->bc_rounds.size() / 3);
-  I.recon_prim = 1;
-  for (int q = 0; q < nsolve; q++) if (ps[q].iflag_reconstruction != 0) I.recon_prim = 0;
-  I.lu_tc = lu_tc;
-  I.lu = &h->lu;
+  h->info.nvar = NV; h->info.time_method = p->time_method; h->info.viscous = p->if_viscous; h->info.turb = turb;
+  h->info.max_plane = h->max_plane;
+  h->info.ncchunk = (int)h->cchunk.size(); h->info.nwchunk = (int)h->wchunk.size();
+  h->info.lu_planes = std::getenv("OCFD_LUSGS_PLANES") ? 1 : 0;
+  h->info.lu_version = lu_v2 ? 2 : 3;
+  h->info.bc_rounds = h->bc_rounds.data(); h->info.nround = (int)(h->bc_rounds.size() / 3);
+  h->info.recon_prim = 1;
+  for (int q = 0; q < nsolve; q++) if (ps[q].iflag_reconstruction != 0) h->info.recon_prim = 0;
   {
-    int dev = 0, nsm = 148;
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    I.lu_grid = std::max(1, std::min(h->lu.ntiles, nsm * 8));
+    cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev);
   }
-  if (h->prec == OCFD_PREC_MIXED) {
-    fill_arena<float>(h, h->A32, h->d_Mf, h->d_volf, h->d_dtmf, h->d_dwf);
-    h->run.reset(make_runner_mixed(h->A32, I));
-  } else {
-    fill_arena<double>(h, h->A64, h->d_Md, h->d_vold, h->d_dtmd, h->d_dwd);
-    h->run.reset(make_runner_fp64(h->A64, I));
-  }
+  if (h->prec == OCFD_PREC_MIXED) fill_arena<float>(h, h->A32, h->d_Mf, h->d_volf, h->d_dtmf, h->d_dwf);
+  else fill_arena<double>(h, h->A64, h->d_Md, h->d_vold, h->d_dtmd, h->d_dwd);
+  select_lu(h, lu_force ? (lu_force == 64 ? 1 : 0) : 0);
   if (!h->run) { M.release(); return OCFD_ERR_UNSUPPORTED; }
+  if (!lu_force && !h->info.lu_planes && !std::getenv("OCFD_NO_AUTOTUNE")) autotune_lu(h);
   h->run->init_flow(h->st);
   if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "init"); }
   int bcerr = 0;

@@ -21,6 +21,7 @@ EXPORTED = [
     "ocfd_limiter_status", "ocfd_array_shape", "ocfd_get_array", "ocfd_version", "ocfd_compute_residual",
     "ocfd_stream", "ocfd_profile", "ocfd_launches_per_step", "ocfd_create_batch", "ocfd_nsolve",
     "ocfd_residual_all", "ocfd_forces_all", "ocfd_footprint", "ocfd_synchronize", "ocfd_residual_static",
+    "ocfd_lu_tile_width",
 ]
 
 
@@ -69,6 +70,7 @@ def lib():
         L.ocfd_footprint.restype = ctypes.c_longlong
         L.ocfd_synchronize.argtypes = [vp]
         L.ocfd_residual_static.argtypes = [vp, dp, dp]
+        L.ocfd_lu_tile_width.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -220,6 +222,10 @@ class Solver:
 
     def launches_per_step(self):
         return int(lib().ocfd_launches_per_step(self.h))
+
+    def lu_tile_width(self):
+        """Columns per CTA tile of the LU-SGS sweeps, as picked by the creation-time autotuner."""
+        return int(lib().ocfd_lu_tile_width(self.h))
 
     def synchronize(self):
         self._check(lib().ocfd_synchronize(self.h), "synchronize")

@@ -111,6 +111,7 @@ def test_profile_and_launch_count(gpu):
     assert set(ph) == set(g.PHASES) and all(v >= 0.0 for v in ph.values()) and ph["step"] > 0.0
     assert 5 <= g.launches_per_step() <= 64
     assert g.stream()
+    assert g.lu_tile_width() in (32, 64)
     g.close()
 
 

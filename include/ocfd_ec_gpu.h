@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define OCFD_ABI_VERSION 1
+#define OCFD_ABI_VERSION 2
 
 /* error codes */
 #define OCFD_OK 0
@@ -68,6 +68,7 @@ extern "C" {
 #define OCFD_BC_INNER (-1)
 #define OCFD_TIME_LU_SGS 0
 #define OCFD_TIME_RK3 3
+#define OCFD_TIME_DUAL_LU_SGS (-1) /* dual time stepping, sub_time_advance.f90:126-202 */
 #define OCFD_TURB_NONE 0
 #define OCFD_TURB_SA 2
 #define OCFD_TURB_SST 3
@@ -92,7 +93,7 @@ typedef struct ocfd_params {
   int iflag_flux;             /* flux id                                                     */
   int iflag_reconstruction;   /* 0 primitive, 1 conservative, 2 characteristic              */
   int iflag_turbulence_model; /* 0, 2 (SA) or 3 (SST)                                       */
-  int time_method;            /* 0 LU-SGS, 3 RK3                                            */
+  int time_method;            /* 0 LU-SGS, 3 RK3, -1 dual-time LU-SGS                      */
   int if_viscous;             /* 0 Euler, 1 Navier-Stokes                                   */
   int iflag_local_dt;         /* 1 local time step, 0 global                               */
   int if_dtime_mesh;          /* 1: scale dt by the mesh-quality factor                    */
@@ -106,6 +107,9 @@ typedef struct ocfd_params {
   double ldmin, ldmax, lpmin, lpmax, lumax, lsamax;
   double ref_s, ref_l, centroid[3];
   double cv, cp;
+  double res_inner_limit;     /* dual time: inner-iteration residual target (Res_Inner_Limit) */
+  int step_inner_limit;       /* dual time: inner iterations per physical step (Step_Inner_Limit) */
+  int reserved;
 } ocfd_params;
 
 /* Opaque solver handle: all blocks of one case resident on one GPU. */
@@ -160,7 +164,11 @@ int ocfd_init_flow(ocfd_handle* h);
  * opencfd_ec3d_v1.16a.f90:167): residual + LU-SGS (or the 3 RK3 stages), U update, flow
  * limiter, BC, halo, vt/k/w clamps.  kstep and tt (may be NULL) receive the step counter and
  * time after the last step (tt advances by dt_global per step, sub_time_advance.f90:115).
- * Asynchronous on the device; the NaN check happens in ocfd_residual.
+ * Asynchronous on the device; the NaN check happens in ocfd_residual.  With time_method = -1 each
+ * step is a physical time step of NS_Time_Dual_LU_SGS (sub_time_advance.f90:126-202): up to
+ * step_inner_limit inner LU-SGS iterations on the physical-time residual, stopping when the largest
+ * residual RMS (of every solve) is at most res_inner_limit; the call then waits for each inner
+ * iteration's norms.
  */
 int ocfd_advance(ocfd_handle* h, int nsteps, int* kstep, double* tt);
 

@@ -91,7 +91,9 @@ struct Arena {
   const unsigned char *bci, *bcj, *bck;  // physical-face flags: bit0 lo face, bit1 hi face
   // state
   double* U;   // NV box planes
-  double* Un;  // NV box planes (RK3)
+  double* Un;  // NV box planes (RK3: stage start; dual time: time level n)
+  double* Un1;  // NV box planes (dual time: time level n-1)
+  const double* sfac;  // dual time: Sfac, Sfac1 of the current residual evaluation
   T* P;        // P_COUNT box planes
   T* mu;       // box
   T* mut;      // box

@@ -82,7 +82,9 @@ struct ocfd_handle {
   double *d_xc = nullptr, *d_yc = nullptr, *d_zc = nullptr;
   float *d_Mf = nullptr, *d_volf = nullptr, *d_dtmf = nullptr, *d_dwf = nullptr;
   unsigned char *d_bci = nullptr, *d_bcj = nullptr, *d_bck = nullptr;
-  double *d_U = nullptr, *d_Un = nullptr, *d_DU = nullptr;
+  double *d_U = nullptr, *d_Un = nullptr, *d_Un1 = nullptr, *d_DU = nullptr, *d_sfac = nullptr;
+  int dual_started = 0;   // Comput_Residual_one_mesh's saved first-call flag (sub_Residual.f90:25-33)
+  double sfac_h[2] = {0.0, 0.0};
   void *d_P = nullptr, *d_mu = nullptr, *d_mut = nullptr, *d_Kt = nullptr, *d_Wt = nullptr, *d_f1 = nullptr;
   void *d_Res = nullptr, *d_dt = nullptr, *d_Lc = nullptr, *d_Lv = nullptr, *d_Fi = nullptr, *d_Fv = nullptr, *d_Ft = nullptr;
   int* d_flags = nullptr;
@@ -127,6 +129,7 @@ extern "C" int ocfd_default_params(ocfd_params* p) {  // set_default_parameter, 
   p->cood_y_up = 1; p->iflag_limit_flow = 1; p->prl = 0.7; p->prt = 0.9;
   p->ldmin = 1.e-6; p->ldmax = 1000.0; p->lpmin = 1.e-6; p->lpmax = 1000.0; p->lumax = 1000.0; p->lsamax = 1000.0;
   p->if_scheme_positivity = 1; p->precision = OCFD_PREC_FP64;
+  p->step_inner_limit = 20; p->res_inner_limit = 1.e-10;  // sub_read_parameter.f90:69-70
   return OCFD_OK;
 }
 
@@ -263,7 +266,7 @@ static void fill_arena(ocfd_handle* h, Arena<T>& A, const T* M, const T* vol, co
   A.vold = h->d_vold; A.dwd = h->d_dwd; A.vol = vol; A.dtm = dtm; A.dw = dw;
   A.xc = h->d_xc; A.yc = h->d_yc; A.zc = h->d_zc;
   A.bci = h->d_bci; A.bcj = h->d_bcj; A.bck = h->d_bck;
-  A.U = h->d_U; A.Un = h->d_Un; A.P = (T*)h->d_P; A.mu = (T*)h->d_mu; A.mut = (T*)h->d_mut; A.Kt = (T*)h->d_Kt; A.Wt = (T*)h->d_Wt;
+  A.U = h->d_U; A.Un = h->d_Un; A.Un1 = h->d_Un1; A.sfac = h->d_sfac; A.P = (T*)h->d_P; A.mu = (T*)h->d_mu; A.mut = (T*)h->d_mut; A.Kt = (T*)h->d_Kt; A.Wt = (T*)h->d_Wt;
   A.f1 = (T*)h->d_f1; A.Res = (T*)h->d_Res; A.DU = h->d_DU; A.dt = (T*)h->d_dt; A.Lc = (T*)h->d_Lc; A.Lv = (T*)h->d_Lv;
   A.Fi = (T*)h->d_Fi; A.Fv = (T*)h->d_Fv; A.Ft = (T*)h->d_Ft; A.flags = h->d_flags;
 }
@@ -307,6 +310,7 @@ static void reset_work(ocfd_handle* h) {
   if (h->d_Fv) cudaMemset(h->d_Fv, 0, ts * 12 * tf);
   if (h->d_Ft) cudaMemset(h->d_Ft, 0, ts * 6 * tf);
   if (h->d_Un) cudaMemset(h->d_Un, 0, sizeof(double) * NV * tb);
+  if (h->d_Un1) cudaMemset(h->d_Un1, 0, sizeof(double) * NV * tb);
   cudaMemset(h->d_flags, 0, sizeof(int) * 4 * h->nblk);
   cudaMemset(h->d_lu_err, 0, sizeof(int));
   reset_mu(h);
@@ -364,7 +368,8 @@ static int check_params(const ocfd_params* ps, int nsolve) {
     const ocfd_params& p = ps[q];
     int tm = p.if_viscous ? p.iflag_turbulence_model : 0;
     if (tm != 0 && tm != 2 && tm != 3) return OCFD_ERR_UNSUPPORTED;
-    if (p.time_method != 0 && p.time_method != 3) return OCFD_ERR_UNSUPPORTED;
+    if (p.time_method != 0 && p.time_method != 3 && p.time_method != -1) return OCFD_ERR_UNSUPPORTED;
+    if (p.time_method == -1 && p.step_inner_limit < 1) return OCFD_ERR_ARG;
     if (p.iflag_flux < 1 || p.iflag_flux > 6) return OCFD_ERR_ARG;
     int tm0 = p0.if_viscous ? p0.iflag_turbulence_model : 0;
     if (tm != tm0 || p.if_viscous != p0.if_viscous || p.time_method != p0.time_method || p.precision != p0.precision) return OCFD_ERR_ARG;
@@ -573,7 +578,9 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   h->d_xc = M.alloc<double>(tb, e); h->d_yc = M.alloc<double>(tb, e); h->d_zc = M.alloc<double>(tb, e);
   h->d_bci = M.alloc<unsigned char>(obci, e); h->d_bcj = M.alloc<unsigned char>(obcj, e); h->d_bck = M.alloc<unsigned char>(obck, e);
   h->d_U = M.alloc<double>((size_t)NV * tb, e);
-  if (p->time_method == 3) h->d_Un = M.alloc<double>((size_t)NV * tb, e);
+  if (p->time_method == 3 || p->time_method == -1) h->d_Un = M.alloc<double>((size_t)NV * tb, e);
+  if (p->time_method == -1) h->d_Un1 = M.alloc<double>((size_t)NV * tb, e);
+  h->d_sfac = M.alloc<double>(2, e);
   h->d_DU = M.alloc<double>((size_t)std::max(NV, 5) * tc, e);
   h->d_P = M.alloc<char>(ts * P_COUNT * tb, e);
   h->d_mu = M.alloc<char>(ts * tb, e);
@@ -714,6 +721,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   if (!h->run) { M.release(); return OCFD_ERR_UNSUPPORTED; }
   if (!lu_force && !h->info.lu_planes && !std::getenv("OCFD_NO_AUTOTUNE")) autotune_lu(h);
   h->run->init_flow(h->st);
+  if (p->time_method == -1) h->run->dual_init(h->st);
   if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "init"); }
   int bcerr = 0;
   {
@@ -797,6 +805,7 @@ extern "C" int ocfd_set_state(ocfd_handle* h, int b, const double* U) {
   cudaError_t e = cudaMemcpyAsync(h->d_stage, U, (size_t)h->nvar * box * 8, cudaMemcpyHostToDevice, h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "set_state");
   h->run->scatter_state(h->st, b, h->d_stage, box);
+  if (h->P.time_method == -1) h->run->dual_init(h->st);  // a restart sets both earlier time levels
   if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) return cuda_fail(h, e, "set_state");
   return OCFD_OK;
 }
@@ -815,6 +824,7 @@ extern "C" int ocfd_get_state(ocfd_handle* h, int b, double* U) {
 extern "C" int ocfd_init_flow(ocfd_handle* h) {
   if (!h) return OCFD_ERR_ARG;
   h->run->init_flow(h->st);
+  if (h->P.time_method == -1) h->run->dual_init(h->st);
   cudaError_t e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "init_flow");
   h->kstep = 0;
@@ -835,10 +845,57 @@ static int ensure_graph(ocfd_handle* h) {
   return OCFD_OK;
 }
 
+// Sfac, Sfac1 of the next residual evaluation of a dual-time handle (the first one of the handle's
+// life uses the first-order values, sub_Residual.f90:25-33), copied to the device on its stream
+static void dual_factors(ocfd_handle* h) {
+  const double dt = h->P.dt_global;
+  if (h->dual_started == 0) { h->dual_started = 1; h->sfac_h[0] = 1.0 / (3.0 * dt); h->sfac_h[1] = 1.0 / dt; }
+  else { h->sfac_h[0] = 1.0 / (2.0 * dt); h->sfac_h[1] = 3.0 / (2.0 * dt); }
+  cudaMemcpyAsync(h->d_sfac, h->sfac_h, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st);
+}
+
+static int residual_impl(ocfd_handle* h, double* rmax, double* rrms, int nout);
+
+// NS_Time_Dual_LU_SGS (sub_time_advance.f90:126-202): inner iterations until the largest residual
+// RMS of every solve is at most Res_Inner_Limit or Step_Inner_Limit is reached, then the time
+// levels shift; the graph holds one inner iteration
+static int advance_dual(ocfd_handle* h, int nsteps) {
+  std::vector<double> rmax(7 * (size_t)h->nsolve), rrms(7 * (size_t)h->nsolve);
+  for (int s = 0; s < nsteps; s++) {
+    for (int kt = 1; kt <= h->P.step_inner_limit; kt++) {
+      dual_factors(h);
+      if (h->gexec) {
+        cudaError_t e = cudaGraphLaunch(h->gexec, h->st);
+        if (e != cudaSuccess) return cuda_fail(h, e, "graph launch");
+      } else {
+        h->run->step(h->st);
+      }
+      int rc = residual_impl(h, rmax.data(), rrms.data(), h->nsolve);
+      if (rc) return rc;
+      double mx = 0.0;
+      for (int q = 0; q < h->nsolve; q++) {
+        double m0 = rrms[7 * q];
+        for (int m = 0; m < h->nvar; m++) m0 = std::max(m0, rrms[7 * q + m]);
+        mx = std::max(mx, m0);
+      }
+      if (mx <= h->P.res_inner_limit) break;
+    }
+    h->run->dual_end(h->st);
+    h->tt = h->tt + h->P.dt_global;
+    h->kstep = h->kstep + 1;
+  }
+  return OCFD_OK;
+}
+
 extern "C" int ocfd_advance(ocfd_handle* h, int nsteps, int* kstep, double* tt) {
   if (!h || nsteps < 0) return OCFD_ERR_ARG;
   int rc = ensure_graph(h);
   if (rc) return rc;
+  if (h->P.time_method == -1) {
+    rc = advance_dual(h, nsteps);
+    if (rc) return rc;
+    nsteps = 0;
+  }
   for (int s = 0; s < nsteps; s++) {
     if (h->gexec) {
       cudaError_t e = cudaGraphLaunch(h->gexec, h->st);
@@ -858,6 +915,7 @@ extern "C" int ocfd_advance(ocfd_handle* h, int nsteps, int* kstep, double* tt) 
 
 extern "C" int ocfd_compute_residual(ocfd_handle* h, int with_lusgs) {
   if (!h) return OCFD_ERR_ARG;
+  if (h->P.time_method == -1) dual_factors(h);
   h->run->residual(h->st, with_lusgs != 0);
   cudaError_t e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "compute_residual");

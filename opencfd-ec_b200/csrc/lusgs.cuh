@@ -335,6 +335,8 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
     const int nsteps = nxm + TJ + TK - 2;
     const double w = s.w_lu, gamma = s.gamma;
     const bool visc = s.viscous == 1;
+    const bool dual = s.time_method == -1;
+    const double sfac1 = dual ? A.sfac[1] : 0.0;
     const int off = UPPER ? 1 : -1;
     auto i_of = [&](int t) { int il = t - lj - lk; return UPPER ? (nxm - il) : (il + 1); };
     auto on_at = [&](int t) { int il = t - lj - lk; return active && il >= 0 && il < nxm; };
@@ -432,6 +434,10 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
           if (!UPPER) alfa[5] = alfa[5] + lv;
           else alfa[5] = alfa[5] + x.Lv[0] + x.Lv[1] + x.Lv[2];
         }
+      }
+      if (dual) {  // dual time: + Sfac1 vol (sub_LU_SGS.f90:39, 92)
+#pragma unroll
+        for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + sfac1 * x.vol;
       }
     };
 

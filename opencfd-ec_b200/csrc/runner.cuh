@@ -82,6 +82,7 @@ class RunnerT : public Runner {
       k_visc_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
     }
     k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
+    if (I_.time_method == -1) k_dual_res<T, NV><<<grid_of(tc), 256, 0, st>>>(A);
     if (lusgs) {
       lusgs_sweep(st, false);
       lusgs_sweep(st, true);
@@ -134,6 +135,16 @@ class RunnerT : public Runner {
     const Arena<T>& A = A_;
     auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
     rec(0);
+    if (I_.time_method == -1) {  // one inner iteration of NS_Time_Dual_LU_SGS (sub_time_advance.f90:136-166)
+      residual_phases(st, ev);
+      cudaMemsetAsync(A.flags + A.nblk, 0, sizeof(int) * 2 * A.nblk, st);
+      k_update<T, NV, 4><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+      limit(st);
+      rec(4);
+      bc_halo(st);
+      rec(5);
+      return;
+    }
     if (I_.time_method == 0) {
       residual_phases(st, ev);
       cudaMemsetAsync(A.flags + A.nblk, 0, sizeof(int) * 2 * A.nblk, st);
@@ -180,10 +191,17 @@ class RunnerT : public Runner {
     for (int r = 0; r < I_.nround; r++) nbc += I_.bc_rounds[3 * r + 2] > 0;
     int bch = nbc + 1 + (A_.tot_halo > 0 ? 1 : 0);
     int n;
+    if (I_.time_method == -1) return res + 1 + lu + upd + bch;  // one dual-time inner iteration
     if (I_.time_method == 0) n = res + lu + upd + bch;
     else n = 1 + 3 * (res + upd + bch);
     if (NV >= 6) n += 1;
     return n;
+  }
+
+  void dual_init(cudaStream_t st) override { k_dual_init<T, NV><<<grid_of((long long)NV * A_.tot_box), 256, 0, st>>>(A_); }
+  void dual_end(cudaStream_t st) override {
+    k_dual_shift<T, NV><<<grid_of(A_.tot_cell), 256, 0, st>>>(A_);
+    if (NV >= 6) k_vtkw<T, NV><<<grid_of(A_.tot_cell), 256, 0, st>>>(A_);
   }
 
   void init_flow(cudaStream_t st) override {

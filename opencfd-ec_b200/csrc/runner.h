@@ -35,6 +35,10 @@ class Runner {
   virtual void residual(cudaStream_t st, bool lusgs) = 0;
   // freestream + BC + halo + corners (init_flow_zero, sub_init.f90:302-410)
   virtual void init_flow(cudaStream_t st) = 0;
+  // dual time: Un = Un1 = U (after an initialisation or a restart) / end of a physical step
+  // (Un1 = Un, Un = U, then the vt/k/w clamps of NS_Time_advance)
+  virtual void dual_init(cudaStream_t st) = 0;
+  virtual void dual_end(cudaStream_t st) = 0;
   // BC + halo + corners only
   virtual void bc_halo(cudaStream_t st) = 0;
   // residual norms: 14 doubles per solve into out (max[7], sum of squares[7])

@@ -848,6 +848,10 @@ __global__ void k_lusgs(Arena<T> A, int plane) {
         else alfa[5] = alfa[5] + Lvi + Lvj + Lvk;
       }
     }
+    if (s.time_method == -1) {  // dual time: + Sfac1 vol (sub_LU_SGS.f90:39, 92)
+#pragma unroll
+      for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + A.sfac[1] * (double)A.vold[c];
+    }
     double acc[NV];
 #pragma unroll
     for (int m = 0; m < NV; m++) acc[m] = 0.0;
@@ -901,7 +905,7 @@ __device__ __forceinline__ bool lim_bad(const SolveP& s, double d, double u, dou
   return d < s.ldmin || p < s.lpmin || d > s.ldmax || p > s.lpmax || fabs(u) > s.lumax || fabs(v) > s.lumax || fabs(w) > s.lumax;
 }
 
-template <class T, int NV, int MODE>  // MODE 0: LU-SGS; 1,2,3: RK3 stage KRK
+template <class T, int NV, int MODE>  // MODE 0: LU-SGS; 1,2,3: RK3 stage KRK; 4: dual-time inner iteration
 __global__ void k_update(Arena<T> A) {
   const long long tb = A.tot_box, tc = A.tot_cell;
   OCFD_GRID_STRIDE(g, tc) {
@@ -917,6 +921,10 @@ __global__ void k_update(Arena<T> A) {
       double u;
       if (MODE == 0) {
         u = A.U[m * tb + c] + A.DU[m * tc + g];
+      } else if (MODE == 4) {  // U = U + DU with U6/U7 as limit_vt left them (sub_time_advance.f90:138-147)
+        double cur = A.U[m * tb + c];
+        if (m >= 5) cur = clamp0(cur);
+        u = cur + A.DU[m * tc + g];
       } else {
         const double Ra = MODE == 1 ? 1.0 : (MODE == 2 ? 3.0 / 4.0 : 1.0 / 3.0);
         const double Rb = MODE == 1 ? 1.0 : (MODE == 2 ? 1.0 / 4.0 : 2.0 / 3.0);
@@ -936,6 +944,49 @@ __global__ void k_update(Arena<T> A) {
       if (lim_bad(s, d1, u1, v1, w1, p1)) atomicAdd(&A.flags[A.nblk + b], 1);
     }
   }
+}
+
+// dual time: physical-time derivative on the residual (sub_Residual.f90:94-104), U6/U7 clamped as
+// limit_vt leaves them in the reference
+template <class T, int NV>
+__global__ void k_dual_res(Arena<T> A) {
+  const long long tb = A.tot_box, tc = A.tot_cell;
+  const double Sfac = A.sfac[0];
+  OCFD_GRID_STRIDE(g, tc) {
+    int b = find_blk(A.pre_cell, A.nblk, g);
+    const BlkD& B = A.blk[b];
+    int i, j, k;
+    dec_cell(B, g - B.ocell, i, j, k);
+    const long long c = bix(B, i, j, k);
+    const double vol = A.vold[g];
+#pragma unroll
+    for (int m = 0; m < NV; m++) {
+      double u = A.U[m * tb + c];
+      if (m >= 5) u = clamp0(u);
+      double r = (double)A.Res[m * tc + g] - (3.0 * u - 4.0 * A.Un[m * tb + c] + A.Un1[m * tb + c]) * vol * Sfac;
+      A.Res[m * tc + g] = (T)r;
+    }
+  }
+}
+// dual time: end of a physical step, Un1 = Un, Un = U on the interior (sub_time_advance.f90:178-196)
+template <class T, int NV>
+__global__ void k_dual_shift(Arena<T> A) {
+  const long long tb = A.tot_box, tc = A.tot_cell;
+  OCFD_GRID_STRIDE(g, tc) {
+    int b = find_blk(A.pre_cell, A.nblk, g);
+    const BlkD& B = A.blk[b];
+    int i, j, k;
+    dec_cell(B, g - B.ocell, i, j, k);
+    const long long c = bix(B, i, j, k);
+#pragma unroll
+    for (int m = 0; m < NV; m++) { A.Un1[m * tb + c] = A.Un[m * tb + c]; A.Un[m * tb + c] = A.U[m * tb + c]; }
+  }
+}
+// dual time: Un = Un1 = U everywhere (Init_flow, sub_init.f90:278-296)
+template <class T, int NV>
+__global__ void k_dual_init(Arena<T> A) {
+  const long long n = (long long)NV * A.tot_box;
+  OCFD_GRID_STRIDE(g, n) { A.Un[g] = A.U[g]; A.Un1[g] = A.U[g]; }
 }
 
 // neighbour-average repair of bad cells (sub_limitflow.f90:84-150); DU planes 0..4 hold d,u,v,w,p

@@ -57,6 +57,9 @@ class OcfdParams(ctypes.Structure):
         ("centroid", ctypes.c_double * 3),
         ("cv", ctypes.c_double),
         ("cp", ctypes.c_double),
+        ("res_inner_limit", ctypes.c_double),
+        ("step_inner_limit", ctypes.c_int),
+        ("reserved", ctypes.c_int),
     ]
 
     def copy(self):
@@ -103,6 +106,7 @@ def default_params(**raw):
     p.ldmin, p.ldmax, p.lpmin, p.lpmax, p.lumax, p.lsamax = 1.0e-6, 1000.0, 1.0e-6, 1000.0, 1000.0, 1000.0
     p.if_scheme_positivity = 1
     p.precision = 0
+    p.step_inner_limit, p.res_inner_limit = 20, 1.0e-10
     for k, v in raw.items():
         if k == "centroid":
             for q in range(3):

@@ -174,6 +174,7 @@ struct Block {
   A3 ix1, iy1, iz1, jx1, jy1, jz1, kx1, ky1, kz1, ix2, iy2, iz2, jx2, jy2, jz2, kx2, ky2, kz2;
   A3 ix3, iy3, iz3, jx3, jy3, jz3, kx3, ky3, kz3, ix0, iy0, iz0, jx0, jy0, jz0, kx0, ky0, kz0;
   A4 U, Un, Res, DU;
+  A4 Un1;  // dual time: the state two physical steps back
   A3 dt, dw, mu, mu_t, dtime_mesh;
   A3 surf1, surf2, surf3, surf4, surf5, surf6;  // (n,n,3)
   I3 BcI, BcJ, BcK;
@@ -190,6 +191,7 @@ struct Case {
   double Ralfa[3], Rbeta[3], Rgamma[3];
   std::string err;
   int threads = 0;
+  int dual_started = 0;  // Comput_Residual_one_mesh's saved Iflag1 (sub_Residual.f90:25-33)
 };
 
 // per-block flow temporaries (Flow_Var module: d,uu,v,w,T,cc,p, Flux, Lci..Lvk)
@@ -1765,7 +1767,7 @@ static void comput_DFn(int NV, double* DF, const double* U, const double* DU, do
   if (NV == 7) DF[6] = U2[6] * un2 - U[6] * un1;
 }
 
-static void du_LU_SGS(Case& C, Block& B, Work& W) {  // sub_LU_SGS.f90:4-129
+static void du_LU_SGS(Case& C, Block& B, Work& W, double Sfac1 = 0.0) {  // sub_LU_SGS.f90:4-129
   int NV = C.NVAR, nx = B.nx, ny = B.ny, nz = B.nz;
   double gamma = C.P.gamma, w_LU = C.P.w_lu;
   int visc = C.P.if_viscous;
@@ -1781,6 +1783,7 @@ static void du_LU_SGS(Case& C, Block& B, Work& W) {  // sub_LU_SGS.f90:4-129
           for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + 2.0 * (W.Lvi(i, j, k) + W.Lvj(i, j, k) + W.Lvk(i, j, k));
           if (NV == 6) alfa[5] = alfa[5] + (W.Lvi(i, j, k) + W.Lvj(i, j, k) + W.Lvk(i, j, k));
         }
+        if (C.P.time_method == -1) for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + Sfac1 * B.vol(i, j, k);  // line 39
         if (i != 1) {
           for (int m = 0; m < NV; m++) { Uv[m] = B.U(m + 1, i - 1, j, k); DUv[m] = B.DU(m + 1, i - 1, j, k); }
           comput_DFn(NV, DF, Uv, DUv, B.ni1(i, j, k), B.ni2(i, j, k), B.ni3(i, j, k), gamma);
@@ -1821,6 +1824,7 @@ static void du_LU_SGS(Case& C, Block& B, Work& W) {  // sub_LU_SGS.f90:4-129
           for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + 2.0 * (W.Lvi(i, j, k) + W.Lvj(i, j, k) + W.Lvk(i, j, k));
           if (NV == 6) alfa[5] = alfa[5] + W.Lvi(i, j, k) + W.Lvj(i, j, k) + W.Lvk(i, j, k);
         }
+        if (C.P.time_method == -1) for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + Sfac1 * B.vol(i, j, k);  // line 92
         if (i != nx - 1) {
           for (int m = 0; m < NV; m++) { Uv[m] = B.U(m + 1, i + 1, j, k); DUv[m] = B.DU(m + 1, i + 1, j, k); }
           comput_DFn(NV, DF, Uv, DUv, B.ni1(i, j, k), B.ni2(i, j, k), B.ni3(i, j, k), gamma);
@@ -1851,7 +1855,7 @@ static void du_LU_SGS(Case& C, Block& B, Work& W) {  // sub_LU_SGS.f90:4-129
   }
 }
 
-static int residual_block(Case& C, Block& B, bool lusgs) {  // Comput_Residual_one_mesh body, sub_Residual.f90:45-124
+static int residual_block(Case& C, Block& B, bool lusgs, double Sfac = 0.0, double Sfac1 = 0.0) {  // Comput_Residual_one_mesh body, sub_Residual.f90:45-124
   Work W;
   int nx = B.nx, ny = B.ny, nz = B.nz;
   W.d.alloc(1 - LAP, nx + LAP - 1, 1 - LAP, ny + LAP - 1, 1 - LAP, nz + LAP - 1);
@@ -1871,9 +1875,16 @@ static int residual_block(Case& C, Block& B, bool lusgs) {  // Comput_Residual_o
   flux_inviscid(C, B, W, 1);
   flux_inviscid(C, B, W, 2);
   if (C.P.if_viscous == 1) { flux_viscous(C, B, W, 0); flux_viscous(C, B, W, 1); flux_viscous(C, B, W, 2); }
+  if (C.P.time_method == -1) {  // physical-time derivative of the dual-time scheme (sub_Residual.f90:94-104)
+    for (int k = 1; k <= nz - 1; k++)
+      for (int j = 1; j <= ny - 1; j++)
+        for (int i = 1; i <= nx - 1; i++)
+          for (int m = 1; m <= C.NVAR; m++)
+            B.Res(m, i, j, k) = B.Res(m, i, j, k) - (3.0 * B.U(m, i, j, k) - 4.0 * B.Un(m, i, j, k) + B.Un1(m, i, j, k)) * B.vol(i, j, k) * Sfac;
+  }
   comput_Lijk(C, B, W);
   comput_dt(C, B, W);
-  if (lusgs) du_LU_SGS(C, B, W);
+  if (lusgs) du_LU_SGS(C, B, W, Sfac1);
   return 0;
 }
 
@@ -2020,10 +2031,61 @@ static int advance_rk3(Case& C) {  // sub_time_advance.f90:265-326
   return 0;
 }
 
+static int norms(Case& C, double* rmax, double* rrms);
+
+// Sfac, Sfac1 of one Comput_Residual_one_mesh call: the first call of the run uses the
+// first-order values, every later call the second-order ones (sub_Residual.f90:25-33)
+static void dual_factors(Case& C, double& Sfac, double& Sfac1) {
+  const double dt = C.P.dt_global;
+  if (C.dual_started == 0) { C.dual_started = 1; Sfac = 1.0 / (3.0 * dt); Sfac1 = 1.0 / dt; }
+  else { Sfac = 1.0 / (2.0 * dt); Sfac1 = 3.0 / (2.0 * dt); }
+}
+
+static void dual_init(Case& C) {  // Init_flow, sub_init.f90:278-296
+  for (Block& B : C.B)
+    for (int k = -1; k <= B.nz + 1; k++)
+      for (int j = -1; j <= B.ny + 1; j++)
+        for (int i = -1; i <= B.nx + 1; i++)
+          for (int m = 1; m <= C.NVAR; m++) { B.Un(m, i, j, k) = B.U(m, i, j, k); B.Un1(m, i, j, k) = B.U(m, i, j, k); }
+}
+
+static int advance_dual(Case& C) {  // NS_Time_Dual_LU_SGS, sub_time_advance.f90:126-202
+  int NV = C.NVAR;
+  for (int kt = 1; kt <= C.P.step_inner_limit; kt++) {
+    double Sfac, Sfac1;
+    dual_factors(C, Sfac, Sfac1);
+    for (Block& B : C.B) residual_block(C, B, true, Sfac, Sfac1);
+    for (Block& B : C.B)
+      for (int k = 1; k <= B.nz - 1; k++)
+        for (int j = 1; j <= B.ny - 1; j++)
+          for (int i = 1; i <= B.nx - 1; i++)
+            for (int m = 1; m <= NV; m++) B.U(m, i, j, k) = B.U(m, i, j, k) + B.DU(m, i, j, k);
+    if (C.P.iflag_limit_flow == 1) limit_flow(C);
+    int rc = boundary_all(C);
+    if (rc) return rc;
+    halo(C);
+    double rmax[7], rrms[7];
+    rc = norms(C, rmax, rrms);
+    if (rc) return rc;
+    double max_res = rrms[0];
+    for (int m = 0; m < NV; m++) max_res = std::max(max_res, rrms[m]);
+    if (max_res <= C.P.res_inner_limit) break;
+  }
+  for (Block& B : C.B)
+    for (int k = 1; k <= B.nz - 1; k++)
+      for (int j = 1; j <= B.ny - 1; j++)
+        for (int i = 1; i <= B.nx - 1; i++)
+          for (int m = 1; m <= NV; m++) { B.Un1(m, i, j, k) = B.Un(m, i, j, k); B.Un(m, i, j, k) = B.U(m, i, j, k); }
+  C.tt = C.tt + C.P.dt_global;
+  C.Kstep = C.Kstep + 1;
+  return 0;
+}
+
 static int advance(Case& C) {  // NS_Time_advance, sub_time_advance.f90:6-23
   int rc;
   if (C.P.time_method == 0) rc = advance_lusgs(C);
   else if (C.P.time_method == 3) rc = advance_rk3(C);
+  else if (C.P.time_method == -1) rc = advance_dual(C);
   else { C.err = "time method not supported"; return OCFD_ERR_UNSUPPORTED; }
   if (rc) return rc;
   force_vt_kw(C);
@@ -2211,6 +2273,7 @@ int oracle_create(const ocfd_params* p, int nblk, const int* nijk, const double*
           else if (NV == 7) { B.U(6, i, j, k) = 0.0; B.U(7, i, j, k) = 1.0; }
         }
     B.Un.alloc(NV, -1, nx + 1, -1, ny + 1, -1, nz + 1);
+    if (p->time_method == -1) B.Un1.alloc(NV, -1, nx + 1, -1, ny + 1, -1, nz + 1);
     B.Res.alloc(NV, -1, nx + 1, -1, ny + 1, -1, nz + 1);
     B.DU.alloc(NV, -1, nx + 1, -1, ny + 1, -1, nz + 1);
     B.dt.alloc(-1, nx + 1, -1, ny + 1, -1, nz + 1);
@@ -2236,6 +2299,7 @@ int oracle_create(const ocfd_params* p, int nblk, const int* nijk, const double*
   }
   for (Block& B : C->B) mesh_quality(B);
   init_flow(*C);
+  if (C->P.time_method == -1) dual_init(*C);
   *out = C;
   return 0;
 }
@@ -2255,11 +2319,19 @@ int oracle_advance(void* h, int nsteps, int* kstep, double* tt) {
 // current state, no update.
 int oracle_compute_residual(void* h, int lusgs) {
   Case* C = (Case*)h;
-  for (Block& B : C->B) residual_block(*C, B, lusgs != 0);
+  double Sfac = 0.0, Sfac1 = 0.0;
+  if (C->P.time_method == -1) dual_factors(*C, Sfac, Sfac1);
+  for (Block& B : C->B) residual_block(*C, B, lusgs != 0, Sfac, Sfac1);
   return 0;
 }
 
-int oracle_init_flow(void* h) { Case* C = (Case*)h; C->Kstep = 0; C->tt = 0.0; init_flow(*C); return 0; }
+int oracle_init_flow(void* h) {
+  Case* C = (Case*)h;
+  C->Kstep = 0; C->tt = 0.0;
+  init_flow(*C);
+  if (C->P.time_method == -1) dual_init(*C);
+  return 0;
+}
 
 int oracle_residual(void* h, double* rmax, double* rrms) { return norms(*(Case*)h, rmax, rrms); }
 
@@ -2271,7 +2343,17 @@ long long oracle_state_size(void* h, int b) {
   return (long long)C->NVAR * (B.nx + 7) * (B.ny + 7) * (B.nz + 7);
 }
 int oracle_get_state(void* h, int b, double* U) { Block& B = ((Case*)h)->B[b]; std::memcpy(U, B.U.v.data(), B.U.v.size() * 8); return 0; }
-int oracle_set_state(void* h, int b, const double* U) { Block& B = ((Case*)h)->B[b]; std::memcpy(B.U.v.data(), U, B.U.v.size() * 8); return 0; }
+int oracle_set_state(void* h, int b, const double* U) {
+  Case* C = (Case*)h;
+  Block& B = C->B[b];
+  std::memcpy(B.U.v.data(), U, B.U.v.size() * 8);
+  if (C->P.time_method == -1)  // a restart sets both earlier time levels too (Init_flow, sub_init.f90:278-296)
+    for (int k = -1; k <= B.nz + 1; k++)
+      for (int j = -1; j <= B.ny + 1; j++)
+        for (int i = -1; i <= B.nx + 1; i++)
+          for (int m = 1; m <= C->NVAR; m++) { B.Un(m, i, j, k) = B.U(m, i, j, k); B.Un1(m, i, j, k) = B.U(m, i, j, k); }
+  return 0;
+}
 
 int oracle_limiter_status(void* h, int b, int* n, int* ov) { Block& B = ((Case*)h)->B[b]; *n = B.nlimited; *ov = B.overlimit; return 0; }
 

@@ -21,6 +21,9 @@ def small_cases():
         "wing8": lambda: cases.config2_small(),
         "wing24_sst_roe": lambda: cases.config3_small(),
         "wing24_sst_rk3": lambda: cases.config3_small(time_method=3, cfl=0.5),
+        "foil_sa_dual": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=4, turb=2, time_method=-1, dt_global=0.05,
+                                              step_inner_limit=4, res_inner_limit=1e-14),
+        "bump_dual": lambda: cases.config1(scale=0.25, time_method=-1, dt_global=0.2, step_inner_limit=3, res_inner_limit=1e-14),
     }
 
 

@@ -79,7 +79,7 @@ def test_create_rejects_bad_arguments_before_touching_the_device(clib):
     q.iflag_turbulence_model = 1   # Baldwin-Lomax: not on the hot path
     assert call(q, 1, nijk) == OCFD_ERR_UNSUPPORTED
     q = p.copy()
-    q.time_method = 1              # dual time: not on the hot path
+    q.time_method = 1              # first-order explicit Euler (Time_Euler1): not built
     assert call(q, 1, nijk) == OCFD_ERR_UNSUPPORTED
     q = p.copy()
     q.iflag_flux = 9

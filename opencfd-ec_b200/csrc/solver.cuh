@@ -16,6 +16,11 @@
 #include "arena.h"
 #include "physics.cuh"
 
+// residual kernels bound by memory latency: at most 64 registers, four 256-thread CTAs per SM
+#ifndef OCFD_MEM_MINB
+#define OCFD_MEM_MINB 4
+#endif
+
 namespace ocfd {
 
 #define OCFD_GRID_STRIDE(g, n) for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < (n); g += (long long)gridDim.x * blockDim.x)
@@ -137,7 +142,7 @@ __global__ void k_sa_pre(Arena<T> A) {
 
 // SA face fluxes Fluxv / Fluxv2 (SA.f90:74-96, 110-131, 145-167) for direction DIR
 template <class T, int DIR>
-__global__ void k_sa_flux(Arena<T> A) {
+__global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_flux(Arena<T> A) {
   const long long tb = A.tot_box, tf = A.tot_face;
   OCFD_GRID_STRIDE(g, tf) {
     int b = find_blk(A.pre_face, A.nblk, g);
@@ -189,7 +194,7 @@ __global__ void k_sa_flux(Arena<T> A) {
 
 // Res(6): flux sums in the i, j, k order of SA.f90:99-178 plus the source (180-254)
 template <class T>
-__global__ void k_sa_res(Arena<T> A) {
+__global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_res(Arena<T> A) {
   const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
   OCFD_GRID_STRIDE(g, tc) {
     int b = find_blk(A.pre_cell, A.nblk, g);
@@ -338,7 +343,7 @@ __global__ void k_sst_mut_ghost(Arena<T> A) {
 
 // SST diffusion + first-order convection fluxes (SST.f90:182-318) for direction DIR
 template <class T, int DIR>
-__global__ void k_sst_flux(Arena<T> A) {
+__global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sst_flux(Arena<T> A) {
   const long long tb = A.tot_box, tf = A.tot_face;
   OCFD_GRID_STRIDE(g, tf) {
     int b = find_blk(A.pre_face, A.nblk, g);
@@ -403,7 +408,7 @@ __global__ void k_sst_flux(Arena<T> A) {
 
 // Res(6,7) += flux differences in the i, j, k order (SST.f90:221-330)
 template <class T>
-__global__ void k_sst_res(Arena<T> A) {
+__global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sst_res(Arena<T> A) {
   const long long tf = A.tot_face, tc = A.tot_cell;
   OCFD_GRID_STRIDE(g, tc) {
     int b = find_blk(A.pre_cell, A.nblk, g);
@@ -635,7 +640,7 @@ __global__ void k_inv_kbc(Arena<T> A) {
 // viscous fluxes (flux_viscous_i/j/k, sub_Residual.f90:712-1247)
 // ============================================================================================
 template <class T, int DIR>
-__global__ void k_visc_flux(Arena<T> A) {
+__global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_visc_flux(Arena<T> A) {
   const long long tb = A.tot_box, tf = A.tot_face;
   OCFD_GRID_STRIDE(g, tf) {
     int b = find_blk(A.pre_face, A.nblk, g);
@@ -735,7 +740,7 @@ __global__ void k_visc_flux(Arena<T> A) {
 // spectral radii (comput_Lijk, sub_time_acceleraction.f90:7-56) and local dt (comput_dt, 61-112)
 // ============================================================================================
 template <class T>
-__global__ void k_assemble(Arena<T> A) {
+__global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
   const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
   OCFD_GRID_STRIDE(g, tc) {
     int b = find_blk(A.pre_cell, A.nblk, g);

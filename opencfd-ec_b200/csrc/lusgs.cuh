@@ -467,15 +467,20 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
     if (grp == 4) {
       // poller warp: its flag traffic (release of this tile's progress after B1, acquire of the
       // upstream tiles' progress) never sits on the compute warps' paths
-      if (tid == 4 * TC) poll(0);
+      // waits one step ahead of the compute warps (the upstream tiles run at least one step
+      // further ahead than the dependency needs), so the cross-tile DU of step t+1 can be loaded
+      // during step t
+      if (tid == 4 * TC) { poll(0); if (1 < nsteps) poll(1); }
+      cta_bar<NT>();  // B0
       for (int t = 0; t < nsteps; t++) {
         cta_bar<NT>();  // B1
         if (tid == 4 * TC && t > 0) st_release(L.progress + my, t);
         cta_bar<NT>();  // B2
-        if (tid == 4 * TC && t + 1 < nsteps) poll(t + 1);
+        if (tid == 4 * TC && t + 2 < nsteps) poll(t + 2);
       }
     } else if (owner) {
       if (on_at(0)) load_own(0, on);
+      cta_bar<NT>();  // B0
       for (int t = 0; t < nsteps; t++) {
         cta_bar<NT>();  // B1
         if (on_at(t)) {
@@ -498,6 +503,14 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
     } else {
       if (on_at(0) && has_at(0)) load_dir(0, dn);
       prep_dir(0, dn);
+      double xdu[NV];  // cross-tile neighbour's DU of the current step, loaded one step early
+      auto load_xdu = [&](int t) {
+        const long long cn = cix(B, i_of(t), j + (d == 1 ? off : 0), k + (d == 2 ? off : 0));
+#pragma unroll
+        for (int m = 0; m < NV; m++) xdu[m] = __ldcg(A.DU + m * tc + cn);
+      };
+      cta_bar<NT>();  // B0: the poller's first waits are done
+      if (xt && has) load_xdu(0);
       for (int t = 0; t < nsteps; t++) {
         cta_bar<NT>();  // B1: step t-1 finished (DU in s_pub and in HBM), upstream tiles ready
         if (on_at(t + 1) && has_at(t + 1)) load_dir(t + 1, dn);
@@ -507,10 +520,8 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
 #pragma unroll
             for (int m = 0; m < NV; m++) DUn[m] = s_pub[m][pubcol];
           } else {
-            const int i = i_of(t);
-            const long long cn = cix(B, i, j + (d == 1 ? off : 0), k + (d == 2 ? off : 0));
 #pragma unroll
-            for (int m = 0; m < NV; m++) DUn[m] = __ldcg(A.DU + m * tc + cn);
+            for (int m = 0; m < NV; m++) DUn[m] = xdu[m];
           }
           double U2[NV];
 #pragma unroll
@@ -540,6 +551,7 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
         cta_bar<NT>();  // B2
         if (on_at(t)) finish(d, cix(B, i_of(t), j, k));
         prep_dir(t + 1, dn);
+        if (xt && has) load_xdu(t + 1);  // ready since the poller's wait of step t-1
       }
     }
     __syncthreads();

@@ -67,6 +67,7 @@ extern "C" {
 #define OCFD_BC_EXTRAPOLATE 401
 #define OCFD_BC_INNER (-1)
 #define OCFD_TIME_LU_SGS 0
+#define OCFD_TIME_EULER1 1 /* explicit first-order Euler, sub_time_advance.f90:217-260 */
 #define OCFD_TIME_RK3 3
 #define OCFD_TIME_DUAL_LU_SGS (-1) /* dual time stepping, sub_time_advance.f90:126-202 */
 #define OCFD_TURB_NONE 0
@@ -93,7 +94,7 @@ typedef struct ocfd_params {
   int iflag_flux;             /* flux id                                                     */
   int iflag_reconstruction;   /* 0 primitive, 1 conservative, 2 characteristic              */
   int iflag_turbulence_model; /* 0, 2 (SA) or 3 (SST)                                       */
-  int time_method;            /* 0 LU-SGS, 3 RK3, -1 dual-time LU-SGS                      */
+  int time_method;            /* 0 LU-SGS, 1 explicit Euler, 3 RK3, -1 dual-time LU-SGS    */
   int if_viscous;             /* 0 Euler, 1 Navier-Stokes                                   */
   int iflag_local_dt;         /* 1 local time step, 0 global                               */
   int if_dtime_mesh;          /* 1: scale dt by the mesh-quality factor                    */
@@ -109,7 +110,9 @@ typedef struct ocfd_params {
   double cv, cp;
   double res_inner_limit;     /* dual time: inner-iteration residual target (Res_Inner_Limit) */
   int step_inner_limit;       /* dual time: inner iterations per physical step (Step_Inner_Limit) */
-  int reserved;
+  int if_residual_smoothing;  /* 1: upwind implicit residual smoothing of Res(1:5) after the
+                                 spectral radii (If_Residual_smoothing, sub_Residual.f90:111-113;
+                                 Residual_smoothing, sub_time_acceleraction.f90:119-217)  */
 } ocfd_params;
 
 /* Opaque solver handle: all blocks of one case resident on one GPU. */
@@ -161,7 +164,8 @@ int ocfd_init_flow(ocfd_handle* h);
 
 /*
  * nsteps calls of NS_Time_advance(1) (sub_time_advance.f90:6-23; the driver call at
- * opencfd_ec3d_v1.16a.f90:167): residual + LU-SGS (or the 3 RK3 stages), U update, flow
+ * opencfd_ec3d_v1.16a.f90:167): residual + LU-SGS (or the 3 RK3 stages, or one explicit Euler
+ * stage U = Un + dt Res/vol for time_method = 1), U update, flow
  * limiter, BC, halo, vt/k/w clamps.  kstep and tt (may be NULL) receive the step counter and
  * time after the last step (tt advances by dt_global per step, sub_time_advance.f90:115).
  * Asynchronous on the device; the NaN check happens in ocfd_residual.  With time_method = -1 each

@@ -67,6 +67,8 @@ struct Arena {
   const long long* pre_cell;  // nblk+1
   const long long* pre_face;  // nblk+1
   const long long* pre_col;   // nblk+1, (ny-1)(nz-1) columns per block
+  const long long* pre_lnj;   // nblk+1, (nx-1)(nz-1) j-lines per block
+  const long long* pre_lnk;   // nblk+1, (nx-1)(ny-1) k-lines per block
   const SubD* sub;
   int nsub;
   const long long* pre_subcell;  // nsub+1 prefix sums of face cells per subface (transverse ranges b..e-1)
@@ -80,7 +82,7 @@ struct Arena {
   int nwchunk;
   const SolveP* sp;
   int nsolve;
-  long long tot_box, tot_cell, tot_face, tot_node, tot_col, tot_subcell, tot_halo;
+  long long tot_box, tot_cell, tot_face, tot_node, tot_col, tot_subcell, tot_halo, tot_lnj, tot_lnk;
   // geometry
   const double *x, *y, *z;   // node
   const double* Md;          // 48 FP64 metric planes (face)

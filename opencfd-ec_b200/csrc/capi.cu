@@ -59,7 +59,7 @@ struct ocfd_handle {
   int nvar = 5, prec = 0, nblk = 0, nsolve = 1;
   std::vector<BlkD> blk;
   std::vector<SubD> sub;
-  std::vector<long long> pre_box, pre_cell, pre_face, pre_col, pre_subcell, pre_halo;
+  std::vector<long long> pre_box, pre_cell, pre_face, pre_col, pre_subcell, pre_halo, pre_lnj, pre_lnk;
   std::vector<int4> cchunk, wchunk;
   std::vector<SolveP> sps;
   long long tot_box = 0, tot_cell = 0, tot_face = 0, tot_node = 0, tot_col = 0, tot_subcell = 0, tot_halo = 0;
@@ -71,6 +71,7 @@ struct ocfd_handle {
   SubD* d_sub = nullptr;
   SolveP* d_sp = nullptr;
   long long *d_pre_box = nullptr, *d_pre_cell = nullptr, *d_pre_face = nullptr, *d_pre_col = nullptr, *d_pre_subcell = nullptr, *d_pre_halo = nullptr;
+  long long *d_pre_lnj = nullptr, *d_pre_lnk = nullptr;  // j-line and k-line prefix sums (residual smoothing)
   int4 *d_cchunk = nullptr, *d_wchunk = nullptr;
   int* d_cspre = nullptr;
   std::vector<int> cspre;
@@ -78,6 +79,11 @@ struct ocfd_handle {
   std::vector<long long> bc_pre;
   int* d_bc_ent = nullptr;
   long long* d_bc_pre = nullptr;
+  std::vector<int> halo_ent, halo_levels;  // ordered interface copies (entries grouped by level)
+  std::vector<long long> halo_pre;
+  int* d_halo_ent = nullptr;
+  long long* d_halo_pre = nullptr;
+  double* d_halo_stage = nullptr;
   double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr, *d_Md = nullptr, *d_vold = nullptr, *d_dtmd = nullptr, *d_dwd = nullptr;
   double *d_xc = nullptr, *d_yc = nullptr, *d_zc = nullptr;
   float *d_Mf = nullptr, *d_volf = nullptr, *d_dtmf = nullptr, *d_dwf = nullptr;
@@ -254,6 +260,7 @@ template <class T>
 static void fill_arena(ocfd_handle* h, Arena<T>& A, const T* M, const T* vol, const T* dtm, const T* dw) {
   A.blk = h->d_blk; A.nblk = h->nblk;
   A.pre_box = h->d_pre_box; A.pre_cell = h->d_pre_cell; A.pre_face = h->d_pre_face; A.pre_col = h->d_pre_col;
+  A.pre_lnj = h->d_pre_lnj; A.pre_lnk = h->d_pre_lnk; A.tot_lnj = h->pre_lnj[h->nblk]; A.tot_lnk = h->pre_lnk[h->nblk];
   A.sub = h->d_sub; A.nsub = (int)h->sub.size();
   A.pre_subcell = h->d_pre_subcell; A.pre_halo = h->d_pre_halo;
   A.cchunk = h->d_cchunk; A.ncchunk = (int)h->cchunk.size(); A.cspre = h->d_cspre;
@@ -368,11 +375,14 @@ static int check_params(const ocfd_params* ps, int nsolve) {
     const ocfd_params& p = ps[q];
     int tm = p.if_viscous ? p.iflag_turbulence_model : 0;
     if (tm != 0 && tm != 2 && tm != 3) return OCFD_ERR_UNSUPPORTED;
-    if (p.time_method != 0 && p.time_method != 3 && p.time_method != -1) return OCFD_ERR_UNSUPPORTED;
+    if (p.time_method != 0 && p.time_method != 1 && p.time_method != 3 && p.time_method != -1) return OCFD_ERR_UNSUPPORTED;
+    if (p.if_residual_smoothing != 0 && p.if_residual_smoothing != 1) return OCFD_ERR_ARG;
     if (p.time_method == -1 && p.step_inner_limit < 1) return OCFD_ERR_ARG;
     if (p.iflag_flux < 1 || p.iflag_flux > 6) return OCFD_ERR_ARG;
     int tm0 = p0.if_viscous ? p0.iflag_turbulence_model : 0;
-    if (tm != tm0 || p.if_viscous != p0.if_viscous || p.time_method != p0.time_method || p.precision != p0.precision) return OCFD_ERR_ARG;
+    if (tm != tm0 || p.if_viscous != p0.if_viscous || p.time_method != p0.time_method || p.precision != p0.precision ||
+        p.if_residual_smoothing != p0.if_residual_smoothing)
+      return OCFD_ERR_ARG;
   }
   return OCFD_OK;
 }
@@ -404,6 +414,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   // ---- tables
   h->blk.resize(nblk);
   h->pre_box.assign(nblk + 1, 0); h->pre_cell.assign(nblk + 1, 0); h->pre_face.assign(nblk + 1, 0); h->pre_col.assign(nblk + 1, 0);
+  h->pre_lnj.assign(nblk + 1, 0); h->pre_lnk.assign(nblk + 1, 0);
   long long onode = 0, obci = 0, obcj = 0, obck = 0;
   const int* q = inc;
   for (int b = 0; b < nblk; b++) {
@@ -421,6 +432,8 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     h->pre_face[b + 1] = h->pre_face[b] + (long long)B.nx * B.ny * B.nz;
     h->pre_cell[b + 1] = h->pre_cell[b] + (long long)(B.nx - 1) * (B.ny - 1) * (B.nz - 1);
     h->pre_col[b + 1] = h->pre_col[b] + (long long)(B.ny - 1) * (B.nz - 1);
+    h->pre_lnj[b + 1] = h->pre_lnj[b] + (long long)(B.nx - 1) * (B.nz - 1);
+    h->pre_lnk[b + 1] = h->pre_lnk[b] + (long long)(B.nx - 1) * (B.ny - 1);
     onode += (long long)B.NXn * B.NYn * B.NZn;
     obci += (long long)(B.ny - 1) * (B.nz - 1);
     obcj += (long long)(B.nx - 1) * (B.nz - 1);
@@ -503,6 +516,69 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
       h->bc_rounds.push_back(e0); h->bc_rounds.push_back((int)h->bc_ent.size() - 1); h->bc_rounds.push_back((int)cells);
     }
   }
+  // interface copies.  update_buffer_onemesh copies subface after subface in block order, each
+  // through its own buffer (sub_update_buffer_mpi.f90:55-140).  When no copy touches cells that
+  // another copy writes (every block at least LAP cells thick across its interfaces) the order is
+  // immaterial and one launch does them all.  Otherwise copy t is placed one level after every
+  // earlier copy whose target it reads or writes, and no earlier than any earlier copy that reads
+  // its target; each level gathers all its sources before it scatters.
+  long long max_level_cells = 0;
+  {
+    struct Rng { int b, lo[3], hi[3]; };
+    auto ranges = [](const SubD& S, Rng& R, Rng& W) {
+      int kb[3] = {S.ib, S.jb, S.kb}, ke[3] = {S.ie - 1, S.je - 1, S.ke - 1};
+      int d = (S.face - 1) % 3;
+      if (S.face > 3) kb[d] -= LAPH;
+      ke[d] = kb[d] + LAPH - 1;
+      int kb1[3] = {S.ib1, S.jb1, S.kb1}, ke1[3] = {S.ie1 - 1, S.je1 - 1, S.ke1 - 1};
+      int d1 = (S.face1 - 1) % 3;
+      if (S.face1 <= 3) kb1[d1] -= LAPH;
+      ke1[d1] = kb1[d1] + LAPH - 1;
+      R.b = S.blk; W.b = S.nb1;
+      for (int a = 0; a < 3; a++) { R.lo[a] = kb[a]; R.hi[a] = ke[a]; W.lo[a] = kb1[a]; W.hi[a] = ke1[a]; }
+    };
+    auto meet = [](const Rng& a, const Rng& b) {
+      if (a.b != b.b) return false;
+      for (int q = 0; q < 3; q++)
+        if (a.hi[q] < b.lo[q] || b.hi[q] < a.lo[q]) return false;
+      return true;
+    };
+    std::vector<int> inner;
+    std::vector<Rng> R, W;
+    for (int s = 0; s < ns; s++) {
+      if (h->sub[s].bc >= 0 || h->pre_halo[s + 1] == h->pre_halo[s]) continue;
+      Rng r, w;
+      ranges(h->sub[s], r, w);
+      inner.push_back(s); R.push_back(r); W.push_back(w);
+    }
+    const int ni = (int)inner.size();
+    std::vector<int> lvl(ni, 0);
+    bool ordered = false;
+    for (int t = 0; t < ni; t++) {
+      if (meet(R[t], W[t])) ordered = true;
+      for (int q = 0; q < t; q++) {
+        if (meet(W[q], R[t]) || meet(W[q], W[t])) { lvl[t] = std::max(lvl[t], lvl[q] + 1); ordered = true; }
+        if (meet(R[q], W[t])) { lvl[t] = std::max(lvl[t], lvl[q]); ordered = true; }
+      }
+    }
+    if (ordered) {
+      const int nl = ni ? *std::max_element(lvl.begin(), lvl.end()) + 1 : 0;
+      for (int v = 0; v < nl; v++) {
+        const int e0 = (int)h->halo_ent.size();
+        long long cells = 0;
+        for (int t = 0; t < ni; t++) {
+          if (lvl[t] != v) continue;
+          h->halo_pre.push_back(cells);
+          h->halo_ent.push_back(inner[t]);
+          cells += h->pre_halo[inner[t] + 1] - h->pre_halo[inner[t]];
+        }
+        h->halo_pre.push_back(cells);
+        h->halo_ent.push_back(-1);
+        h->halo_levels.push_back(e0); h->halo_levels.push_back((int)h->halo_ent.size() - 1); h->halo_levels.push_back((int)cells);
+        max_level_cells = std::max(max_level_cells, cells);
+      }
+    }
+  }
   // physical-face flags (set_BcK, sub_init.f90:545-577)
   std::vector<unsigned char> bci(obci, 0), bcj(obcj, 0), bck(obck, 0);
   for (const SubD& S : h->sub) {
@@ -567,10 +643,16 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   h->d_sp = M.alloc<SolveP>(nsolve, e);
   h->d_pre_box = M.alloc<long long>(nblk + 1, e); h->d_pre_cell = M.alloc<long long>(nblk + 1, e);
   h->d_pre_face = M.alloc<long long>(nblk + 1, e); h->d_pre_col = M.alloc<long long>(nblk + 1, e);
+  h->d_pre_lnj = M.alloc<long long>(nblk + 1, e); h->d_pre_lnk = M.alloc<long long>(nblk + 1, e);
   h->d_pre_subcell = M.alloc<long long>(ns + 1, e); h->d_pre_halo = M.alloc<long long>(ns + 1, e);
   h->d_cspre = M.alloc<int>(nsolve + 1, e);
   h->d_bc_ent = M.alloc<int>(std::max<size_t>(1, h->bc_ent.size()), e);
   h->d_bc_pre = M.alloc<long long>(std::max<size_t>(1, h->bc_pre.size()), e);
+  if (!h->halo_levels.empty()) {
+    h->d_halo_ent = M.alloc<int>(h->halo_ent.size(), e);
+    h->d_halo_pre = M.alloc<long long>(h->halo_pre.size(), e);
+    h->d_halo_stage = M.alloc<double>((size_t)NV * max_level_cells, e);
+  }
   h->d_cchunk = M.alloc<int4>(h->cchunk.size(), e); h->d_wchunk = M.alloc<int4>(std::max<size_t>(1, h->wchunk.size()), e);
   h->d_x = M.alloc<double>(onode, e); h->d_y = M.alloc<double>(onode, e); h->d_z = M.alloc<double>(onode, e);
   h->d_Md = M.alloc<double>((size_t)M_COUNT * tf, e);
@@ -578,7 +660,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   h->d_xc = M.alloc<double>(tb, e); h->d_yc = M.alloc<double>(tb, e); h->d_zc = M.alloc<double>(tb, e);
   h->d_bci = M.alloc<unsigned char>(obci, e); h->d_bcj = M.alloc<unsigned char>(obcj, e); h->d_bck = M.alloc<unsigned char>(obck, e);
   h->d_U = M.alloc<double>((size_t)NV * tb, e);
-  if (p->time_method == 3 || p->time_method == -1) h->d_Un = M.alloc<double>((size_t)NV * tb, e);
+  if (p->time_method != 0) h->d_Un = M.alloc<double>((size_t)NV * tb, e);
   if (p->time_method == -1) h->d_Un1 = M.alloc<double>((size_t)NV * tb, e);
   h->d_sfac = M.alloc<double>(2, e);
   h->d_DU = M.alloc<double>((size_t)std::max(NV, 5) * tc, e);
@@ -622,21 +704,27 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
       wcpre[q + 1] = (int)wch.size();
     }
   }
-  if (need_dw && !Xw.empty()) {
-    d_Xw = M.alloc<double>(Xw.size(), e); d_wpre = M.alloc<long long>(nsolve + 1, e);
-    d_wch = M.alloc<WallChunk>(wch.size(), e); d_wcpre = M.alloc<int>(nsolve + 1, e);
+  if (need_dw) {  // a handle without wall nodes still runs the search: every distance is then 1e8
+    d_Xw = M.alloc<double>(std::max<size_t>(3, Xw.size()), e); d_wpre = M.alloc<long long>(nsolve + 1, e);
+    d_wch = M.alloc<WallChunk>(std::max<size_t>(1, wch.size()), e); d_wcpre = M.alloc<int>(nsolve + 1, e);
   }
   if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "allocation"); }
   // ---- uploads
   if ((e = up(h->d_blk, h->blk)) || (e = up(h->d_sub, h->sub)) || (e = up(h->d_sp, h->sps)) ||
       (e = up(h->d_pre_box, h->pre_box)) || (e = up(h->d_pre_cell, h->pre_cell)) || (e = up(h->d_pre_face, h->pre_face)) ||
       (e = up(h->d_pre_col, h->pre_col)) || (e = up(h->d_pre_subcell, h->pre_subcell)) || (e = up(h->d_pre_halo, h->pre_halo)) ||
+      (e = up(h->d_pre_lnj, h->pre_lnj)) || (e = up(h->d_pre_lnk, h->pre_lnk)) ||
       (e = up(h->d_cchunk, h->cchunk)) || (e = up(h->d_cspre, h->cspre)) || (e = up(h->d_bc_ent, h->bc_ent)) || (e = up(h->d_bc_pre, h->bc_pre)) || (e = up(h->d_wchunk, h->wchunk)) || (e = up(h->d_x, hx)) || (e = up(h->d_y, hy)) ||
       (e = up(h->d_z, hz)) || (e = up(h->d_bci, bci)) || (e = up(h->d_bcj, bcj)) || (e = up(h->d_bck, bck))) {
     M.release();
     return cuda_fail(nullptr, e, "upload");
   }
-  if (d_Xw) { cudaMemcpy(d_Xw, Xw.data(), Xw.size() * 8, cudaMemcpyHostToDevice); up(d_wpre, wpre); up(d_wch, wch); up(d_wcpre, wcpre); }
+  if (!h->halo_levels.empty()) { up(h->d_halo_ent, h->halo_ent); up(h->d_halo_pre, h->halo_pre); }
+  if (d_Xw) {
+    if (!Xw.empty()) cudaMemcpy(d_Xw, Xw.data(), Xw.size() * 8, cudaMemcpyHostToDevice);
+    up(d_wpre, wpre); up(d_wcpre, wcpre);
+    if (!wch.empty()) up(d_wch, wch);
+  }
   if (dw && dw[0] && turb != 0) {
     std::vector<double> hdw(tc);
     for (int b = 0; b < nblk; b++) std::memcpy(&hdw[h->pre_cell[b]], dw[b], (h->pre_cell[b + 1] - h->pre_cell[b]) * 8);
@@ -703,11 +791,14 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   }
   // ---- runner
   h->info.nvar = NV; h->info.time_method = p->time_method; h->info.viscous = p->if_viscous; h->info.turb = turb;
+  h->info.smoothing = p->if_residual_smoothing;
   h->info.max_plane = h->max_plane;
   h->info.ncchunk = (int)h->cchunk.size(); h->info.nwchunk = (int)h->wchunk.size();
   h->info.lu_planes = std::getenv("OCFD_LUSGS_PLANES") ? 1 : 0;
   h->info.lu_version = lu_v2 ? 2 : 3;
   h->info.bc_rounds = h->bc_rounds.data(); h->info.nround = (int)(h->bc_rounds.size() / 3);
+  h->info.halo_levels = h->halo_levels.data(); h->info.nhlevel = (int)(h->halo_levels.size() / 3);
+  h->info.halo_ent = h->d_halo_ent; h->info.halo_pre = h->d_halo_pre; h->info.halo_stage = h->d_halo_stage;
   h->info.recon_prim = 1;
   for (int q = 0; q < nsolve; q++) if (ps[q].iflag_reconstruction != 0) h->info.recon_prim = 0;
   {
@@ -762,7 +853,7 @@ extern "C" long long ocfd_footprint(const ocfd_params* p, int nblk, const int* n
   const long long ts = p->precision == OCFD_PREC_MIXED ? 4 : 8;
   long long bytes = 0;
   bytes += 3 * tn * 8 + M_COUNT * tf * 8 + 3 * tc * 8 + 3 * tb * 8;              // geometry (FP64)
-  bytes += NV * tb * 8 * (p->time_method == 3 ? 2 : 1) + std::max(NV, 5LL) * tc * 8;  // U, Un, DU
+  bytes += NV * tb * 8 * (p->time_method == 0 ? 1 : (p->time_method == -1 ? 3 : 2)) + std::max(NV, 5LL) * tc * 8;  // U, Un, Un1, DU
   bytes += ts * (P_COUNT + 2) * tb + ts * (NV + 7) * tc;                          // P, mu, mut, Res, dt, Lc, Lv
   bytes += std::max(ts * 15 * tf, 24 * tf) + (p->if_viscous ? ts * 12 * tf : 0) + (tm ? ts * 6 * tf : 0);
   if (tm == 3) bytes += ts * (2 * tb + tf);

@@ -83,6 +83,11 @@ class RunnerT : public Runner {
     }
     k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
     if (I_.time_method == -1) k_dual_res<T, NV><<<grid_of(tc), 256, 0, st>>>(A);
+    if (I_.smoothing) {  // after the spectral radii, before dt (sub_Residual.f90:110-113); dt does not read Res
+      k_smooth<T, 0><<<grid_of(A.tot_col, 128), 128, 0, st>>>(A);
+      k_smooth<T, 1><<<grid_of(A.tot_lnj, 128), 128, 0, st>>>(A);
+      k_smooth<T, 2><<<grid_of(A.tot_lnk, 128), 128, 0, st>>>(A);
+    }
     if (lusgs) {
       lusgs_sweep(st, false);
       lusgs_sweep(st, true);
@@ -117,7 +122,12 @@ class RunnerT : public Runner {
       const int* R = I_.bc_rounds + 3 * r;
       if (R[2] > 0) k_bc_round<T, NV><<<grid_of(R[2]), 256, 0, st>>>(A, R[0], R[1], (long long)R[2]);
     }
-    if (A.tot_halo > 0) k_halo<T, NV><<<grid_of(A.tot_halo), 256, 0, st>>>(A);
+    if (A.tot_halo > 0 && I_.nhlevel == 0) k_halo<T, NV><<<grid_of(A.tot_halo), 256, 0, st>>>(A);
+    for (int v = 0; v < I_.nhlevel; v++) {
+      const int* H = I_.halo_levels + 3 * v;
+      k_halo_level<T, NV, 0><<<grid_of(H[2]), 256, 0, st>>>(A, I_.halo_ent, I_.halo_pre, H[0], H[1], (long long)H[2], I_.halo_stage);
+      k_halo_level<T, NV, 1><<<grid_of(H[2]), 256, 0, st>>>(A, I_.halo_ent, I_.halo_pre, H[0], H[1], (long long)H[2], I_.halo_stage);
+    }
     k_corner<T, NV><<<A.nblk, 256, 0, st>>>(A);
   }
 
@@ -152,6 +162,14 @@ class RunnerT : public Runner {
       limit(st);
       rec(4);
       bc_halo(st);
+    } else if (I_.time_method == 1) {  // NS_Time_advance_1Euler (sub_time_advance.f90:217-260)
+      k_copy_un<T, NV><<<grid_of((long long)NV * A.tot_box), 256, 0, st>>>(A);
+      residual(st, false);
+      cudaMemsetAsync(A.flags + A.nblk, 0, sizeof(int) * 2 * A.nblk, st);
+      k_update<T, NV, 5><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+      limit(st);
+      bc_halo(st);
+      rec(1); rec(2); rec(3); rec(4);
     } else {
       k_copy_un<T, NV><<<grid_of((long long)NV * A.tot_box), 256, 0, st>>>(A);
       for (int krk = 1; krk <= 3; krk++) {
@@ -179,7 +197,7 @@ class RunnerT : public Runner {
     if (ev) cudaEventRecord(ev[3], st);
   }
   int launches_per_step() const override {
-    int res = 1 + 4 /*inviscid*/ + 1 /*assemble*/;
+    int res = 1 + 4 /*inviscid*/ + 1 /*assemble*/ + (I_.smoothing ? 3 : 0);
     if (I_.viscous) {
       res += 1 + 3 + 1;  // mu, viscous fluxes, amut
       if (I_.turb == 2) res += 6;
@@ -189,10 +207,11 @@ class RunnerT : public Runner {
     int upd = 1 + 1 + (NV == 6 ? 3 : 0);
     int nbc = 0;
     for (int r = 0; r < I_.nround; r++) nbc += I_.bc_rounds[3 * r + 2] > 0;
-    int bch = nbc + 1 + (A_.tot_halo > 0 ? 1 : 0);
+    int bch = nbc + 1 + (A_.tot_halo > 0 ? (I_.nhlevel ? 2 * I_.nhlevel : 1) : 0);
     int n;
     if (I_.time_method == -1) return res + 1 + lu + upd + bch;  // one dual-time inner iteration
     if (I_.time_method == 0) n = res + lu + upd + bch;
+    else if (I_.time_method == 1) n = 1 + res + upd + bch;
     else n = 1 + 3 * (res + upd + bch);
     if (NV >= 6) n += 1;
     return n;

@@ -11,6 +11,7 @@ struct LuArgs;
 
 struct RunInfo {
   int nvar, time_method, viscous, turb;
+  int smoothing;          // 1: upwind implicit residual smoothing after the assembly
   int max_plane;          // max over blocks of nx+ny+nz-3 (last LU-SGS hyperplane)
   int ncchunk, nwchunk;   // reduction chunk counts
   int lu_planes;          // 1: one launch per hyperplane (reference order); 0: pipelined wavefront
@@ -21,6 +22,13 @@ struct RunInfo {
   int recon_prim;         // 1: every solve reconstructs primitive variables
   const int* bc_rounds;   // per boundary round: first entry, end entry, cells
   int nround;
+  // ordered interface-copy levels (empty: all copies independent, one launch); per level the
+  // first entry, end entry and cells; entries index halo_ent / halo_pre on the device
+  const int* halo_levels;
+  int nhlevel;
+  const int* halo_ent;
+  const long long* halo_pre;
+  double* halo_stage;     // NV x (largest level) doubles
 };
 
 class Runner {

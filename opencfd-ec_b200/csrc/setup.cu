@@ -370,7 +370,7 @@ cudaError_t run_geometry(const GeoArgs& a, cudaStream_t st) {
   k_geom_jac<3><<<grid_for(a.tot_face), 256, 0, st>>>(G);
   k_geom_jac<0><<<grid_for(a.tot_face), 256, 0, st>>>(G);
   k_mesh_quality<<<grid_for(a.tot_cell), 256, 0, st>>>(G);
-  if (a.nwall > 0 && a.Xw) {
+  if (a.Xw) {  // set whenever distances are computed here, also without wall nodes (all 1e8 then)
     k_wall_dist_nodes<<<grid_for(a.tot_face), 128, 0, st>>>(G, a.Xw, a.wch, a.wcpre, a.scratch);
     k_wall_dist_cells<<<grid_for(a.tot_cell), 256, 0, st>>>(G, a.scratch);
   }

@@ -807,6 +807,80 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
 }
 
 // ============================================================================================
+// upwind implicit residual smoothing (Residual_smoothing, sub_time_acceleraction.f90:119-217, with
+// tridiagonal 222-241): one thread per grid line of direction DIR, Res(1:5) of the line solved in
+// one forward elimination and one back substitution.  The end cells of a line keep their values
+// (Rs(1) = R(1), Rs(n) = R(n)), so lines of fewer than 3 cells are unchanged.  The elimination
+// factor P(p) is common to the five variables; it is parked in DU plane 0 (free between the
+// update's limiter and the next LU-SGS sweep), and Q_m(p) in Res(m) until the back substitution
+// overwrites it with the smoothed value.
+// ============================================================================================
+template <class T, int DIR>
+__global__ void __launch_bounds__(128) k_smooth(Arena<T> A) {
+  const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
+  const long long nl = DIR == 0 ? A.tot_col : (DIR == 1 ? A.tot_lnj : A.tot_lnk);
+  const long long* pre = DIR == 0 ? A.pre_col : (DIR == 1 ? A.pre_lnj : A.pre_lnk);
+  OCFD_GRID_STRIDE(g, nl) {
+    const int b = find_blk(pre, A.nblk, g);
+    const BlkD& B = A.blk[b];
+    const long long l = g - __ldg(pre + b);
+    const int nxm = B.nx - 1, nym = B.ny - 1;
+    int i = 1, j = 1, k = 1, n;
+    long long sc, sf, sb;  // strides along the line in the cell, face and box index spaces
+    if (DIR == 0) { j = (int)(l % nym) + 1; k = (int)(l / nym) + 1; n = nxm; sc = 1; sf = 1; sb = 1; }
+    else if (DIR == 1) { i = (int)(l % nxm) + 1; k = (int)(l / nxm) + 1; n = nym; sc = nxm; sf = B.nx; sb = B.NX; }
+    else { i = (int)(l % nxm) + 1; j = (int)(l / nxm) + 1; n = B.nz - 1; sc = (long long)nxm * nym; sf = (long long)B.nx * B.ny; sb = (long long)B.NX * B.NY; }
+    if (n < 3) continue;
+    const long long c1 = cix(B, i, j, k), f1 = fix_(B, i, j, k), b1 = bix(B, i, j, k);
+    const T* Ld = A.Lc + DIR * tc;
+    const T* La = A.Lc + (DIR == 0 ? 1 : 0) * tc;
+    const T* Lb = A.Lc + (DIR == 2 ? 1 : 2) * tc;
+    const T* n1 = A.M + (M_NI1 + 3 * DIR) * tf;
+    const T* n2 = A.M + (M_NI2 + 3 * DIR) * tf;
+    const T* n3 = A.M + (M_NI3 + 3 * DIR) * tf;
+    double Pp = 0.0, Qp[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) Qp[m] = (double)A.Res[m * tc + c1];
+    for (int q = 2; q <= n - 1; q++) {
+      const long long c = c1 + (q - 1) * sc, f = f1 + (q - 1) * sf, bx = b1 + (q - 1) * sb;
+      const double ld = (double)Ld[c];
+      double ei = 1.0, r = ld / (double)La[c];
+      if (r < ei) ei = r;
+      r = ld / (double)Lb[c];
+      if (r < ei) ei = r;
+      const double uu = A.P[P_U * tb + bx], vv = A.P[P_V * tb + bx], ww = A.P[P_W * tb + bx], cc = A.P[P_C * tb + bx];
+      const double Mn = 0.5 * (uu * ((double)n1[f] + (double)n1[f + sf]) + vv * ((double)n2[f] + (double)n2[f + sf]) +
+                               ww * ((double)n3[f] + (double)n3[f + sf])) / cc;
+      double as, bs, cs;
+      if (Mn > 1.0) { as = -ei; bs = 1.0 + ei; cs = 0.0; }
+      else if (Mn < -1.0) { as = 0.0; bs = 1.0 + ei; cs = -ei; }
+      else { as = -ei; bs = 1.0 + 2.0 * ei; cs = -ei; }
+      const double tmp = 1.0 / (as * Pp + bs);
+      Pp = -cs * tmp;
+      A.DU[c] = Pp;
+#pragma unroll
+      for (int m = 0; m < 5; m++) {
+        Qp[m] = ((double)A.Res[m * tc + c] - as * Qp[m]) * tmp;
+        A.Res[m * tc + c] = (T)Qp[m];
+      }
+    }
+    double Rn[5];
+    const long long cn = c1 + (n - 1) * sc;
+#pragma unroll
+    for (int m = 0; m < 5; m++) Rn[m] = (double)A.Res[m * tc + cn];
+    for (int q = n - 1; q >= 2; q--) {
+      const long long c = c1 + (q - 1) * sc;
+      const double P = A.DU[c];
+#pragma unroll
+      for (int m = 0; m < 5; m++) {
+        Rn[m] = P * Rn[m] + (double)A.Res[m * tc + c];
+        A.Res[m * tc + c] = (T)Rn[m];
+      }
+    }
+  }
+}
+
+// ============================================================================================
 // LU-SGS (du_LU_SGS, sub_LU_SGS.f90:4-129): one launch per hyperplane i+j+k = plane, all blocks
 // ============================================================================================
 __device__ __forceinline__ void comput_DFn(int NV, double* DF, const double* U, const double* DU, double n1, double n2, double n3, double gamma) {
@@ -910,7 +984,7 @@ __device__ __forceinline__ bool lim_bad(const SolveP& s, double d, double u, dou
   return d < s.ldmin || p < s.lpmin || d > s.ldmax || p > s.lpmax || fabs(u) > s.lumax || fabs(v) > s.lumax || fabs(w) > s.lumax;
 }
 
-template <class T, int NV, int MODE>  // MODE 0: LU-SGS; 1,2,3: RK3 stage KRK; 4: dual-time inner iteration
+template <class T, int NV, int MODE>  // MODE 0: LU-SGS; 1,2,3: RK3 stage KRK; 4: dual-time inner iteration; 5: explicit Euler
 __global__ void k_update(Arena<T> A) {
   const long long tb = A.tot_box, tc = A.tot_cell;
   OCFD_GRID_STRIDE(g, tc) {
@@ -930,6 +1004,9 @@ __global__ void k_update(Arena<T> A) {
         double cur = A.U[m * tb + c];
         if (m >= 5) cur = clamp0(cur);
         u = cur + A.DU[m * tc + g];
+      } else if (MODE == 5) {  // U = Un + dt Res/vol (sub_time_advance.f90:238-239)
+        double du = (double)A.Res[m * tc + g] / (double)A.vol[g];
+        u = A.Un[m * tb + c] + (double)A.dt[g] * du;
       } else {
         const double Ra = MODE == 1 ? 1.0 : (MODE == 2 ? 3.0 / 4.0 : 1.0 / 3.0);
         const double Rb = MODE == 1 ? 1.0 : (MODE == 2 ? 1.0 / 4.0 : 2.0 / 3.0);
@@ -1251,35 +1328,58 @@ __global__ void k_bc_round(Arena<T> A, int e0, int e1, long long ncell) {
 // block-interface halo (Umessage_send_mpi, sub_update_buffer_mpi.f90:42-141): LAP ghost layers
 // of every inner subface are copied from the partner's interior with the (L1,L2,L3) permutation
 // ============================================================================================
+template <class T>
+__device__ __forceinline__ void halo_map(const Arena<T>& A, const SubD& S, long long l, long long& cs, long long& ct) {
+  // source: this block's LAP layers next to the face; target: the partner's LAP ghost layers
+  int kb[3] = {S.ib, S.jb, S.kb}, ke[3] = {S.ie - 1, S.je - 1, S.ke - 1};
+  int d = (S.face - 1) % 3;
+  if (S.face > 3) kb[d] = kb[d] - LAP;
+  ke[d] = kb[d] + LAP - 1;
+  int kb1[3] = {S.ib1, S.jb1, S.kb1}, ke1[3] = {S.ie1 - 1, S.je1 - 1, S.ke1 - 1};
+  int d1 = (S.face1 - 1) % 3;
+  if (S.face1 <= 3) kb1[d1] = kb1[d1] - LAP;
+  ke1[d1] = kb1[d1] + LAP - 1;
+  int n0 = ke1[0] - kb1[0] + 1, n1 = ke1[1] - kb1[1] + 1;
+  int ka[3] = {(int)(l % n0), (int)((l / n0) % n1), (int)(l / ((long long)n0 * n1))};
+  int L[3] = {abs(S.L1), abs(S.L2), abs(S.L3)};
+  int P[3] = {S.L1 >= 0 ? 1 : -1, S.L2 >= 0 ? 1 : -1, S.L3 >= 0 ? 1 : -1};
+  int src[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) src[q] = (P[q] > 0 ? kb[q] : ke[q]) + ka[L[q] - 1] * P[q];
+  cs = bix(A.blk[S.blk], src[0], src[1], src[2]);
+  ct = bix(A.blk[S.nb1], kb1[0] + ka[0], kb1[1] + ka[1], kb1[2] + ka[2]);
+}
+
+// every interface copy in one launch: valid when no copy reads or writes cells another copy
+// writes (blocks at least LAP cells thick across their interfaces)
 template <class T, int NV>
 __global__ void k_halo(Arena<T> A) {
   const long long tb = A.tot_box;
   OCFD_GRID_STRIDE(g, A.tot_halo) {
     int s = find_blk(A.pre_halo, A.nsub, g);
-    const SubD S = A.sub[s];
-    long long l = g - A.pre_halo[s];
-    // source: this block's LAP interior layers; target: the partner's LAP ghost layers
-    int kb[3] = {S.ib, S.jb, S.kb}, ke[3] = {S.ie - 1, S.je - 1, S.ke - 1};
-    int d = (S.face - 1) % 3;
-    if (S.face > 3) kb[d] = kb[d] - LAP;
-    ke[d] = kb[d] + LAP - 1;
-    int kb1[3] = {S.ib1, S.jb1, S.kb1}, ke1[3] = {S.ie1 - 1, S.je1 - 1, S.ke1 - 1};
-    int d1 = (S.face1 - 1) % 3;
-    if (S.face1 <= 3) kb1[d1] = kb1[d1] - LAP;
-    ke1[d1] = kb1[d1] + LAP - 1;
-    int n0 = ke1[0] - kb1[0] + 1, n1 = ke1[1] - kb1[1] + 1;
-    int ka[3] = {(int)(l % n0), (int)((l / n0) % n1), (int)(l / ((long long)n0 * n1))};
-    int L[3] = {abs(S.L1), abs(S.L2), abs(S.L3)};
-    int P[3] = {S.L1 >= 0 ? 1 : -1, S.L2 >= 0 ? 1 : -1, S.L3 >= 0 ? 1 : -1};
-    int src[3];
-#pragma unroll
-    for (int q = 0; q < 3; q++) src[q] = (P[q] > 0 ? kb[q] : ke[q]) + ka[L[q] - 1] * P[q];
-    const BlkD& B = A.blk[S.blk];
-    const BlkD& B1 = A.blk[S.nb1];
-    long long cs = bix(B, src[0], src[1], src[2]);
-    long long ct = bix(B1, kb1[0] + ka[0], kb1[1] + ka[1], kb1[2] + ka[2]);
+    long long cs, ct;
+    halo_map(A, A.sub[s], g - A.pre_halo[s], cs, ct);
 #pragma unroll
     for (int m = 0; m < NV; m++) A.U[m * tb + ct] = A.U[m * tb + cs];
+  }
+}
+
+// one level of ordered interface copies: PHASE 0 gathers the level's sources into stage, PHASE 1
+// scatters them, so a copy whose source reaches ghost cells reads them as the reference's
+// subface-by-subface order leaves them (update_buffer_onemesh, sub_update_buffer_mpi.f90:55-140).
+// ent[e0..e1) are the level's subfaces, pre[e] the first staged cell of entry e (from 0).
+template <class T, int NV, int PHASE>
+__global__ void k_halo_level(Arena<T> A, const int* ent, const long long* pre, int e0, int e1, long long cells, double* stage) {
+  const long long tb = A.tot_box;
+  OCFD_GRID_STRIDE(g, cells) {
+    int e = e0 + find_blk(pre + e0, e1 - e0, g);
+    long long cs, ct;
+    halo_map(A, A.sub[ent[e]], g - pre[e], cs, ct);
+#pragma unroll
+    for (int m = 0; m < NV; m++) {
+      if (PHASE == 0) stage[m * cells + g] = A.U[m * tb + cs];
+      else A.U[m * tb + ct] = stage[m * cells + g];
+    }
   }
 }
 

@@ -59,7 +59,7 @@ class OcfdParams(ctypes.Structure):
         ("cp", ctypes.c_double),
         ("res_inner_limit", ctypes.c_double),
         ("step_inner_limit", ctypes.c_int),
-        ("reserved", ctypes.c_int),
+        ("if_residual_smoothing", ctypes.c_int),
     ]
 
     def copy(self):

@@ -1075,13 +1075,22 @@ static void halo(Case& C) {
       int ks[3];
       for (int q = 0; q < 3; q++) ks[q] = P[q] > 0 ? kb[q] : ke[q];
       Block& B1 = C.B[Bc.nb1 - 1];
+      // the whole copy goes through a buffer first (Usend, 97-111), then into the target (126-134):
+      // a source range that reaches ghost cells sees the values before this copy
+      std::vector<double> Usend;
+      Usend.reserve((size_t)NV * (ke1[0] - kb1[0] + 1) * (ke1[1] - kb1[1] + 1) * (ke1[2] - kb1[2] + 1));
       for (int kk = kb1[2]; kk <= ke1[2]; kk++)
         for (int jj = kb1[1]; jj <= ke1[1]; jj++)
           for (int ii = kb1[0]; ii <= ke1[0]; ii++) {
             int ka[3] = {ii - kb1[0], jj - kb1[1], kk - kb1[2]};
             int i1 = ks[0] + ka[L[0] - 1] * P[0], j1 = ks[1] + ka[L[1] - 1] * P[1], k1 = ks[2] + ka[L[2] - 1] * P[2];
-            for (int m = 1; m <= NV; m++) B1.U(m, ii, jj, kk) = B.U(m, i1, j1, k1);
+            for (int m = 1; m <= NV; m++) Usend.push_back(B.U(m, i1, j1, k1));
           }
+      size_t q = 0;
+      for (int kk = kb1[2]; kk <= ke1[2]; kk++)
+        for (int jj = kb1[1]; jj <= ke1[1]; jj++)
+          for (int ii = kb1[0]; ii <= ke1[0]; ii++)
+            for (int m = 1; m <= NV; m++) B1.U(m, ii, jj, kk) = Usend[q++];
     }
   }
   for (Block& B : C.B) {  // get_U_conner 515-549
@@ -1751,6 +1760,80 @@ static void comput_dt(Case& C, Block& B, Work& W) {  // sub_time_acceleraction.f
       }
 }
 
+// tridiagonal (sub_time_acceleraction.f90:222-241): a(i) Rs(i-1) + b(i) Rs(i) + c(i) Rs(i+1) = R(i) on
+// i = 2..n-1 with the end values held, Rs(1) = R(1), Rs(n) = R(n); arrays 1-based (element 0 unused)
+static void tridiagonal(int n, const double* a, const double* b, const double* c, const double* R, double* Rs) {
+  std::vector<double> P(n + 1), Q(n + 1);
+  P[1] = 0.0; Q[1] = R[1];
+  P[n] = 0.0; Q[n] = R[n];
+  for (int i = 2; i <= n; i++) {
+    double tmp = 1.0 / (a[i] * P[i - 1] + b[i]);
+    P[i] = -c[i] * tmp;
+    Q[i] = (R[i] - a[i] * Q[i - 1]) * tmp;
+  }
+  Rs[n] = R[n];
+  Rs[1] = R[1];
+  for (int i = n - 1; i >= 2; i--) Rs[i] = P[i] * Rs[i + 1] + Q[i];
+}
+
+// upwind implicit residual smoothing (Residual_smoothing, sub_time_acceleraction.f90:119-217): per
+// line in i, then j, then k, coefficients from the spectral-radius ratio ei = min(1, L_d/L_a, L_d/L_b)
+// and the cell's normal Mach number on the averaged face normal; Res(1:5) only
+static void residual_smoothing(Case& C, Block& B, Work& W) {
+  (void)C;
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const double epsl = 1.0;
+  const int nmax = std::max(nx, std::max(ny, nz)) + 1;
+  std::vector<double> as(nmax), bs(nmax), cs(nmax), R(nmax), Rs(nmax);
+  auto coef = [&](int q, double ei, double Mn) {
+    if (Mn > 1.0) { as[q] = -ei; bs[q] = 1.0 + ei; cs[q] = 0.0; }
+    else if (Mn < -1.0) { as[q] = 0.0; bs[q] = 1.0 + ei; cs[q] = -ei; }
+    else { as[q] = -ei; bs[q] = 1.0 + 2.0 * ei; cs[q] = -ei; }
+  };
+  for (int k = 1; k <= nz - 1; k++)  // i direction, 131-156
+    for (int j = 1; j <= ny - 1; j++) {
+      for (int i = 1; i <= nx - 1; i++) {
+        double ei = epsl * std::min(std::min(1.0, W.Lci(i, j, k) / W.Lcj(i, j, k)), W.Lci(i, j, k) / W.Lck(i, j, k));
+        double Mn = 0.5 * (W.uu(i, j, k) * (B.ni1(i, j, k) + B.ni1(i + 1, j, k)) + W.v(i, j, k) * (B.ni2(i, j, k) + B.ni2(i + 1, j, k)) +
+                           W.w(i, j, k) * (B.ni3(i, j, k) + B.ni3(i + 1, j, k))) / W.cc(i, j, k);
+        coef(i, ei, Mn);
+      }
+      for (int m = 1; m <= 5; m++) {
+        for (int i = 1; i <= nx - 1; i++) R[i] = B.Res(m, i, j, k);
+        tridiagonal(nx - 1, as.data(), bs.data(), cs.data(), R.data(), Rs.data());
+        for (int i = 1; i <= nx - 1; i++) B.Res(m, i, j, k) = Rs[i];
+      }
+    }
+  for (int k = 1; k <= nz - 1; k++)  // j direction, 159-184
+    for (int i = 1; i <= nx - 1; i++) {
+      for (int j = 1; j <= ny - 1; j++) {
+        double ei = epsl * std::min(std::min(1.0, W.Lcj(i, j, k) / W.Lci(i, j, k)), W.Lcj(i, j, k) / W.Lck(i, j, k));
+        double Mn = 0.5 * (W.uu(i, j, k) * (B.nj1(i, j, k) + B.nj1(i, j + 1, k)) + W.v(i, j, k) * (B.nj2(i, j, k) + B.nj2(i, j + 1, k)) +
+                           W.w(i, j, k) * (B.nj3(i, j, k) + B.nj3(i, j + 1, k))) / W.cc(i, j, k);
+        coef(j, ei, Mn);
+      }
+      for (int m = 1; m <= 5; m++) {
+        for (int j = 1; j <= ny - 1; j++) R[j] = B.Res(m, i, j, k);
+        tridiagonal(ny - 1, as.data(), bs.data(), cs.data(), R.data(), Rs.data());
+        for (int j = 1; j <= ny - 1; j++) B.Res(m, i, j, k) = Rs[j];
+      }
+    }
+  for (int j = 1; j <= ny - 1; j++)  // k direction, 186-213
+    for (int i = 1; i <= nx - 1; i++) {
+      for (int k = 1; k <= nz - 1; k++) {
+        double ei = epsl * std::min(std::min(1.0, W.Lck(i, j, k) / W.Lci(i, j, k)), W.Lck(i, j, k) / W.Lcj(i, j, k));
+        double Mn = 0.5 * (W.uu(i, j, k) * (B.nk1(i, j, k) + B.nk1(i, j, k + 1)) + W.v(i, j, k) * (B.nk2(i, j, k) + B.nk2(i, j, k + 1)) +
+                           W.w(i, j, k) * (B.nk3(i, j, k) + B.nk3(i, j, k + 1))) / W.cc(i, j, k);
+        coef(k, ei, Mn);
+      }
+      for (int m = 1; m <= 5; m++) {
+        for (int k = 1; k <= nz - 1; k++) R[k] = B.Res(m, i, j, k);
+        tridiagonal(nz - 1, as.data(), bs.data(), cs.data(), R.data(), Rs.data());
+        for (int k = 1; k <= nz - 1; k++) B.Res(m, i, j, k) = Rs[k];
+      }
+    }
+}
+
 static void comput_DFn(int NV, double* DF, const double* U, const double* DU, double n1, double n2, double n3, double gamma) {  // sub_LU_SGS.f90:135-157
   double U2[7];
   for (int m = 0; m < NV; m++) U2[m] = U[m] + DU[m];
@@ -1883,6 +1966,7 @@ static int residual_block(Case& C, Block& B, bool lusgs, double Sfac = 0.0, doub
             B.Res(m, i, j, k) = B.Res(m, i, j, k) - (3.0 * B.U(m, i, j, k) - 4.0 * B.Un(m, i, j, k) + B.Un1(m, i, j, k)) * B.vol(i, j, k) * Sfac;
   }
   comput_Lijk(C, B, W);
+  if (C.P.if_residual_smoothing == 1) residual_smoothing(C, B, W);  // sub_Residual.f90:111-113
   comput_dt(C, B, W);
   if (lusgs) du_LU_SGS(C, B, W, Sfac1);
   return 0;
@@ -2008,6 +2092,27 @@ static int advance_lusgs(Case& C) {  // sub_time_advance.f90:75-118
   return 0;
 }
 
+static int advance_euler1(Case& C) {  // NS_Time_advance_1Euler, sub_time_advance.f90:217-260
+  int NV = C.NVAR;
+  set_Un(C);
+  for (Block& B : C.B) residual_block(C, B, false);
+  for (Block& B : C.B)
+    for (int k = 1; k <= B.nz - 1; k++)
+      for (int j = 1; j <= B.ny - 1; j++)
+        for (int i = 1; i <= B.nx - 1; i++)
+          for (int m = 1; m <= NV; m++) {
+            double du = B.Res(m, i, j, k) / B.vol(i, j, k);
+            B.U(m, i, j, k) = B.Un(m, i, j, k) + B.dt(i, j, k) * du;
+          }
+  if (C.P.iflag_limit_flow == 1) limit_flow(C);
+  int rc = boundary_all(C);
+  if (rc) return rc;
+  halo(C);
+  C.tt = C.tt + C.P.dt_global;
+  C.Kstep = C.Kstep + 1;
+  return 0;
+}
+
 static int advance_rk3(Case& C) {  // sub_time_advance.f90:265-326
   int NV = C.NVAR;
   set_Un(C);
@@ -2084,6 +2189,7 @@ static int advance_dual(Case& C) {  // NS_Time_Dual_LU_SGS, sub_time_advance.f90
 static int advance(Case& C) {  // NS_Time_advance, sub_time_advance.f90:6-23
   int rc;
   if (C.P.time_method == 0) rc = advance_lusgs(C);
+  else if (C.P.time_method == 1) rc = advance_euler1(C);
   else if (C.P.time_method == 3) rc = advance_rk3(C);
   else if (C.P.time_method == -1) rc = advance_dual(C);
   else { C.err = "time method not supported"; return OCFD_ERR_UNSUPPORTED; }

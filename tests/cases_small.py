@@ -24,6 +24,13 @@ def small_cases():
         "foil_sa_dual": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=4, turb=2, time_method=-1, dt_global=0.05,
                                               step_inner_limit=4, res_inner_limit=1e-14),
         "bump_dual": lambda: cases.config1(scale=0.25, time_method=-1, dt_global=0.2, step_inner_limit=3, res_inner_limit=1e-14),
+        "bump_euler1": lambda: cases.config1(scale=0.25, cuts_i=(12,), time_method=1, cfl=0.5),
+        "bump_euler1_smooth": lambda: cases.config1(scale=0.25, time_method=1, cfl=1.0, if_residual_smoothing=1),
+        "foil_sa_lusgs_smooth": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=4, turb=2, if_residual_smoothing=1),
+        "foil_lam_rk3_smooth": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=4, turb=0, time_method=3, cfl=1.5,
+                                                     if_residual_smoothing=1),
+        "bump_dual_smooth": lambda: cases.config1(scale=0.25, cuts_i=(12,), time_method=-1, dt_global=0.2, step_inner_limit=3,
+                                                  res_inner_limit=1e-14, if_residual_smoothing=1),
     }
 
 

@@ -5,7 +5,7 @@ from ocfd_b200.connectivity import BC_FARFIELD, BC_SYMMETRY, InpBlock, InpSub, i
 from ocfd_b200.meshgen import Case
 
 
-def wavy_box(nx=17, ny=13, nz=9, amp=0.02, seed=7, nblk=1):
+def wavy_box(nx=17, ny=13, nz=9, amp=0.02, seed=7, nblk=1, cuts=None):
     """Unit box with smooth sinusoidal node displacement (closed-form, so shared node planes of
     split blocks coincide exactly), far-field on every physical face; cut into nblk blocks in i."""
     rng = np.random.default_rng(seed)
@@ -16,7 +16,10 @@ def wavy_box(nx=17, ny=13, nz=9, amp=0.02, seed=7, nblk=1):
     Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
     s = np.sin(np.pi * X) * np.sin(np.pi * Y) * np.sin(2 * np.pi * Z)
     P = np.stack([X + amp * s * np.cos(ph[0]), Y + amp * s * np.cos(ph[1]), Z + amp * s * np.cos(ph[2])])
-    cuts = [1] + [int(round(1 + (nx - 1) * q / nblk)) for q in range(1, nblk)] + [nx]
+    if cuts is None:
+        cuts = [int(round(1 + (nx - 1) * q / nblk)) for q in range(1, nblk)]
+    cuts = [1] + list(cuts) + [nx]
+    nblk = len(cuts) - 1
     xyz, inp = [], []
     for b in range(nblk):
         i0, i1 = cuts[b], cuts[b + 1]

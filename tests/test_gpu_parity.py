@@ -133,3 +133,26 @@ def test_mixed_precision_close_to_fp64(gpu, oracle, name):
     assert state_err(o, g) <= 1e-4
     g.close()
     o.close()
+
+
+@pytest.mark.parametrize("turb,scheme", [(0, 7), (2, 5)])
+def test_ragged_blocks_down_to_one_cell(gpu, oracle, turb, scheme):
+    """Uneven blocks down to a single cell layer (a block of 2 nodes in i) and a 2-cell block, no
+    wall (wall distance 1e8 everywhere): the interface copies of blocks thinner than LAP read
+    ghost cells that other copies write, and the GPU orders them as the reference's
+    subface-by-subface loop does (WENO5 reads all LAP ghost layers); the wavefront tiles, BC
+    rounds and norms handle the thin blocks as the oracle does."""
+    from meshes import wavy_box
+    from ocfd_b200.params import make_params
+    case = wavy_box(nx=21, ny=11, nz=7, cuts=(2, 4, 15))       # blocks of 1, 2, 11, 6 cells in i
+    assert [d[0] - 1 for d in case.dims] == [1, 2, 11, 6]
+    p = make_params(ma=0.5, aoa=3.0, if_viscous=int(turb > 0), iflag_turbulence_model=turb, iflag_scheme=scheme, iflag_flux=4,
+                    re=1e5, cfl=2.0)
+    o, g = oracle.OracleCase(p, case), gpu.Solver(p, case)
+    for _ in range(4):
+        o.advance(1)
+        g.advance(1)
+        np.testing.assert_allclose(g.residual()[1][:p.nvar], o.residual()[1][:p.nvar], rtol=1e-11, atol=1e-300)
+    assert state_err(o, g) <= 1e-11
+    g.close()
+    o.close()

@@ -79,8 +79,11 @@ def test_create_rejects_bad_arguments_before_touching_the_device(clib):
     q.iflag_turbulence_model = 1   # Baldwin-Lomax: not on the hot path
     assert call(q, 1, nijk) == OCFD_ERR_UNSUPPORTED
     q = p.copy()
-    q.time_method = 1              # first-order explicit Euler (Time_Euler1): not built
+    q.time_method = 2              # no such time method (sub_time_advance.f90:10-19)
     assert call(q, 1, nijk) == OCFD_ERR_UNSUPPORTED
+    q = p.copy()
+    q.if_residual_smoothing = 2
+    assert call(q, 1, nijk) == OCFD_ERR_ARG
     q = p.copy()
     q.iflag_flux = 9
     assert call(q, 1, nijk) == OCFD_ERR_ARG

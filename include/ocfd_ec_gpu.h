@@ -39,6 +39,7 @@ extern "C" {
 #define OCFD_ERR_TIMEOUT (-5)     /* a bounded device-side wait gave up                       */
 #define OCFD_ERR_UNSUPPORTED (-6) /* boundary type / model outside the implemented hot path  */
 #define OCFD_ERR_NOSYM (-7)       /* a required symbol or library is missing                  */
+#define OCFD_ERR_COMM (-8)        /* an exchange or all-reduce callback of a sharded handle failed */
 
 /* numeric constants of the reference (sub_modules.f90:21-47) */
 #define OCFD_SCHEME_UD1 0
@@ -250,6 +251,50 @@ int ocfd_synchronize(ocfd_handle* h);
  * OCFD_ERR_NAN without the cell location (ocfd_residual reports it).
  */
 int ocfd_residual_static(ocfd_handle* h, double* res_max, double* res_rms);
+
+/* ---- block-sharded solves: one case split over ranks by whole blocks ----------------------
+ *
+ * The reference's MPI mode (sub_partation_mpi.f90:126-158 assigns whole blocks to ranks;
+ * Umessage_send_mpi / Umessage_recv_mpi, sub_update_buffer_mpi.f90:42-211, exchange the LAP ghost
+ * layers of interfaces between blocks on different ranks; comput_max_Res_onemesh and comput_force
+ * all-reduce their sums, sub_time_advance.f90:373-374, sub_Post.f90:202).  Every rank creates one
+ * handle with the whole case description and owner[] (rank of each block); the handle holds only
+ * the blocks with owner == rank, numbered 0.. in ascending global order (ocfd_part_blocks gives
+ * the map), and ocfd_get_state / ocfd_set_state / ocfd_limiter_status / ocfd_get_array take
+ * those local numbers.  Copies between the handle's own blocks stay on the device; copies to and
+ * from other ranks go through two device buffers handed to comm->exchange once per halo update
+ * (each step, each RK3 stage, each dual-time inner iteration, and at initialisation).
+ * ocfd_create_part, ocfd_advance, ocfd_init_flow, ocfd_residual, ocfd_forces and ocfd_profile
+ * are collective: every rank calls them in the same order.  Norms and forces are all-reduced
+ * through comm->allreduce (RMS over the cells of the whole case; a NaN or a timed-out wait on
+ * any rank is reported on all).  Single solve only; steps run without a CUDA graph; blocks must
+ * be at least LAP (4) cells thick across interfaces between ranks (OCFD_ERR_UNSUPPORTED
+ * otherwise), so that the exchange order cannot matter.
+ */
+typedef struct ocfd_comm {
+  /* send[send_off[q] .. send_off[q+1]) goes to rank peers[q], recv[recv_off[q] .. recv_off[q+1])
+   * comes from it; device pointers, offsets in doubles, npeer + 1 offsets each.  Called on the
+   * handle's host thread after the pack kernel is queued on stream (a cudaStream_t); the transfer
+   * is queued on that stream (NCCL send/recv) or complete when the call returns.  0 = ok. */
+  int (*exchange)(void* user, void* stream, int npeer, const int* peers, const double* send, const long long* send_off,
+                  double* recv, const long long* recv_off);
+  /* in-place all-reduce of n host doubles over the ranks; op 0 = sum, 1 = max.  0 = ok. */
+  int (*allreduce)(void* user, double* buf, int n, int op);
+  void* user;
+} ocfd_comm;
+
+int ocfd_create_part(const ocfd_params* p, int nblk, const int* nijk, const double* const* xyz, const int* nsub,
+                     const int* inc, const double* const* dw, const int* owner, int rank, const ocfd_comm* comm,
+                     ocfd_handle** h);
+/* The exchange plan of rank `rank` without creating anything (host only, no device call): returns
+ * the number of peers (or an error code); when the pointers are not NULL, peers[npeer] and the
+ * per-peer offsets send_off / recv_off[npeer + 1] in CELLS of the exchange buffers (NVAR doubles
+ * per cell).  ocfd_create_part hands the exchange callback the same plan in doubles. */
+int ocfd_part_plan(int nblk, const int* nijk, const int* nsub, const int* inc, const int* owner, int rank, int* peers,
+                   long long* send_off, long long* recv_off);
+/* Number of blocks the handle holds; their global (0-based) block numbers into global_ids when
+ * it is not NULL.  A handle from ocfd_create holds every block (identity map). */
+int ocfd_part_blocks(const ocfd_handle* h, int* global_ids);
 
 /* Library build/ABI information: "ocfd-b200 <abi> sm_100a ..." */
 const char* ocfd_version(void);

@@ -51,6 +51,30 @@ constexpr int LAPH = 4;
 
 }  // namespace
 
+// One rank's share of a block-sharded case (ocfd_create_part)
+struct PartCtx {
+  int rank = 0;
+  std::vector<int> loc2glob;             // local block -> global block
+  long long ncell_global = 0;            // interior cells of the whole case (RMS denominator)
+  std::vector<std::vector<double>> X;    // per local block: node coordinates with the ghost layer
+  std::vector<double> Xw;                // wall nodes of the whole case
+  std::vector<int> send_ent;             // local subface of each outgoing copy (grouped by peer)
+  std::vector<long long> send_pre;       // their cell prefix sums (closing entry included)
+  std::vector<SubD> recv_sub;            // incoming copies: the remote subface, nb1 = local block
+  std::vector<long long> recv_pre;
+  std::vector<int> peers;                // ranks exchanged with, ascending
+  std::vector<long long> send_off, recv_off;  // per peer, in doubles (npeer + 1 each)
+  ocfd_comm comm{};
+  bool xchg = true;                      // false while the tile-width autotuner runs
+  int comm_err = 0;
+  int* d_send_ent = nullptr;
+  long long* d_send_pre = nullptr;
+  SubD* d_recv_sub = nullptr;
+  long long* d_recv_pre = nullptr;
+  double* d_send = nullptr;
+  double* d_recv = nullptr;
+};
+
 struct ocfd_handle {
   ocfd_params P;                   // parameters of solve 0
   std::vector<ocfd_params> Ps;     // per solve
@@ -109,6 +133,7 @@ struct ocfd_handle {
   cudaStream_t st = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph = nullptr;
+  std::unique_ptr<PartCtx> part;   // set for block-sharded handles
   int kstep = 0;
   double tt = 0.0;
   std::string err;
@@ -219,6 +244,7 @@ static void coordinate_ghosts(const std::vector<BlkD>& blk, const std::vector<Su
     }
   }
   for (size_t b = 0; b < blk.size(); b++) {
+    if (X[b].empty()) continue;  // a block of another rank whose nodes no ghost layer here reaches
     int nx = blk[b].nx, ny = blk[b].ny, nz = blk[b].nz;
     for (int c = 0; c < 3; c++) {
       auto x = [&](int i, int j, int k) -> double& { return at((int)b, c, i, j, k); };
@@ -387,8 +413,20 @@ static int check_params(const ocfd_params* ps, int nsolve) {
   return OCFD_OK;
 }
 
+// the exchange hook of a sharded handle's runner: hands the packed buffers to the caller's
+// exchange callback; returns 1 when the receive buffer holds this update's copies
+static int part_exchange(void* ctx, cudaStream_t st) {
+  ocfd_handle* h = (ocfd_handle*)ctx;
+  PartCtx& P = *h->part;
+  if (!P.xchg) return 0;
+  int rc = P.comm.exchange(P.comm.user, (void*)st, (int)P.peers.size(), P.peers.data(), P.d_send, P.send_off.data(), P.d_recv,
+                           P.recv_off.data());
+  if (rc && !P.comm_err) P.comm_err = rc;
+  return rc ? 0 : 1;
+}
+
 static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, const int* nijk, const double* const* xyz, const int* nsub,
-                       const int* inc, const double* const* dw, ocfd_handle** out) {
+                       const int* inc, const double* const* dw, ocfd_handle** out, std::unique_ptr<PartCtx> part = nullptr) {
   if (!ps || nsolve <= 0 || !nblk_s || !nijk || !xyz || !nsub || !inc || !out) return OCFD_ERR_ARG;
   int nblk = 0;
   for (int q = 0; q < nsolve; q++) {
@@ -399,6 +437,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   std::unique_ptr<ocfd_handle> hp(new ocfd_handle());
   ocfd_handle* h = hp.get();
   h->err.reserve(512);
+  h->part = std::move(part);
   const ocfd_params* p = ps;
   h->P = ps[0];
   h->Ps.assign(ps, ps + nsolve);
@@ -449,8 +488,9 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
       if (S.face < 1 || S.face > 6) return fail(nullptr, OCFD_ERR_ARG, "bad face");
       // partner block numbers are 1-based within the solve
       const int sb0 = h->sblk0[B.solve], sbn = h->sblk0[B.solve + 1] - sb0;
-      if (S.bc < 0 && (S.nb1 < 0 || S.nb1 >= sbn)) return OCFD_ERR_ARG;
-      if (S.bc < 0) S.nb1 += sb0;
+      // nb1 = -1 (partner on another rank) only in a sharded handle
+      if (S.bc < 0 && !(h->part && S.nb1 == -1) && (S.nb1 < 0 || S.nb1 >= sbn)) return OCFD_ERR_ARG;
+      if (S.bc < 0 && S.nb1 >= 0) S.nb1 += sb0;
       if (S.bc > 0 && !(S.bc == 2 || S.bc == 3 || S.bc == 4 || S.bc == 5 || S.bc == 6 || S.bc == 401)) return OCFD_ERR_UNSUPPORTED;
       h->sub.push_back(S);
     }
@@ -460,13 +500,14 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   h->ncell = h->tot_cell;
   h->ncell_s.assign(nsolve, 0);
   for (int b = 0; b < nblk; b++) h->ncell_s[h->blk[b].solve] += h->pre_cell[b + 1] - h->pre_cell[b];
+  if (h->part) h->ncell_s[0] = h->part->ncell_global;
   int ns = (int)h->sub.size();
   h->pre_subcell.assign(ns + 1, 0); h->pre_halo.assign(ns + 1, 0);
   for (int s = 0; s < ns; s++) {
     const SubD& S = h->sub[s];
     h->pre_subcell[s + 1] = h->pre_subcell[s] + subcell_count(S);
     long long nh = 0;
-    if (S.bc < 0) {
+    if (S.bc < 0 && S.nb1 >= 0) {
       int kb1[3] = {S.ib1, S.jb1, S.kb1}, ke1[3] = {S.ie1 - 1, S.je1 - 1, S.ke1 - 1};
       int d1 = (S.face1 - 1) % 3;
       if (S.face1 <= 3) kb1[d1] -= LAPH;
@@ -602,7 +643,8 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
           for (int i = 1; i <= B.nx; i++)
             X[b][c * nn + i + (size_t)B.NXn * (j + (size_t)B.NYn * k)] = xyz[b][c * np + (i - 1) + (size_t)B.nx * ((j - 1) + (size_t)B.ny * (k - 1))];
   }
-  coordinate_ghosts(h->blk, h->sub, X);
+  if (h->part) X = h->part->X;  // ghost layer from the whole case, across rank boundaries too
+  else coordinate_ghosts(h->blk, h->sub, X);
   std::vector<double> hx(onode), hy(onode), hz(onode);
   for (int b = 0; b < nblk; b++) {
     const BlkD& B = h->blk[b];
@@ -615,7 +657,10 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   std::vector<long long> wpre(nsolve + 1, 0);  // wall nodes of solve q: [wpre[q], wpre[q+1])
   int turb = h->sps[0].turb;
   bool need_dw = turb != 0 && !(dw && dw[0]);
-  if (need_dw) {
+  if (need_dw && h->part) {  // the wall nodes of every rank's blocks
+    Xw = h->part->Xw;
+    wpre[1] = (long long)(Xw.size() / 3);
+  } else if (need_dw) {
     for (int sq_ = 0; sq_ < nsolve; sq_++) {
      for (const SubD& S : h->sub) {
       if (S.bc != 2 || h->blk[S.blk].solve != sq_) continue;
@@ -799,6 +844,27 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   h->info.bc_rounds = h->bc_rounds.data(); h->info.nround = (int)(h->bc_rounds.size() / 3);
   h->info.halo_levels = h->halo_levels.data(); h->info.nhlevel = (int)(h->halo_levels.size() / 3);
   h->info.halo_ent = h->d_halo_ent; h->info.halo_pre = h->d_halo_pre; h->info.halo_stage = h->d_halo_stage;
+  if (h->part) {
+    PartCtx& Pc = *h->part;
+    const long long ns_cells = Pc.send_pre.back(), nr_cells = Pc.recv_pre.back();
+    Pc.d_send_ent = M.alloc<int>(std::max<size_t>(1, Pc.send_ent.size()), e);
+    Pc.d_send_pre = M.alloc<long long>(Pc.send_pre.size(), e);
+    Pc.d_recv_sub = M.alloc<SubD>(std::max<size_t>(1, Pc.recv_sub.size()), e);
+    Pc.d_recv_pre = M.alloc<long long>(Pc.recv_pre.size(), e);
+    Pc.d_send = M.alloc<double>((size_t)NV * std::max(1LL, ns_cells), e);
+    Pc.d_recv = M.alloc<double>((size_t)NV * std::max(1LL, nr_cells), e);
+    if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "exchange buffers"); }
+    if (!Pc.send_ent.empty()) up(Pc.d_send_ent, Pc.send_ent);
+    up(Pc.d_send_pre, Pc.send_pre);
+    if (!Pc.recv_sub.empty()) up(Pc.d_recv_sub, Pc.recv_sub);
+    up(Pc.d_recv_pre, Pc.recv_pre);
+    for (long long& o : Pc.send_off) o *= NV;
+    for (long long& o : Pc.recv_off) o *= NV;
+    h->info.exchange = part_exchange; h->info.exchange_ctx = h;
+    h->info.xs_ent = Pc.d_send_ent; h->info.xs_pre = Pc.d_send_pre; h->info.nxs = (int)Pc.send_ent.size(); h->info.xs_cells = ns_cells;
+    h->info.xr_sub = Pc.d_recv_sub; h->info.xr_pre = Pc.d_recv_pre; h->info.nxr = (int)Pc.recv_sub.size(); h->info.xr_cells = nr_cells;
+    h->info.xsend = Pc.d_send; h->info.xrecv = Pc.d_recv;
+  }
   h->info.recon_prim = 1;
   for (int q = 0; q < nsolve; q++) if (ps[q].iflag_reconstruction != 0) h->info.recon_prim = 0;
   {
@@ -810,7 +876,11 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   else fill_arena<double>(h, h->A64, h->d_Md, h->d_vold, h->d_dtmd, h->d_dwd);
   select_lu(h, lu_force ? (lu_force == 64 ? 1 : 0) : 0);
   if (!h->run) { M.release(); return OCFD_ERR_UNSUPPORTED; }
-  if (!lu_force && !h->info.lu_planes && !std::getenv("OCFD_NO_AUTOTUNE")) autotune_lu(h);
+  if (!lu_force && !h->info.lu_planes && !std::getenv("OCFD_NO_AUTOTUNE")) {
+    if (h->part) h->part->xchg = false;  // the timed steps are discarded: no exchange with other ranks
+    autotune_lu(h);
+    if (h->part) h->part->xchg = true;
+  }
   h->run->init_flow(h->st);
   if (p->time_method == -1) h->run->dual_init(h->st);
   if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "init"); }
@@ -821,6 +891,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     for (int b = 0; b < nblk; b++) bcerr |= fl[3 * nblk + b];
   }
   if (bcerr) { M.release(); return OCFD_ERR_UNSUPPORTED; }
+  if (h->part && h->part->comm_err) { M.release(); return OCFD_ERR_COMM; }
   *out = hp.release();
   return OCFD_OK;
 }
@@ -834,6 +905,210 @@ extern "C" int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, cons
 extern "C" int ocfd_create_batch(const ocfd_params* ps, int nsolve, const int* nblk, const int* nijk, const double* const* xyz,
                                  const int* nsub, const int* inc, const double* const* dw, ocfd_handle** out) {
   return create_impl(ps, nsolve, nblk, nijk, xyz, nsub, inc, dw, out);
+}
+
+// ---- block-sharded handles ------------------------------------------------------------------
+// The whole case is described on every rank (as every MPI rank of the reference knows the whole
+// block list and .inc table); the node ghost layer and the wall nodes are taken from the whole
+// case here, then the rank's blocks go through create_impl with interfaces to other ranks marked
+// (partner -1) and the exchange lists attached.
+// whole-case block and subface tables of a sharded case (0-based partner blocks)
+static int parse_whole(int nblk, const int* nijk, const int* nsub, const int* inc, const int* owner, std::vector<BlkD>& fb,
+                       std::vector<SubD>& fs, std::vector<int>& fsub0) {
+  fb.assign(nblk, BlkD{});
+  fs.clear();
+  fsub0.assign(nblk + 1, 0);
+  const int* q = inc;
+  for (int b = 0; b < nblk; b++) {
+    BlkD& B = fb[b];
+    B.nx = nijk[3 * b]; B.ny = nijk[3 * b + 1]; B.nz = nijk[3 * b + 2];
+    if (B.nx < 2 || B.ny < 2 || B.nz < 2 || owner[b] < 0 || nsub[b] < 0) return OCFD_ERR_ARG;
+    B.NX = B.nx + 7; B.NY = B.ny + 7; B.NZ = B.nz + 7;
+    B.NXn = B.nx + 2; B.NYn = B.ny + 2; B.NZn = B.nz + 2;
+    fsub0[b] = (int)fs.size();
+    for (int r = 0; r < nsub[b]; r++, q += 21) {
+      SubD S{};
+      S.blk = b;
+      S.ib = q[0]; S.ie = q[1]; S.jb = q[2]; S.je = q[3]; S.kb = q[4]; S.ke = q[5]; S.bc = q[6]; S.face = q[7]; S.f_no = q[8];
+      S.ib1 = q[9]; S.ie1 = q[10]; S.jb1 = q[11]; S.je1 = q[12]; S.kb1 = q[13]; S.ke1 = q[14]; S.nb1 = q[15] - 1; S.face1 = q[16];
+      S.f_no1 = q[17]; S.L1 = q[18]; S.L2 = q[19]; S.L3 = q[20];
+      if (S.face < 1 || S.face > 6 || (S.bc < 0 && (S.nb1 < 0 || S.nb1 >= nblk || S.face1 < 1 || S.face1 > 6))) return OCFD_ERR_ARG;
+      fs.push_back(S);
+    }
+  }
+  fsub0[nblk] = (int)fs.size();
+  // interfaces between ranks: both blocks at least LAP cells thick across them, so that no copy
+  // between ranks reads a ghost cell another copy writes
+  auto thick = [&](int b, int face) {
+    const BlkD& B = fb[b];
+    int n = (face - 1) % 3 == 0 ? B.nx : ((face - 1) % 3 == 1 ? B.ny : B.nz);
+    return n - 1 >= LAPH;
+  };
+  for (const SubD& S : fs)
+    if (S.bc < 0 && owner[S.blk] != owner[S.nb1] && (!thick(S.blk, S.face) || !thick(S.nb1, S.face1))) return OCFD_ERR_UNSUPPORTED;
+  return OCFD_OK;
+}
+
+// the exchange lists of one rank, per peer in ascending rank order; within a peer both sides list
+// the copies in the whole case's subface order (block by block, subface by subface), so the
+// sender's and the receiver's entries line up; sizes in cells (the target's LAP ghost layers)
+static void make_plan(const std::vector<SubD>& fs, const std::vector<int>& fsub0, const int* owner, int nblk, int rank,
+                      const std::vector<int>& glob2loc, const std::vector<int>& lsub0, PartCtx& Pc) {
+  auto target_cells = [](const SubD& S) {
+    int kb1[3] = {S.ib1, S.jb1, S.kb1}, ke1[3] = {S.ie1 - 1, S.je1 - 1, S.ke1 - 1};
+    int d1 = (S.face1 - 1) % 3;
+    if (S.face1 <= 3) kb1[d1] -= LAPH;
+    ke1[d1] = kb1[d1] + LAPH - 1;
+    return (long long)(ke1[0] - kb1[0] + 1) * (ke1[1] - kb1[1] + 1) * (ke1[2] - kb1[2] + 1);
+  };
+  int nrank = 0;
+  for (int b = 0; b < nblk; b++) nrank = std::max(nrank, owner[b] + 1);
+  Pc.send_pre.assign(1, 0); Pc.recv_pre.assign(1, 0); Pc.send_off.assign(1, 0); Pc.recv_off.assign(1, 0);
+  Pc.send_ent.clear(); Pc.recv_sub.clear(); Pc.peers.clear();
+  for (int peer = 0; peer < nrank; peer++) {
+    if (peer == rank) continue;
+    bool any = false;
+    for (int t = 0; t < (int)fs.size(); t++) {
+      const SubD& S = fs[t];
+      if (S.bc < 0 && owner[S.blk] == rank && owner[S.nb1] == peer) {  // outgoing: local source, target on the peer
+        Pc.send_ent.push_back(lsub0[glob2loc[S.blk]] + (t - fsub0[S.blk]));
+        Pc.send_pre.push_back(Pc.send_pre.back() + target_cells(S));
+        any = true;
+      }
+    }
+    for (int t = 0; t < (int)fs.size(); t++) {
+      const SubD& S = fs[t];
+      if (S.bc < 0 && owner[S.blk] == peer && owner[S.nb1] == rank) {  // incoming: source on the peer, local target
+        SubD R = S;
+        R.blk = -1;
+        R.nb1 = glob2loc[S.nb1];
+        Pc.recv_sub.push_back(R);
+        Pc.recv_pre.push_back(Pc.recv_pre.back() + target_cells(S));
+        any = true;
+      }
+    }
+    if (!any) continue;
+    Pc.peers.push_back(peer);
+    Pc.send_off.push_back(Pc.send_pre.back());
+    Pc.recv_off.push_back(Pc.recv_pre.back());
+  }
+}
+
+static void local_numbering(int nblk, const int* owner, int rank, const int* nsub, std::vector<int>& loc2glob, std::vector<int>& glob2loc,
+                            std::vector<int>& lsub0) {
+  loc2glob.clear();
+  glob2loc.assign(nblk, -1);
+  for (int b = 0; b < nblk; b++)
+    if (owner[b] == rank) { glob2loc[b] = (int)loc2glob.size(); loc2glob.push_back(b); }
+  lsub0.assign(loc2glob.size() + 1, 0);
+  for (size_t l = 0; l < loc2glob.size(); l++) lsub0[l + 1] = lsub0[l] + nsub[loc2glob[l]];
+}
+
+extern "C" int ocfd_part_plan(int nblk, const int* nijk, const int* nsub, const int* inc, const int* owner, int rank, int* peers,
+                              long long* send_off, long long* recv_off) {
+  if (nblk <= 0 || !nijk || !nsub || !inc || !owner || rank < 0) return OCFD_ERR_ARG;
+  std::vector<BlkD> fb;
+  std::vector<SubD> fs;
+  std::vector<int> fsub0, glob2loc, lsub0;
+  if (int rc = parse_whole(nblk, nijk, nsub, inc, owner, fb, fs, fsub0)) return rc;
+  PartCtx Pc;
+  local_numbering(nblk, owner, rank, nsub, Pc.loc2glob, glob2loc, lsub0);
+  make_plan(fs, fsub0, owner, nblk, rank, glob2loc, lsub0, Pc);
+  const int np = (int)Pc.peers.size();
+  for (int q = 0; q < np; q++)
+    if (peers) peers[q] = Pc.peers[q];
+  for (int q = 0; q <= np; q++) {
+    if (send_off) send_off[q] = Pc.send_off[q];
+    if (recv_off) recv_off[q] = Pc.recv_off[q];
+  }
+  return np;
+}
+
+// ---- block-sharded handles ------------------------------------------------------------------
+// The whole case is described on every rank (as every MPI rank of the reference knows the whole
+// block list and .inc table); the node ghost layer and the wall nodes are taken from the whole
+// case here, then the rank's blocks go through create_impl with interfaces to other ranks marked
+// (partner -1) and the exchange lists attached.
+extern "C" int ocfd_create_part(const ocfd_params* p, int nblk, const int* nijk, const double* const* xyz, const int* nsub,
+                                const int* inc, const double* const* dw, const int* owner, int rank, const ocfd_comm* comm,
+                                ocfd_handle** out) {
+  if (!p || nblk <= 0 || !nijk || !xyz || !nsub || !inc || !owner || !comm || !comm->exchange || !comm->allreduce || !out || rank < 0)
+    return OCFD_ERR_ARG;
+  std::unique_ptr<PartCtx> Pc(new PartCtx());
+  Pc->rank = rank;
+  Pc->comm = *comm;
+  std::vector<BlkD> fb;
+  std::vector<SubD> fs;
+  std::vector<int> fsub0, glob2loc, lsub0;
+  if (int rc = parse_whole(nblk, nijk, nsub, inc, owner, fb, fs, fsub0)) return rc;
+  local_numbering(nblk, owner, rank, nsub, Pc->loc2glob, glob2loc, lsub0);
+  if (Pc->loc2glob.empty()) return OCFD_ERR_ARG;
+  for (const BlkD& B : fb) Pc->ncell_global += (long long)(B.nx - 1) * (B.ny - 1) * (B.nz - 1);
+  // node coordinates with the ghost layer, from the whole case: this rank's blocks and the blocks
+  // whose nodes their ghost layer copies
+  std::vector<std::vector<double>> X(nblk);
+  for (int b = 0; b < nblk; b++) {
+    const BlkD& B = fb[b];
+    if (owner[b] != rank) {
+      bool touches = false;
+      for (int t = fsub0[b]; t < fsub0[b + 1]; t++) touches |= fs[t].bc < 0 && owner[fs[t].nb1] == rank;
+      if (!touches) continue;
+    }
+    size_t nn = (size_t)B.NXn * B.NYn * B.NZn, np = (size_t)B.nx * B.ny * B.nz;
+    X[b].assign(3 * nn, 0.0);
+    for (int c = 0; c < 3; c++)
+      for (int k = 1; k <= B.nz; k++)
+        for (int j = 1; j <= B.ny; j++)
+          for (int i = 1; i <= B.nx; i++)
+            X[b][c * nn + i + (size_t)B.NXn * (j + (size_t)B.NYn * k)] = xyz[b][c * np + (i - 1) + (size_t)B.nx * ((j - 1) + (size_t)B.ny * (k - 1))];
+  }
+  {
+    std::vector<SubD> used;  // copies into this rank's blocks and the physical faces of its blocks, in order
+    for (const SubD& S : fs)
+      if ((S.bc < 0 && owner[S.nb1] == rank) || (S.bc >= 0 && owner[S.blk] == rank)) used.push_back(S);
+    coordinate_ghosts(fb, used, X);
+  }
+  for (int b : Pc->loc2glob) Pc->X.push_back(std::move(X[b]));
+  // wall nodes of the whole case (comput_dw searches the walls of every block)
+  for (const SubD& S : fs) {
+    if (S.bc != OCFD_BC_WALL) continue;
+    const BlkD& B = fb[S.blk];
+    size_t np = (size_t)B.nx * B.ny * B.nz;
+    for (int k = S.kb; k <= S.ke; k++)
+      for (int j = S.jb; j <= S.je; j++)
+        for (int i = S.ib; i <= S.ie; i++) {
+          size_t o = (size_t)(i - 1) + (size_t)B.nx * ((size_t)(j - 1) + (size_t)B.ny * (k - 1));
+          for (int c = 0; c < 3; c++) Pc->Xw.push_back(xyz[S.blk][c * np + o]);
+        }
+  }
+  make_plan(fs, fsub0, owner, nblk, rank, glob2loc, lsub0, *Pc);
+  // the local case: this rank's blocks, interfaces to other ranks with partner 0 (-1 after the
+  // 1-based conversion)
+  const int nl = (int)Pc->loc2glob.size();
+  std::vector<int> lnijk, lnsub, linc;
+  std::vector<const double*> lxyz, ldw;
+  for (int l = 0; l < nl; l++) {
+    const int b = Pc->loc2glob[l];
+    lnijk.insert(lnijk.end(), nijk + 3 * b, nijk + 3 * b + 3);
+    lxyz.push_back(xyz[b]);
+    if (dw && dw[0]) ldw.push_back(dw[b]);
+    lnsub.push_back(nsub[b]);
+    for (int t = fsub0[b]; t < fsub0[b + 1]; t++) {
+      const int* r = inc + 21 * (size_t)t;
+      const size_t o = linc.size();
+      linc.insert(linc.end(), r, r + 21);
+      if (fs[t].bc < 0) linc[o + 15] = owner[fs[t].nb1] == rank ? glob2loc[fs[t].nb1] + 1 : 0;
+    }
+  }
+  return create_impl(p, 1, &nl, lnijk.data(), lxyz.data(), lnsub.data(), linc.data(), ldw.empty() ? nullptr : ldw.data(), out,
+                     std::move(Pc));
+}
+
+extern "C" int ocfd_part_blocks(const ocfd_handle* h, int* global_ids) {
+  if (!h) return 0;
+  for (int b = 0; b < h->nblk; b++)
+    if (global_ids) global_ids[b] = h->part ? h->part->loc2glob[b] : b;
+  return h->nblk;
 }
 
 extern "C" int ocfd_nsolve(const ocfd_handle* h) { return h ? h->nsolve : 0; }
@@ -918,6 +1193,7 @@ extern "C" int ocfd_init_flow(ocfd_handle* h) {
   if (h->P.time_method == -1) h->run->dual_init(h->st);
   cudaError_t e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "init_flow");
+  if (h->part && h->part->comm_err) return fail(h, OCFD_ERR_COMM, "halo exchange callback failed");
   h->kstep = 0;
   h->tt = 0.0;
   return OCFD_OK;
@@ -925,7 +1201,7 @@ extern "C" int ocfd_init_flow(ocfd_handle* h) {
 
 static int ensure_graph(ocfd_handle* h) {
   if (h->gexec) return OCFD_OK;
-  if (std::getenv("OCFD_NO_GRAPH")) return OCFD_OK;
+  if (std::getenv("OCFD_NO_GRAPH") || h->part) return OCFD_OK;  // a sharded step calls back to the host
   cudaError_t e = cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return cuda_fail(h, e, "capture begin");
   h->run->step(h->st);
@@ -999,6 +1275,7 @@ extern "C" int ocfd_advance(ocfd_handle* h, int nsteps, int* kstep, double* tt) 
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(h, e, "advance");
+  if (h->part && h->part->comm_err) return fail(h, OCFD_ERR_COMM, "halo exchange callback failed");
   if (kstep) *kstep = h->kstep;
   if (tt) *tt = h->tt;
   return OCFD_OK;
@@ -1024,17 +1301,31 @@ static int residual_impl(ocfd_handle* h, double* rmax, double* rrms, int nout) {
   cudaMemcpyAsync(&nan_at, h->d_nan, 8, cudaMemcpyDeviceToHost, h->st);
   cudaError_t e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "residual");
+  int lu_err = 0;
+  cudaMemcpy(&lu_err, h->d_lu_err, 4, cudaMemcpyDeviceToHost);
+  bool other_nan = false, other_lu = false;
+  if (h->part) {  // MPI_ALLREDUCE of the maxima and the sums of squares (sub_time_advance.f90:373-374)
+    double mx[9], sm[7];
+    for (int m = 0; m < 7; m++) { mx[m] = out[m]; sm[m] = out[7 + m]; }
+    mx[7] = nan_at != ~0ULL ? 1.0 : 0.0;
+    mx[8] = lu_err ? 1.0 : 0.0;
+    const ocfd_comm& C = h->part->comm;
+    if (C.allreduce(C.user, mx, 9, 1) || C.allreduce(C.user, sm, 7, 0)) return fail(h, OCFD_ERR_COMM, "norm all-reduce callback failed");
+    for (int m = 0; m < 7; m++) { out[m] = mx[m]; out[7 + m] = sm[m]; }
+    other_nan = mx[7] != 0.0 && nan_at == ~0ULL;
+    other_lu = mx[8] != 0.0 && !lu_err;
+  }
   for (int q = 0; q < nout; q++)
     for (int m = 0; m < 7; m++) {
       rmax[7 * q + m] = m < h->nvar ? out[14 * q + m] : 0.0;
       rrms[7 * q + m] = m < h->nvar ? std::sqrt(out[14 * q + 7 + m] / (double)h->ncell_s[q]) : 0.0;
     }
-  int lu_err = 0;
-  cudaMemcpy(&lu_err, h->d_lu_err, 4, cudaMemcpyDeviceToHost);
   if (lu_err) {
     cudaMemset(h->d_lu_err, 0, 4);
     return fail(h, OCFD_ERR_TIMEOUT, "LU-SGS wavefront: a bounded wait between tiles timed out");
   }
+  if (other_lu) return fail(h, OCFD_ERR_TIMEOUT, "LU-SGS wavefront: a bounded wait timed out on another rank");
+  if (other_nan) return fail(h, OCFD_ERR_NAN, "NaN in residual on another rank");
   if (nan_at != ~0ULL) {
     long long g = (long long)(nan_at / 8);
     int m = (int)(nan_at % 8);
@@ -1043,7 +1334,9 @@ static int residual_impl(ocfd_handle* h, double* rmax, double* rrms, int nout) {
     long long l = g - h->pre_cell[b];
     int i = (int)(l % (B.nx - 1)) + 1, j = (int)((l / (B.nx - 1)) % (B.ny - 1)) + 1, k = (int)(l / ((long long)(B.nx - 1) * (B.ny - 1))) + 1;
     char buf[200];
-    if (h->nsolve > 1)
+    if (h->part)
+      std::snprintf(buf, sizeof buf, "NaN in residual: block %d i,j,k,m = %d %d %d %d", h->part->loc2glob[b] + 1, i, j, k, m + 1);
+    else if (h->nsolve > 1)
       std::snprintf(buf, sizeof buf, "NaN in residual: solve %d block %d i,j,k,m = %d %d %d %d", B.solve, b - h->sblk0[B.solve] + 1, i, j, k, m + 1);
     else
       std::snprintf(buf, sizeof buf, "NaN in residual: block %d i,j,k,m = %d %d %d %d", b + 1, i, j, k, m + 1);
@@ -1108,6 +1401,7 @@ static int static_norm_area(ocfd_handle* h, StaticNormArea& a) {
 
 extern "C" int ocfd_residual_static(ocfd_handle* h, double* rmax, double* rrms) {
   if (!h || !rmax || !rrms) return OCFD_ERR_ARG;
+  if (h->part) return fail(h, OCFD_ERR_UNSUPPORTED, "residual_static: not for sharded handles (the norms are all-reduced); use ocfd_residual");
   if ((long long)h->cchunk.size() > kStaticNormChunks)
     return fail(h, OCFD_ERR_ARG, "residual_static: the handle has more than 33,554,432 interior cells (4096 chunks); use ocfd_residual");
   if (h->nsolve > kStaticNormSolves) return fail(h, OCFD_ERR_ARG, "residual_static: the handle has more than 256 solves; use ocfd_residual");
@@ -1156,6 +1450,8 @@ static int forces_impl(ocfd_handle* h, double* ft, double* cl, double* cd, doubl
     double Ft[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int b = h->sblk0[sv]; b < h->sblk0[sv + 1]; b++)
       for (int q = 0; q < 9; q++) Ft[q] = Ft[q] + blk[9 * b + q];
+    if (h->part && h->part->comm.allreduce(h->part->comm.user, Ft, 9, 0))  // MPI_ALLREDUCE, sub_Post.f90:202
+      return fail(h, OCFD_ERR_COMM, "force all-reduce callback failed");
     const ocfd_params& P = h->Ps[sv];
     double* f = ft + 9 * sv;
     for (int q = 0; q < 6; q++) f[q] = 2.0 * Ft[q] / P.ref_s;

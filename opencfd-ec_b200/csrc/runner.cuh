@@ -128,6 +128,11 @@ class RunnerT : public Runner {
       k_halo_level<T, NV, 0><<<grid_of(H[2]), 256, 0, st>>>(A, I_.halo_ent, I_.halo_pre, H[0], H[1], (long long)H[2], I_.halo_stage);
       k_halo_level<T, NV, 1><<<grid_of(H[2]), 256, 0, st>>>(A, I_.halo_ent, I_.halo_pre, H[0], H[1], (long long)H[2], I_.halo_stage);
     }
+    if (I_.exchange) {
+      if (I_.xs_cells > 0) k_halo_pack<T, NV><<<grid_of(I_.xs_cells), 256, 0, st>>>(A, I_.xs_ent, I_.xs_pre, I_.nxs, I_.xs_cells, I_.xsend);
+      const int fresh = I_.exchange(I_.exchange_ctx, st);
+      if (fresh && I_.xr_cells > 0) k_halo_unpack<T, NV><<<grid_of(I_.xr_cells), 256, 0, st>>>(A, I_.xr_sub, I_.xr_pre, I_.nxr, I_.xr_cells, I_.xrecv);
+    }
     k_corner<T, NV><<<A.nblk, 256, 0, st>>>(A);
   }
 
@@ -207,7 +212,7 @@ class RunnerT : public Runner {
     int upd = 1 + 1 + (NV == 6 ? 3 : 0);
     int nbc = 0;
     for (int r = 0; r < I_.nround; r++) nbc += I_.bc_rounds[3 * r + 2] > 0;
-    int bch = nbc + 1 + (A_.tot_halo > 0 ? (I_.nhlevel ? 2 * I_.nhlevel : 1) : 0);
+    int bch = nbc + 1 + (A_.tot_halo > 0 ? (I_.nhlevel ? 2 * I_.nhlevel : 1) : 0) + (I_.xs_cells > 0) + (I_.xr_cells > 0);
     int n;
     if (I_.time_method == -1) return res + 1 + lu + upd + bch;  // one dual-time inner iteration
     if (I_.time_method == 0) n = res + lu + upd + bch;

@@ -29,6 +29,21 @@ struct RunInfo {
   const int* halo_ent;
   const long long* halo_pre;
   double* halo_stage;     // NV x (largest level) doubles
+  // block-sharded handles: copies to other ranks are packed into xsend (entries xs_ent, cell
+  // prefix xs_pre), exchange(ctx, stream) hands the buffers over (returns 1 when xrecv holds
+  // fresh data to unpack), copies from other ranks are unpacked from xrecv (entries xr_sub)
+  int (*exchange)(void* ctx, cudaStream_t st);
+  void* exchange_ctx;
+  const int* xs_ent;
+  const long long* xs_pre;
+  int nxs;
+  long long xs_cells;
+  const SubD* xr_sub;
+  const long long* xr_pre;
+  int nxr;
+  long long xr_cells;
+  double* xsend;
+  double* xrecv;
 };
 
 class Runner {

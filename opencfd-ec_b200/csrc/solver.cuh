@@ -1328,9 +1328,10 @@ __global__ void k_bc_round(Arena<T> A, int e0, int e1, long long ncell) {
 // block-interface halo (Umessage_send_mpi, sub_update_buffer_mpi.f90:42-141): LAP ghost layers
 // of every inner subface are copied from the partner's interior with the (L1,L2,L3) permutation
 // ============================================================================================
-template <class T>
-__device__ __forceinline__ void halo_map(const Arena<T>& A, const SubD& S, long long l, long long& cs, long long& ct) {
-  // source: this block's LAP layers next to the face; target: the partner's LAP ghost layers
+// cell l of subface S's copy, counted in the target's order: the source cell (i,j,k) in the
+// subface's own block (its LAP layers next to the face) and the target cell in the partner block
+// (its LAP ghost layers)
+__device__ __forceinline__ void halo_idx(const SubD& S, long long l, int* src, int* dst) {
   int kb[3] = {S.ib, S.jb, S.kb}, ke[3] = {S.ie - 1, S.je - 1, S.ke - 1};
   int d = (S.face - 1) % 3;
   if (S.face > 3) kb[d] = kb[d] - LAP;
@@ -1343,11 +1344,18 @@ __device__ __forceinline__ void halo_map(const Arena<T>& A, const SubD& S, long 
   int ka[3] = {(int)(l % n0), (int)((l / n0) % n1), (int)(l / ((long long)n0 * n1))};
   int L[3] = {abs(S.L1), abs(S.L2), abs(S.L3)};
   int P[3] = {S.L1 >= 0 ? 1 : -1, S.L2 >= 0 ? 1 : -1, S.L3 >= 0 ? 1 : -1};
-  int src[3];
 #pragma unroll
-  for (int q = 0; q < 3; q++) src[q] = (P[q] > 0 ? kb[q] : ke[q]) + ka[L[q] - 1] * P[q];
+  for (int q = 0; q < 3; q++) {
+    src[q] = (P[q] > 0 ? kb[q] : ke[q]) + ka[L[q] - 1] * P[q];
+    dst[q] = kb1[q] + ka[q];
+  }
+}
+template <class T>
+__device__ __forceinline__ void halo_map(const Arena<T>& A, const SubD& S, long long l, long long& cs, long long& ct) {
+  int src[3], dst[3];
+  halo_idx(S, l, src, dst);
   cs = bix(A.blk[S.blk], src[0], src[1], src[2]);
-  ct = bix(A.blk[S.nb1], kb1[0] + ka[0], kb1[1] + ka[1], kb1[2] + ka[2]);
+  ct = bix(A.blk[S.nb1], dst[0], dst[1], dst[2]);
 }
 
 // every interface copy in one launch: valid when no copy reads or writes cells another copy
@@ -1380,6 +1388,39 @@ __global__ void k_halo_level(Arena<T> A, const int* ent, const long long* pre, i
       if (PHASE == 0) stage[m * cells + g] = A.U[m * tb + cs];
       else A.U[m * tb + ct] = stage[m * cells + g];
     }
+  }
+}
+
+// copies between ranks of a block-sharded handle (Umessage_send_mpi / Umessage_recv_mpi,
+// sub_update_buffer_mpi.f90:42-211): the pack gathers the source cells of the subfaces ent[0..n)
+// (this rank's blocks, partner on another rank) into buf, cell-major with NV values per cell;
+// the unpack scatters buf into the ghost cells of the subfaces sub[0..n) of other ranks' blocks
+// whose partner (nb1, renumbered to this handle's block) is here.  Both sides count a copy's
+// cells in the target's order, so the two buffers line up entry by entry.
+template <class T, int NV>
+__global__ void k_halo_pack(Arena<T> A, const int* ent, const long long* pre, int n, long long cells, double* buf) {
+  const long long tb = A.tot_box;
+  OCFD_GRID_STRIDE(g, cells) {
+    const int e = find_blk(pre, n, g);
+    const SubD S = A.sub[ent[e]];
+    int src[3], dst[3];
+    halo_idx(S, g - pre[e], src, dst);
+    const long long cs = bix(A.blk[S.blk], src[0], src[1], src[2]);
+#pragma unroll
+    for (int m = 0; m < NV; m++) buf[g * NV + m] = A.U[m * tb + cs];
+  }
+}
+template <class T, int NV>
+__global__ void k_halo_unpack(Arena<T> A, const SubD* sub, const long long* pre, int n, long long cells, const double* buf) {
+  const long long tb = A.tot_box;
+  OCFD_GRID_STRIDE(g, cells) {
+    const int e = find_blk(pre, n, g);
+    const SubD S = sub[e];
+    int src[3], dst[3];
+    halo_idx(S, g - pre[e], src, dst);
+    const long long ct = bix(A.blk[S.nb1], dst[0], dst[1], dst[2]);
+#pragma unroll
+    for (int m = 0; m < NV; m++) A.U[m * tb + ct] = buf[g * NV + m];
   }
 }
 

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(ROOT_DIR, "libocfd_b200.so")
 _lib = None
 
 OCFD_OK, OCFD_ERR_ARG, OCFD_ERR_CUDA, OCFD_ERR_OOM, OCFD_ERR_NAN, OCFD_ERR_TIMEOUT, OCFD_ERR_UNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
+OCFD_ERR_COMM = -8
 
 EXPORTED = [
     "ocfd_default_params", "ocfd_finalize_params", "ocfd_create", "ocfd_destroy", "ocfd_last_error", "ocfd_state_size",
@@ -21,7 +22,7 @@ EXPORTED = [
     "ocfd_limiter_status", "ocfd_array_shape", "ocfd_get_array", "ocfd_version", "ocfd_compute_residual",
     "ocfd_stream", "ocfd_profile", "ocfd_launches_per_step", "ocfd_create_batch", "ocfd_nsolve",
     "ocfd_residual_all", "ocfd_forces_all", "ocfd_footprint", "ocfd_synchronize", "ocfd_residual_static",
-    "ocfd_lu_tile_width",
+    "ocfd_lu_tile_width", "ocfd_create_part", "ocfd_part_blocks", "ocfd_part_plan",
 ]
 
 

@@ -20,6 +20,8 @@
 // wait is bounded; a timeout sets an error flag and the CTA finishes its tile without waiting
 // (the host reports OCFD_ERR_TIMEOUT).
 #pragma once
+#include <type_traits>
+
 #include "solver.cuh"
 
 namespace ocfd {
@@ -289,11 +291,43 @@ template <int NT>
 __device__ __forceinline__ void cta_bar() { asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory"); }
 __device__ __forceinline__ double ldro(const float* p) { return (double)__ldg(p); }
 
+// cp.async (sm_80+) of one 4- or 8-byte value into shared memory, and the group controls: each
+// thread waits only for its own copies and reads only the slots it filled itself
+__device__ __forceinline__ void cpa(void* dst, const void* src, int bytes) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(dst);
+  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(a), "l"(src) : "memory");
+}
+template <class X>
+__device__ __forceinline__ void cpa(X* dst, const X* src) { cpa((void*)dst, (const void*)src, (int)sizeof(X)); }
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Per-column input data of the sweep, staged through a ring of LU_RING steps in dynamic shared
+// memory: step t's loads are issued two steps before the step uses them, so their HBM latency
+// overlaps two steps of the dependency chain instead of half a step.
+constexpr int LU_RING = 3;
+template <class T, int NV, bool UPPER, int TC>
+struct LuRing {
+  using RT = typename std::conditional<UPPER, double, T>::type;  // R: Res (lower) or DU* (upper)
+  double oU[LU_RING][NV][TC];      // owner: the cell's state
+  double ovol[LU_RING][TC];
+  double dU[LU_RING][3][NV][TC];   // direction threads: the cross-tile neighbour's state
+  RT oR[LU_RING][NV][TC];
+  T odt[LU_RING][TC];
+  T oLc[LU_RING][3][TC], oLv[LU_RING][3][TC];
+  T dn[LU_RING][3][4][TC];         // n1, n2, n3 of the face and S (the lower or the upper face)
+  T dL[LU_RING][3][2][TC];         // Lc, Lv of the cross-tile neighbour
+};
+
 #ifndef OCFD_LU_MINB
 #define OCFD_LU_MINB (64 / TC)
 #endif
 template <class T, int NV, bool UPPER, int TC>
 __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena<T> A, LuArgs L) {
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  LuRing<T, NV, UPPER, TC>& R = *reinterpret_cast<LuRing<T, NV, UPPER, TC>*>(s_dyn);
   __shared__ int s_tile;
   __shared__ double s_acc[3][NV][TC];      // direction terms of the current step
   __shared__ double s_pub[NV][TC];         // DU of each column's last cell
@@ -348,68 +382,111 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
     // a neighbour column in another tile: its DU comes through L2 after the progress wait
     const bool xt = !owner && ((d == 1 && lj == 0) || (d == 2 && lk == 0));
     const int pubcol = d == 0 ? c : (d == 1 ? c - 1 : c - TJ);
+    // the column's index bases (cell, box and face spaces; add i) and this thread's upstream
+    // neighbour offset in direction d, so a step's indices are additions
+    const long long cb = B.ocell - 1 + (long long)nxm * ((j - 1) + (long long)nym * (k - 1));
+    const long long bb = B.obox + 3 + (long long)B.NX * ((j + 3) + (long long)B.NY * (k + 3));
+    const long long fb = B.oface - 1 + (long long)B.nx * ((j - 1) + (long long)B.ny * (k - 1));
+    const long long dcn = d == 0 ? off : (d == 1 ? (long long)off * nxm : (long long)off * nxm * nym);
+    const long long dbn = d == 0 ? off : (d == 1 ? (long long)off * B.NX : (long long)off * B.NX * B.NY);
+    const long long dfs = !UPPER ? 0 : (d == 0 ? 1 : (d == 1 ? (long long)B.nx : (long long)B.nx * B.ny));
 
-    LuDir<NV> dn;  // prefetched direction data (raw) for the next step
-    LuOwn<NV> on;  // prefetched owner data (raw) for the next step
-    auto load_dir = [&](int t, LuDir<NV>& x) {
-      const int i = i_of(t);
-      const long long f = fix_(B, i, j, k);
-      x.n1 = ldro(A.M + (M_NI1 + 3 * d) * tf + f);
-      x.n2 = ldro(A.M + (M_NI2 + 3 * d) * tf + f);
-      x.n3 = ldro(A.M + (M_NI3 + 3 * d) * tf + f);
-      // the lower face's area (lower sweep) or the upper face's (upper sweep, sub_LU_SGS.f90:96-97)
-      const long long fs = UPPER ? fix_(B, i + (d == 0), j + (d == 1), k + (d == 2)) : f;
-      x.S = ldro(A.M + (M_SI + d) * tf + fs);
-      if (!xt) return;  // in-tile neighbours publish their old state in shared memory
-      const int ii = i + (d == 0 ? off : 0), jj = j + (d == 1 ? off : 0), kk = k + (d == 2 ? off : 0);
-      const long long bn = bix(B, ii, jj, kk), cn = cix(B, ii, jj, kk);
+    // step t's face data of direction d (and, across a tile edge, the neighbour's old state) into
+    // ring slot t % LU_RING; one commit group per step, empty when the step has nothing to load
+    auto issue_dir = [&](int t) {
+      if (on_at(t) && has_at(t)) {
+        const int sl = t % LU_RING, i = i_of(t);
+        const long long f = fb + i;
+        cpa(&R.dn[sl][d][0][c], A.M + (M_NI1 + 3 * d) * tf + f);
+        cpa(&R.dn[sl][d][1][c], A.M + (M_NI2 + 3 * d) * tf + f);
+        cpa(&R.dn[sl][d][2][c], A.M + (M_NI3 + 3 * d) * tf + f);
+        // the lower face's area (lower sweep) or the upper face's (upper sweep, sub_LU_SGS.f90:96-97)
+        cpa(&R.dn[sl][d][3][c], A.M + (M_SI + d) * tf + f + dfs);
+        if (xt) {  // in-tile neighbours publish their old state in shared memory
+          const long long bn = bb + i + dbn, cn = cb + i + dcn;
+#pragma unroll
+          for (int m = 0; m < NV; m++) cpa(&R.dU[sl][d][m][c], A.U + m * tb + bn);
+          cpa(&R.dL[sl][d][0][c], A.Lc + d * tc + cn);
+          cpa(&R.dL[sl][d][1][c], A.Lv + d * tc + cn);
+        }
+      }
+      cpa_commit();
+    };
+    auto take_dir = [&](int t, LuDir<NV>& x) {
+      const int sl = t % LU_RING;
+      x.n1 = (double)R.dn[sl][d][0][c]; x.n2 = (double)R.dn[sl][d][1][c]; x.n3 = (double)R.dn[sl][d][2][c];
+      x.S = (double)R.dn[sl][d][3][c];
+      if (!xt) return;
 #pragma unroll
       for (int m = 0; m < NV; m++) {
-        double u = __ldg(A.U + m * tb + bn);
+        const double u = R.dU[sl][d][m][c];
         x.Unb[m] = m >= 5 ? clamp0(u) : u;
       }
-      x.wLc = ldro(A.Lc + d * tc + cn);
-      x.Lv = ldro(A.Lv + d * tc + cn);
+      x.wLc = (double)R.dL[sl][d][0][c];
+      x.Lv = (double)R.dL[sl][d][1][c];
     };
-    auto load_own = [&](int t, LuOwn<NV>& x) {
-      const int i = i_of(t);
-      const long long bi = bix(B, i, j, k), ci = cix(B, i, j, k);
+    using RT = typename LuRing<T, NV, UPPER, TC>::RT;
+    auto issue_own = [&](int t) {
+      if (on_at(t)) {
+        const int sl = t % LU_RING, i = i_of(t);
+        const long long bi = bb + i, ci = cb + i;
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          cpa(&R.oU[sl][m][c], A.U + m * tb + bi);
+          // upper sweep: R is DU* of the lower sweep, read before this column overwrites it
+          if (UPPER) cpa(&R.oR[sl][m][c], (const RT*)(A.DU + m * tc + ci));
+          else cpa(&R.oR[sl][m][c], (const RT*)(A.Res + m * tc + ci));
+        }
+        cpa(&R.ovol[sl][c], A.vold + ci);
+        cpa(&R.odt[sl][c], A.dt + ci);
+#pragma unroll
+        for (int q2 = 0; q2 < 3; q2++) { cpa(&R.oLc[sl][q2][c], A.Lc + q2 * tc + ci); cpa(&R.oLv[sl][q2][c], A.Lv + q2 * tc + ci); }
+      }
+      cpa_commit();
+    };
+    auto take_own = [&](int t, LuOwn<NV>& x) {
+      const int sl = t % LU_RING;
 #pragma unroll
       for (int m = 0; m < NV; m++) {
-        double u = __ldg(A.U + m * tb + bi);
+        const double u = R.oU[sl][m][c];
         x.U[m] = m >= 5 ? clamp0(u) : u;
-        // upper sweep: R is DU* of the lower sweep, read before this thread overwrites it
-        x.R[m] = UPPER ? A.DU[m * tc + ci] : ldro(A.Res + m * tc + ci);
+        x.R[m] = (double)R.oR[sl][m][c];
       }
-      x.vol = __ldg(A.vold + ci);
-      x.dt = ldro(A.dt + ci);
+      x.vol = R.ovol[sl][c];
+      x.dt = (double)R.odt[sl][c];
 #pragma unroll
-      for (int q2 = 0; q2 < 3; q2++) { x.Lc[q2] = ldro(A.Lc + q2 * tc + ci); x.Lv[q2] = ldro(A.Lv + q2 * tc + ci); }
+      for (int q2 = 0; q2 < 3; q2++) { x.Lc[q2] = (double)R.oLc[sl][q2][c]; x.Lv[q2] = (double)R.oLv[sl][q2][c]; }
     };
 
-    // direction thread state for the current step: old-state half of the flux difference
-    double un1 = 0.0, F1[NV], n1 = 0.0, n2 = 0.0, n3 = 0.0, S = 0.0, wLc = 0.0, Lvn = 0.0, Unb[NV];
+    // direction thread state for the current step: old-state half of the flux difference.  The
+    // flux difference DF = F(U+DU)n - F(U)n is evaluated in the flux precision DFT (FP32 in the
+    // mixed form, as the reconstruction and the fluxes; FP64 otherwise); its products with S and
+    // the spectral-radius terms, the sum and the division by the diagonal stay FP64.
+    using DFT = T;
+    DFT un1 = 0, F1[NV], n1 = 0, n2 = 0, n3 = 0, Unb[NV];
+    double S = 0.0, wLc = 0.0, Lvn = 0.0;
     bool has = false;
     // comput_DFn's U terms (sub_LU_SGS.f90:135-157) of step t; in-tile neighbours' old state is
     // read from s_old[(t-1)&1], published by their owners during step t-1
     auto prep_dir = [&](int t, const LuDir<NV>& x) {
       has = on_at(t) && has_at(t);
       if (!has) return;
-      n1 = x.n1; n2 = x.n2; n3 = x.n3; S = x.S;
+      n1 = (DFT)x.n1; n2 = (DFT)x.n2; n3 = (DFT)x.n3; S = x.S;
       if (xt) {
         Lvn = x.Lv;
         wLc = w * x.wLc;
 #pragma unroll
-        for (int m = 0; m < NV; m++) Unb[m] = x.Unb[m];
+        for (int m = 0; m < NV; m++) Unb[m] = (DFT)x.Unb[m];
       } else {
         const int pb = (t - 1) & 1;
         Lvn = s_old[pb][NV + 3 + d][pubcol];
         wLc = w * s_old[pb][NV + d][pubcol];
 #pragma unroll
-        for (int m = 0; m < NV; m++) Unb[m] = s_old[pb][m][pubcol];
+        for (int m = 0; m < NV; m++) Unb[m] = (DFT)s_old[pb][m][pubcol];
       }
+      const DFT g1 = (DFT)(gamma - 1.0), half = (DFT)0.5;
       un1 = (Unb[1] * n1 + Unb[2] * n2 + Unb[3] * n3) / Unb[0];
-      const double p1 = (gamma - 1.0) * (Unb[4] - 0.5 * (sq(Unb[1]) + sq(Unb[2]) + sq(Unb[3])) / Unb[0]);
+      const DFT p1 = g1 * (Unb[4] - half * (sq(Unb[1]) + sq(Unb[2]) + sq(Unb[3])) / Unb[0]);
       F1[0] = Unb[0] * un1;
       F1[1] = Unb[1] * un1 + p1 * n1;
       F1[2] = Unb[2] * un1 + p1 * n2;
@@ -479,11 +556,15 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
         if (tid == 4 * TC && t + 2 < nsteps) poll(t + 2);
       }
     } else if (owner) {
-      if (on_at(0)) load_own(0, on);
+      issue_own(0);
+      issue_own(1);
       cta_bar<NT>();  // B0
       for (int t = 0; t < nsteps; t++) {
         cta_bar<NT>();  // B1
+        cpa_wait<1>();  // step t's group (only step t+1's may be outstanding)
         if (on_at(t)) {
+          LuOwn<NV> on;
+          take_own(t, on);
           prep_own(on);
 #pragma unroll
           for (int m = 0; m < NV; m++) { s_old[t & 1][m][c] = oU[m]; s_diag[m][c] = oR[m]; }
@@ -492,20 +573,26 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
           s_diag[NV][c] = alfa[0];
           s_diag[NV + 1][c] = alfa[NV - 1];
         }
-        if (on_at(t + 1)) load_own(t + 1, on);
+        issue_own(t + 2);  // into the slot step t-1 used
         cta_bar<NT>();  // B2: the three direction terms of step t are in shared memory
         if (on_at(t)) {
-          const long long ci = cix(B, i_of(t), j, k);
+          const long long ci = cb + i_of(t);
 #pragma unroll
           for (int m = 3; m < NV; m++) finish(m, ci);
         }
       }
     } else {
-      if (on_at(0) && has_at(0)) load_dir(0, dn);
-      prep_dir(0, dn);
+      {
+        issue_dir(0);
+        cpa_wait<0>();
+        LuDir<NV> dn;
+        take_dir(0, dn);
+        prep_dir(0, dn);
+        issue_dir(1);
+      }
       double xdu[NV];  // cross-tile neighbour's DU of the current step, loaded one step early
       auto load_xdu = [&](int t) {
-        const long long cn = cix(B, i_of(t), j + (d == 1 ? off : 0), k + (d == 2 ? off : 0));
+        const long long cn = cb + i_of(t) + dcn;
 #pragma unroll
         for (int m = 0; m < NV; m++) xdu[m] = __ldcg(A.DU + m * tc + cn);
       };
@@ -513,7 +600,7 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
       if (xt && has) load_xdu(0);
       for (int t = 0; t < nsteps; t++) {
         cta_bar<NT>();  // B1: step t-1 finished (DU in s_pub and in HBM), upstream tiles ready
-        if (on_at(t + 1) && has_at(t + 1)) load_dir(t + 1, dn);
+        issue_dir(t + 2);  // into the slot step t-1 used
         if (has) {
           double DUn[NV];
           if (!xt) {
@@ -523,12 +610,13 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
 #pragma unroll
             for (int m = 0; m < NV; m++) DUn[m] = xdu[m];
           }
-          double U2[NV];
+          DFT U2[NV];
 #pragma unroll
-          for (int m = 0; m < NV; m++) U2[m] = Unb[m] + DUn[m];
-          const double un2 = (U2[1] * n1 + U2[2] * n2 + U2[3] * n3) / U2[0];
-          const double pp2 = (gamma - 1.0) * (U2[4] - 0.5 * (sq(U2[1]) + sq(U2[2]) + sq(U2[3])) / U2[0]);
-          double DF[NV];
+          for (int m = 0; m < NV; m++) U2[m] = (DFT)((double)Unb[m] + DUn[m]);
+          const DFT g1 = (DFT)(gamma - 1.0), half = (DFT)0.5;
+          const DFT un2 = (U2[1] * n1 + U2[2] * n2 + U2[3] * n3) / U2[0];
+          const DFT pp2 = g1 * (U2[4] - half * (sq(U2[1]) + sq(U2[2]) + sq(U2[3])) / U2[0]);
+          DFT DF[NV];
           DF[0] = U2[0] * un2 - F1[0];
           DF[1] = (U2[1] * un2 + pp2 * n1) - F1[1];
           DF[2] = (U2[2] * un2 + pp2 * n2) - F1[2];
@@ -539,8 +627,8 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
 #pragma unroll
           for (int m = 0; m < NV; m++) {
             double v;
-            if (!UPPER) v = 0.5 * (DF[m] * S + wLc * DUn[m]);
-            else v = -(0.5 * (DF[m] * S - wLc * DUn[m]));
+            if (!UPPER) v = 0.5 * ((double)DF[m] * S + wLc * DUn[m]);
+            else v = -(0.5 * ((double)DF[m] * S - wLc * DUn[m]));
             if (visc) v = v + Lvn * DUn[m];
             s_acc[d][m][c] = v;
           }
@@ -549,14 +637,28 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
           for (int m = 0; m < NV; m++) s_acc[d][m][c] = 0.0;
         }
         cta_bar<NT>();  // B2
-        if (on_at(t)) finish(d, cix(B, i_of(t), j, k));
-        prep_dir(t + 1, dn);
+        if (on_at(t)) finish(d, cb + i_of(t));
+        cpa_wait<1>();  // step t+1's group (only step t+2's may be outstanding)
+        {
+          LuDir<NV> dn;
+          take_dir(t + 1, dn);
+          prep_dir(t + 1, dn);
+        }
         if (xt && has) load_xdu(t + 1);  // ready since the poller's wait of step t-1
       }
     }
+    cpa_wait<0>();  // no copy of this tile is still landing when the next tile reuses the ring
     __syncthreads();
     if (tid == 0) st_release(L.progress + my, nsteps);
   }
+}
+
+template <class T, int NV, bool UPPER, int TC>
+inline size_t lu_wave3_smem() { return sizeof(LuRing<T, NV, UPPER, TC>); }
+// the ring lives in dynamic shared memory (above the 48 KB static limit for TC = 64)
+template <class T, int NV, bool UPPER, int TC>
+inline void lu_wave3_prepare() {
+  cudaFuncSetAttribute(k_lusgs_wave3<T, NV, UPPER, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_wave3_smem<T, NV, UPPER, TC>());
 }
 
 }  // namespace ocfd

@@ -278,11 +278,6 @@ struct LuDir {      // direction-thread data of one step (old state only)
   double wLc, Lv;   // Lc and Lv of the neighbour in this direction (cross-tile only)
 };
 
-template <int NV>
-struct LuOwn {      // owner data of one step
-  double U[NV], R[NV];
-  double vol, dt, Lc[3], Lv[3];
-};
 
 __device__ __forceinline__ double ldro(const double* p) { return __ldg(p); }
 // CTA-wide barrier on a named barrier (warp-uniform callers; the owner and direction warps
@@ -331,8 +326,7 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
   __shared__ int s_tile;
   __shared__ double s_acc[3][NV][TC];      // direction terms of the current step
   __shared__ double s_pub[NV][TC];         // DU of each column's last cell
-  __shared__ double s_old[2][NV + 6][TC];  // old state U, Lc(3), Lv(3) of each column's cell, by step parity
-  __shared__ double s_diag[NV + 2][TC];    // R (NV) and the diagonal (all variables; the SA variable's) of the current step
+  __shared__ double s_diag[2][TC];         // the diagonal of the current step (all variables; the SA variable's)
   const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
   const int TJ = L.TJ, TK = L.TK;
   // thread groups: 0..2 direction threads, 3 owner (TC threads each), 4 the poller warp (lane 0
@@ -444,19 +438,6 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
       }
       cpa_commit();
     };
-    auto take_own = [&](int t, LuOwn<NV>& x) {
-      const int sl = t % LU_RING;
-#pragma unroll
-      for (int m = 0; m < NV; m++) {
-        const double u = R.oU[sl][m][c];
-        x.U[m] = m >= 5 ? clamp0(u) : u;
-        x.R[m] = (double)R.oR[sl][m][c];
-      }
-      x.vol = R.ovol[sl][c];
-      x.dt = (double)R.odt[sl][c];
-#pragma unroll
-      for (int q2 = 0; q2 < 3; q2++) { x.Lc[q2] = (double)R.oLc[sl][q2][c]; x.Lv[q2] = (double)R.oLv[sl][q2][c]; }
-    };
 
     // direction thread state for the current step: old-state half of the flux difference.  The
     // flux difference DF = F(U+DU)n - F(U)n is evaluated in the flux precision DFT (FP32 in the
@@ -466,8 +447,9 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
     DFT un1 = 0, F1[NV], n1 = 0, n2 = 0, n3 = 0, Unb[NV];
     double S = 0.0, wLc = 0.0, Lvn = 0.0;
     bool has = false;
-    // comput_DFn's U terms (sub_LU_SGS.f90:135-157) of step t; in-tile neighbours' old state is
-    // read from s_old[(t-1)&1], published by their owners during step t-1
+    // comput_DFn's U terms (sub_LU_SGS.f90:135-157) of step t; an in-tile neighbour's old state is
+    // read from its owner's ring slot of step t-1 (complete since the owner's wait in step t-1,
+    // ordered before this read by barrier B2 of step t-1)
     auto prep_dir = [&](int t, const LuDir<NV>& x) {
       has = on_at(t) && has_at(t);
       if (!has) return;
@@ -478,11 +460,14 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
 #pragma unroll
         for (int m = 0; m < NV; m++) Unb[m] = (DFT)x.Unb[m];
       } else {
-        const int pb = (t - 1) & 1;
-        Lvn = s_old[pb][NV + 3 + d][pubcol];
-        wLc = w * s_old[pb][NV + d][pubcol];
+        const int pb = (t + LU_RING - 1) % LU_RING;
+        Lvn = (double)R.oLv[pb][d][pubcol];
+        wLc = w * (double)R.oLc[pb][d][pubcol];
 #pragma unroll
-        for (int m = 0; m < NV; m++) Unb[m] = (DFT)s_old[pb][m][pubcol];
+        for (int m = 0; m < NV; m++) {
+          const double u = R.oU[pb][m][pubcol];
+          Unb[m] = (DFT)(m >= 5 ? clamp0(u) : u);
+        }
       }
       const DFT g1 = (DFT)(gamma - 1.0), half = (DFT)0.5;
       un1 = (Unb[1] * n1 + Unb[2] * n2 + Unb[3] * n3) / Unb[0];
@@ -495,27 +480,29 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
 #pragma unroll
       for (int m = 5; m < NV; m++) F1[m] = Unb[m] * un1;
     };
-    // owner state for the current step
-    double oU[NV], oR[NV], alfa[NV], oL[6];
-    auto prep_own = [&](const LuOwn<NV>& x) {  // diagonal (sub_LU_SGS.f90:50-62, 90-92)
-      const double a0 = x.vol / x.dt + w * (x.Lc[0] + x.Lc[1] + x.Lc[2]);
-#pragma unroll
-      for (int m = 0; m < NV; m++) { alfa[m] = a0; oU[m] = x.U[m]; oR[m] = x.R[m]; }
-#pragma unroll
-      for (int q2 = 0; q2 < 3; q2++) { oL[q2] = x.Lc[q2]; oL[3 + q2] = x.Lv[q2]; }
+    // the diagonal of step t's cell from the owner's ring slot (sub_LU_SGS.f90:50-62, 90-92): the
+    // value of every variable, and the SA variable's (its extra Lv term)
+    auto diag_own = [&](int t) {
+      const int sl = t % LU_RING;
+      const double vol = R.ovol[sl][c], dt = (double)R.odt[sl][c];
+      const double a0 = vol / dt + w * ((double)R.oLc[sl][0][c] + (double)R.oLc[sl][1][c] + (double)R.oLc[sl][2][c]);
+      double al = a0, als = a0;
       if (visc) {
-        const double lv = x.Lv[0] + x.Lv[1] + x.Lv[2];
-#pragma unroll
-        for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + 2.0 * lv;
-        if (NV == 6) {
-          if (!UPPER) alfa[5] = alfa[5] + lv;
-          else alfa[5] = alfa[5] + x.Lv[0] + x.Lv[1] + x.Lv[2];
+        const double lv0 = R.oLv[sl][0][c], lv1 = R.oLv[sl][1][c], lv2 = R.oLv[sl][2][c];
+        const double lv = lv0 + lv1 + lv2;
+        al = al + 2.0 * lv;
+        als = als + 2.0 * lv;
+        if (NV == 6) {  // lower: + (Lv sum); upper: + Lv1 + Lv2 + Lv3 term by term (sub_LU_SGS.f90:60-62, 90-92)
+          if (!UPPER) als = als + lv;
+          else als = als + lv0 + lv1 + lv2;
         }
       }
       if (dual) {  // dual time: + Sfac1 vol (sub_LU_SGS.f90:39, 92)
-#pragma unroll
-        for (int m = 0; m < NV; m++) alfa[m] = alfa[m] + sfac1 * x.vol;
+        al = al + sfac1 * vol;
+        als = als + sfac1 * vol;
       }
+      s_diag[0][c] = al;
+      s_diag[1][c] = NV == 6 ? als : al;
     };
 
     int seen_j = 0, seen_k = 0;
@@ -533,11 +520,12 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
     //   phase B (after B2): the final divisions are shared: direction thread d computes DU of
     //     variable d, the owner the variables 3..NV-1; direction threads then prepare the next
     //     step's old-state terms, and thread 0 completes the poll of the upstream tiles.
-    auto diag_of = [&](int m) { return (NV == 6 && m == 5) ? s_diag[NV + 1][c] : s_diag[NV][c]; };
-    auto finish = [&](int m, long long ci) {  // sub_LU_SGS.f90:63-72 (lower), 108-117 (upper)
+    auto diag_of = [&](int m) { return (NV == 6 && m == 5) ? s_diag[1][c] : s_diag[0][c]; };
+    auto finish = [&](int m, int t, long long ci) {  // sub_LU_SGS.f90:63-72 (lower), 108-117 (upper)
+      const double rm = (double)R.oR[t % LU_RING][m][c];
       double r;
-      if (!UPPER) r = (s_diag[m][c] + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
-      else r = s_diag[m][c] + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
       A.DU[m * tc + ci] = r;
       s_pub[m][c] = r;
     };
@@ -562,23 +550,13 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
       for (int t = 0; t < nsteps; t++) {
         cta_bar<NT>();  // B1
         cpa_wait<1>();  // step t's group (only step t+1's may be outstanding)
-        if (on_at(t)) {
-          LuOwn<NV> on;
-          take_own(t, on);
-          prep_own(on);
-#pragma unroll
-          for (int m = 0; m < NV; m++) { s_old[t & 1][m][c] = oU[m]; s_diag[m][c] = oR[m]; }
-#pragma unroll
-          for (int q2 = 0; q2 < 6; q2++) s_old[t & 1][NV + q2][c] = oL[q2];
-          s_diag[NV][c] = alfa[0];
-          s_diag[NV + 1][c] = alfa[NV - 1];
-        }
+        if (on_at(t)) diag_own(t);
         issue_own(t + 2);  // into the slot step t-1 used
         cta_bar<NT>();  // B2: the three direction terms of step t are in shared memory
         if (on_at(t)) {
           const long long ci = cb + i_of(t);
 #pragma unroll
-          for (int m = 3; m < NV; m++) finish(m, ci);
+          for (int m = 3; m < NV; m++) finish(m, t, ci);
         }
       }
     } else {
@@ -637,7 +615,7 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
           for (int m = 0; m < NV; m++) s_acc[d][m][c] = 0.0;
         }
         cta_bar<NT>();  // B2
-        if (on_at(t)) finish(d, cb + i_of(t));
+        if (on_at(t)) finish(d, t, cb + i_of(t));
         cpa_wait<1>();  // step t+1's group (only step t+2's may be outstanding)
         {
           LuDir<NV> dn;

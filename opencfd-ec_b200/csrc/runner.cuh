@@ -137,7 +137,8 @@ class RunnerT : public Runner {
       const int fresh = I_.exchange(I_.exchange_ctx, st);
       if (fresh && I_.xr_cells > 0) k_halo_unpack<T, NV><<<grid_of(I_.xr_cells), 256, 0, st>>>(A, I_.xr_sub, I_.xr_pre, I_.nxr, I_.xr_cells, I_.xrecv);
     }
-    k_corner<T, NV><<<A.nblk, 256, 0, st>>>(A);
+    k_corner<T, NV><<<dim3(A.nblk, 8), 256, 0, st>>>(A);
+    k_corner_vtx<T, NV><<<grid_of((long long)A.nblk * NV * 8, 128), 128, 0, st>>>(A);
   }
 
   void limit(cudaStream_t st) {
@@ -216,7 +217,7 @@ class RunnerT : public Runner {
     int upd = 1 + 1 + (NV == 6 ? 3 : 0);
     int nbc = 0;
     for (int r = 0; r < I_.nround; r++) nbc += I_.bc_rounds[3 * r + 2] > 0;
-    int bch = nbc + 1 + (A_.tot_halo > 0 ? (I_.nhlevel ? 2 * I_.nhlevel : 1) : 0) + (I_.xs_cells > 0) + (I_.xr_cells > 0);
+    int bch = nbc + 2 + (A_.tot_halo > 0 ? (I_.nhlevel ? 2 * I_.nhlevel : 1) : 0) + (I_.xs_cells > 0) + (I_.xr_cells > 0);
     int n;
     if (I_.time_method == -1) return res + 1 + lu + upd + bch;  // one dual-time inner iteration
     if (I_.time_method == 0) n = res + lu + upd + bch;

@@ -1426,7 +1426,7 @@ __global__ void k_halo_unpack(Arena<T> A, const SubD* sub, const long long* pre,
 
 // edge and vertex ghosts by averaging (get_U_conner, sub_update_buffer_mpi.f90:515-549)
 template <class T, int NV>
-__global__ void k_corner(Arena<T> A) {
+__global__ void k_corner(Arena<T> A) {  // edges: grid (blocks, CTAs per block)
   const int b = blockIdx.x;
   if (b >= A.nblk) return;
   const BlkD& B = A.blk[b];
@@ -1436,7 +1436,7 @@ __global__ void k_corner(Arena<T> A) {
   auto u = [&](int m, int i, int j, int k) -> double& { return U[m * tb + bix(B, i, j, k)]; };
   int nk = nz - 1, nj = ny - 1, ni = nx - 1;
   long long n = (long long)NV * 4 * (nk + nj + ni);
-  for (long long l = threadIdx.x; l < n; l += blockDim.x) {
+  for (long long l = (long long)blockIdx.y * blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.y * blockDim.x) {
     int m = (int)(l % NV);
     long long r = l / NV;
     int e = (int)(r % 4);
@@ -1461,9 +1461,21 @@ __global__ void k_corner(Arena<T> A) {
       else u(m, i, ny, nz) = (u(m, i, ny - 1, nz) + u(m, i, ny, nz - 1)) * 0.5;
     }
   }
-  __syncthreads();
-  if (threadIdx.x < NV * 8) {
-    int m = threadIdx.x % NV, v = threadIdx.x / NV;
+}
+// the 8 vertices of every block from the edge values (after k_corner)
+template <class T, int NV>
+__global__ void k_corner_vtx(Arena<T> A) {
+  const long long tb = A.tot_box;
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)A.nblk * NV * 8) return;
+  const int b = (int)(g / (NV * 8));
+  const BlkD& B = A.blk[b];
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  double* U = A.U;
+  auto u = [&](int m, int i, int j, int k) -> double& { return U[m * tb + bix(B, i, j, k)]; };
+  {
+    const int r = (int)(g % (NV * 8));
+    int m = r % NV, v = r / NV;
     int ia = (v & 1) ? nx : 0, ja = (v & 2) ? ny : 0, kz = (v & 4) ? nz : 0;
     int ib = (v & 1) ? nx - 1 : 1, jb = (v & 2) ? ny - 1 : 1, kb = (v & 4) ? nz - 1 : 1;
     u(m, ia, ja, kz) = (2.0 * (u(m, ib, ja, kz) + u(m, ia, jb, kz) + u(m, ia, ja, kb)) - (u(m, ib, jb, kz) + u(m, ib, ja, kb) + u(m, ia, jb, kb))) / 3.0;

@@ -238,7 +238,7 @@ def config3_leg(args, nsteps=20):
     return out
 
 
-def serving_leg(max_iters=1500, n=14, rate=2.0):
+def serving_leg(max_iters=5000, n=14, rate=2.0):
     """Continuous batching: Poisson arrivals (rate/s) of seeded airfoil solves (config 4 sizes) and
     reduced swept wings, run to a 1e-6 residual drop or |dCL| < 1e-4 over 200 iterations (at most
     max_iters); p50 / p99 time from arrival to convergence, beside the same requests run one at a

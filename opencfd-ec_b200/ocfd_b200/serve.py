@@ -2,9 +2,10 @@
 
 Requests (a case + its parameters) arrive over time.  The loop admits a waiting request as soon
 as a slot is free and its device footprint (``ocfd_footprint``) fits in the HBM budget, keeps
-every admitted solve resident on the device, and advances all admitted solves together: each
-round queues ``chunk`` iterations on every handle's own stream (so the solves overlap on the
-GPU) and then reads back each solve's residual norms and forces.  A solve leaves as soon as it
+every admitted solve resident on the device, and advances every admitted solve at its own pace:
+``chunk`` iterations are queued on the handle's own stream (so the solves overlap on the GPU),
+and as soon as that stream is idle the loop reads back the solve's residual norms and forces and
+queues its next chunk, without waiting for larger solves in the mix.  A solve leaves as soon as it
 converges (density-residual RMS down by ``drop`` from its first iteration, or |dCL| below
 ``dcl`` over the last ``dcl_window`` iterations) or reaches ``max_iters``; its memory is
 released for the next admission.
@@ -53,10 +54,12 @@ class Result:
 
 class _Active:
     def __init__(self, req, solver, admitted):
+        import torch
         self.req, self.s, self.admitted = req, solver, admitted
         self.iters = 0
         self.rms0 = None
         self.cl_hist = []    # (iteration, CL) at every read-back
+        self.stream = torch.cuda.ExternalStream(solver.stream())  # idle test without blocking
 
 
 class Server:
@@ -121,17 +124,19 @@ class Server:
                 if pending:
                     time.sleep(max(0.0, min(0.05, pending[0].arrival - (self.clock() - t0))))
                 continue
-            # one round: queue work on every stream first, then read each solve back
+            # every solve whose queued chunk has finished is read back and given its next chunk;
+            # the others keep running
+            still, progressed = [], False
             for a in active:
-                if a.iters > 1 or a.rms0 is not None:
-                    n = min(self.chunk, a.req.max_iters - a.iters)
-                    if n > 0:
-                        a.s.advance(n)
-                        a.iters += n
-            still = []
-            for a in active:
+                if not a.stream.query():
+                    still.append(a)
+                    continue
+                progressed = True
                 why, rms, cl, cd = self._done(a)
                 if why is None:
+                    n = min(self.chunk, a.req.max_iters - a.iters)
+                    a.s.advance(n)
+                    a.iters += n
                     still.append(a)
                     continue
                 fin = self.clock() - t0
@@ -140,6 +145,8 @@ class Server:
                 a.s.close()
                 used -= fp[a.req.rid]
             active = still
+            if not progressed:
+                time.sleep(0.0002)
         return sorted(results, key=lambda r: r.rid)
 
 

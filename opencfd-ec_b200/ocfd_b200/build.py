@@ -36,8 +36,26 @@ def up_to_date():
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
+DRIVER_SRC = os.path.join(ROOT_DIR, "driver", "ocfd_drive.cpp")
+DRIVER_PATH = os.path.join(ROOT_DIR, "ocfd_drive")
+
+
+def build_driver(force=False):
+    """The compiled C++ caller of the C-ABI (driver/ocfd_drive.cpp), linked against the in-tree
+    library (found next to it at run time)."""
+    deps = [DRIVER_SRC, LIB_PATH, os.path.join(os.path.dirname(ROOT_DIR), "include", "ocfd_ec_gpu.h")]
+    if not force and os.path.exists(DRIVER_PATH) and all(os.path.getmtime(d) <= os.path.getmtime(DRIVER_PATH) for d in deps):
+        return DRIVER_PATH
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-ffp-contract=off", "-std=c++17", DRIVER_SRC, "-L" + ROOT_DIR, "-locfd_b200",
+           "-Wl,-rpath,$ORIGIN", "-o", DRIVER_PATH + ".tmp"]
+    subprocess.check_call(cmd)
+    os.replace(DRIVER_PATH + ".tmp", DRIVER_PATH)
+    return DRIVER_PATH
+
+
 def build(force=False, verbose=False, extra=()):
     if not force and up_to_date():
+        build_driver()
         return LIB_PATH
     os.makedirs(BUILD_DIR, exist_ok=True)
     objs = []
@@ -63,6 +81,7 @@ def build(force=False, verbose=False, extra=()):
     cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
     subprocess.check_call(cmd)
     os.replace(tmp, LIB_PATH)
+    build_driver(force=True)
     return LIB_PATH
 
 

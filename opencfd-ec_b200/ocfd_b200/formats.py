@@ -105,6 +105,33 @@ def case_from_files(mesh_path, inp_path, name=None, formatted=False):
     return Case(name or os.path.basename(os.path.dirname(os.path.abspath(mesh_path))), xyz, inp)
 
 
+# ---- bc3d.inc ------------------------------------------------------------------------------
+def write_bc3d_inc(path, case):
+    """bc3d.inc as convert_inp_inc writes it (sub_convert_inp.f90:103-114) and read_inc reads it
+    (sub_IO.f90:656-743): a title line, the block count, then per block its node counts, a label
+    line, its subface count and per subface the 9 + 12 integers of the .inc record."""
+    nijk, _, nsub, inc = case.flat()
+    rec = np.asarray(inc).reshape(-1, 21)
+    with open(path, "w") as f:
+        f.write(" Inp-liked file of OpenCFD-EC\n")
+        f.write(" %d\n" % len(case.dims))
+        t = 0
+        for b, (nx, ny, nz) in enumerate(case.dims):
+            f.write(" %d %d %d\n" % (nx, ny, nz))
+            f.write(" Block %d\n" % (b + 1))
+            f.write(" %d\n" % nsub[b])
+            for _ in range(nsub[b]):
+                f.write("".join("%6d" % v for v in rec[t, :9]) + "\n")
+                f.write("".join("%6d" % v for v in rec[t, 9:]) + "\n")
+                t += 1
+
+
+def write_case_files(directory, case, formatted=False):
+    """Mesh3d.dat and bc3d.inc of a case, the two files the reference's driver reads."""
+    write_mesh3d(os.path.join(directory, "Mesh3d.dat"), case.xyz, formatted)
+    write_bc3d_inc(os.path.join(directory, "bc3d.inc"), case)
+
+
 # ---- wall_dist.dat -----------------------------------------------------------------------
 def write_wall_dist(path, dw):
     """dw: per block cell-centre distances, (nz-1, ny-1, nx-1)."""

@@ -120,6 +120,7 @@ struct ocfd_handle {
   int* d_flags = nullptr;
   double *d_norm_part = nullptr, *d_norm_out = nullptr, *d_force_part = nullptr, *d_stage = nullptr;
   unsigned long long* d_nan = nullptr;
+  double* h_pin = nullptr;  // pinned read-back area of the monitors: norms, NaN location, wait flag, force partials
   long long max_box_b = 0;
   Arena<double> A64;
   Arena<float> A32;
@@ -526,7 +527,8 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   for (int s = 0; s < ns; s++) {
     if (h->sub[s].bc != 2) continue;
     long long n = subcell_count(h->sub[s]);
-    for (long long s0 = 0; s0 < n; s0 += 4096) h->wchunk.push_back(make_int4(s, (int)s0, (int)std::min<long long>(4096, n - s0), 0));
+    // 512 wall faces per chunk: enough CTAs for a wing's few thousand wall faces
+    for (long long s0 = 0; s0 < n; s0 += 512) h->wchunk.push_back(make_int4(s, (int)s0, (int)std::min<long long>(512, n - s0), 0));
   }
   // boundary rounds: round r holds the r-th subface of every block (physical subfaces only); the
   // cells of an entry are the subface's face cells (walls, symmetry) or its inclusive node range
@@ -1147,6 +1149,7 @@ extern "C" int ocfd_synchronize(ocfd_handle* h) {
 extern "C" int ocfd_destroy(ocfd_handle* h) {
   if (!h) return OCFD_OK;
   if (h->st) cudaStreamSynchronize(h->st);
+  if (h->h_pin) cudaFreeHost(h->h_pin);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   h->run.reset();
@@ -1290,19 +1293,33 @@ extern "C" int ocfd_compute_residual(ocfd_handle* h, int with_lusgs) {
   return OCFD_OK;
 }
 
+// pinned host area the monitors are read back into (one asynchronous copy each, one wait per call);
+// allocated at the first read-back
+static double* pin_area(ocfd_handle* h) {
+  if (!h->h_pin) {
+    const size_t n = 14 * (size_t)h->nsolve + 2 + 9 * std::max<size_t>(1, h->wchunk.size());
+    if (cudaMallocHost((void**)&h->h_pin, n * sizeof(double)) != cudaSuccess) h->h_pin = nullptr;
+  }
+  return h->h_pin;
+}
+
 // norms of every solve (nout = 1: solve 0 only); NaN -> OCFD_ERR_NAN with the first location
 static int residual_impl(ocfd_handle* h, double* rmax, double* rrms, int nout) {
-  unsigned long long init = ~0ULL;
-  cudaMemcpyAsync(h->d_nan, &init, 8, cudaMemcpyHostToDevice, h->st);
+  double* pin = pin_area(h);
+  if (!pin) return fail(h, OCFD_ERR_OOM, "pinned read-back area");
+  const size_t no = 14 * (size_t)h->nsolve;
+  cudaMemsetAsync(h->d_nan, 0xFF, 8, h->st);  // "no NaN seen": all ones
   h->run->norms(h->st, h->d_norm_part, h->d_norm_out, h->d_nan);
-  std::vector<double> out(14 * (size_t)h->nsolve);
-  unsigned long long nan_at = 0;
-  cudaMemcpyAsync(out.data(), h->d_norm_out, out.size() * 8, cudaMemcpyDeviceToHost, h->st);
-  cudaMemcpyAsync(&nan_at, h->d_nan, 8, cudaMemcpyDeviceToHost, h->st);
+  cudaMemcpyAsync(pin, h->d_norm_out, no * 8, cudaMemcpyDeviceToHost, h->st);
+  cudaMemcpyAsync(pin + no, h->d_nan, 8, cudaMemcpyDeviceToHost, h->st);
+  cudaMemcpyAsync(pin + no + 1, h->d_lu_err, 4, cudaMemcpyDeviceToHost, h->st);
   cudaError_t e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "residual");
+  std::vector<double> out(pin, pin + no);
+  unsigned long long nan_at = 0;
+  std::memcpy(&nan_at, pin + no, 8);
   int lu_err = 0;
-  cudaMemcpy(&lu_err, h->d_lu_err, 4, cudaMemcpyDeviceToHost);
+  std::memcpy(&lu_err, pin + no + 1, 4);
   bool other_nan = false, other_lu = false;
   if (h->part) {  // MPI_ALLREDUCE of the maxima and the sums of squares (sub_time_advance.f90:373-374)
     double mx[9], sm[7];
@@ -1434,13 +1451,17 @@ extern "C" int ocfd_residual_static(ocfd_handle* h, double* rmax, double* rrms) 
 // the solve's blocks (sub_Post.f90:31-202)
 static int forces_impl(ocfd_handle* h, double* ft, double* cl, double* cd, double* cs, int nout) {
   size_t nw = h->wchunk.size();
+  double* pin = pin_area(h);
+  if (!pin) return fail(h, OCFD_ERR_OOM, "pinned read-back area");
+  double* pf = pin + 14 * (size_t)h->nsolve + 2;
   std::vector<double> part(9 * std::max<size_t>(nw, 1), 0.0);
   if (nw) {
     h->run->forces(h->st, h->d_force_part);
-    cudaMemcpyAsync(part.data(), h->d_force_part, nw * 9 * 8, cudaMemcpyDeviceToHost, h->st);
+    cudaMemcpyAsync(pf, h->d_force_part, nw * 9 * 8, cudaMemcpyDeviceToHost, h->st);
   }
   cudaError_t e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "forces");
+  if (nw) std::copy(pf, pf + 9 * nw, part.begin());
   std::vector<double> blk(9 * h->nblk, 0.0);
   for (size_t c = 0; c < nw; c++) {
     int b = h->sub[h->wchunk[c].x].blk;

@@ -1496,7 +1496,8 @@ __global__ void k_norms(Arena<T> A, double* part, unsigned long long* nan_at) {
   double mx[NV], sm[NV];
 #pragma unroll
   for (int m = 0; m < NV; m++) { mx[m] = 0.0; sm[m] = 0.0; }
-  for (int l = threadIdx.x; l < ch.z; l += blockDim.x) {
+#pragma unroll 4
+  for (int l = threadIdx.x; l < ch.z; l += blockDim.x) {  // unrolled: loads of 4 cells in flight, sums in order
     long long g = B.ocell + ch.y + l;
 #pragma unroll
     for (int m = 0; m < NV; m++) {

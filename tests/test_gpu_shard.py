@@ -1,8 +1,9 @@
 """Block-sharded solves on the GPU (ocfd_create_part): n ranks as host threads of one process on
 one GPU (ThreadComm: the exchange buffers move by device copies, the waits are host barriers with
 a timeout, no kernel waits on another rank).  Each rank's blocks must equal the same blocks of the
-unsharded solve bit for bit after every step (LU-SGS, RK3, dual time), and the all-reduced norms
-and forces must equal the unsharded ones up to the summation order (1e-12)."""
+unsharded solve bit for bit after every step (LU-SGS in FP64 and mixed precision, RK3, dual time),
+and the all-reduced norms and forces must equal the unsharded ones up to the summation order
+(1e-12)."""
 import threading
 
 import numpy as np
@@ -47,6 +48,7 @@ def _cases():
     return {
         "wing8_sa_lusgs": (lambda: cases.config2_small(), 2),
         "wing8_sa_lusgs_3ranks": (lambda: cases.config2_small(), 3),
+        "wing8_sa_lusgs_mixed": (lambda: cases.config2_small(precision=1), 2),
         "bump2_rk3": (lambda: cases.config1(scale=0.25, cuts_i=(12,), time_method=3, cfl=1.0), 2),
         "bump2_dual": (lambda: cases.config1(scale=0.25, cuts_i=(12,), time_method=-1, dt_global=0.2, step_inner_limit=3,
                                              res_inner_limit=1e-14), 2),

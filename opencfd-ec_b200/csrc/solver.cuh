@@ -480,14 +480,15 @@ __global__ void k_amut(Arena<T> A) {
 }
 
 #ifndef INV_FLUX_MIXED_MINB
-#define INV_FLUX_MIXED_MINB 3
+#define INV_FLUX_MIXED_MINB 4
 #endif
 // ============================================================================================
 // inviscid fluxes (flux_inviscous_i/j/k, sub_Residual.f90:182-705)
 // ============================================================================================
-// both precisions: three 256-thread CTAs per SM (at most 80 registers; FP64 spills a few hundred
-// bytes to L1), since the kernel is bound by arithmetic latency and more warps hide more of it
-// (FP64 on config 2: 0.34 -> 0.29 ms per direction against two CTAs at 120 registers)
+// FP64: three 256-thread CTAs per SM (at most 80 registers; a few hundred bytes of spills to L1),
+// FP32: four (64 registers, no spills): the kernel is bound by arithmetic latency and more warps
+// hide more of it (FP64 on config 2: 0.34 -> 0.29 ms per direction against two CTAs at 120
+// registers; FP32: config 2 residual phase -0.07 ms, config 3 -0.26 ms against three CTAs)
 template <class T>
 struct InvFluxOcc { static constexpr int value = sizeof(T) == 8 ? 3 : INV_FLUX_MIXED_MINB; };
 // PRIM: every solve of the handle reconstructs the primitive variables (IFlag_Reconstruction = 0),

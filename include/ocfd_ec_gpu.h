@@ -312,10 +312,15 @@ void* ocfd_stream(ocfd_handle* h);
 int ocfd_profile(ocfd_handle* h, int nsteps, double* phase_ms);
 /* Kernel launches queued by one ocfd_advance step (all of them this library's own kernels). */
 int ocfd_launches_per_step(ocfd_handle* h);
-/* Columns per CTA tile (32 or 64) of the LU-SGS wavefront sweeps.  ocfd_create times both on the
- * new case (a few steps from freestream, before the state is initialised; the result does not
- * depend on the choice) and keeps the faster; OCFD_LU_TC=32|64 or OCFD_NO_AUTOTUNE=1 skip that. */
+/* Columns per CTA tile (32 or 64) of the LU-SGS wavefront sweeps, and the wavefront kernel version
+ * in use (3: inputs staged by element; 4: staged by 32-byte sector, helper warps off the step's
+ * phases; 2: one thread per column).  ocfd_create times each tile width with versions 3 and 4 on
+ * the new case (a few steps from freestream, before the state is initialised; the result does not
+ * depend on the choice) and keeps the fastest; OCFD_LU_TC=32|64 fixes the width, OCFD_LU_V3=1 or
+ * OCFD_LU_V4=1 the version, OCFD_NO_AUTOTUNE=1 takes the first candidate (64 columns if fixed,
+ * else 32; version 4 unless fixed). */
 int ocfd_lu_tile_width(const ocfd_handle* h);
+int ocfd_lu_kernel_version(const ocfd_handle* h);
 
 #ifdef __cplusplus
 }

@@ -34,9 +34,11 @@ struct DevMem {
     if (err != cudaSuccess) return nullptr;
     if (n == 0) n = 1;
     void* p = nullptr;
-    err = cudaMalloc(&p, n * sizeof(T));
+    // 32 bytes of padding: the LU-SGS sweep stages whole aligned 32-byte sectors, and the sector
+    // of an array's last element may reach up to 28 bytes past its end
+    err = cudaMalloc(&p, n * sizeof(T) + 32);
     if (err != cudaSuccess) return nullptr;
-    cudaMemset(p, 0, n * sizeof(T));
+    cudaMemset(p, 0, n * sizeof(T) + 32);
     ptrs.push_back(p);
     bytes += n * sizeof(T);
     return (T*)p;
@@ -350,10 +352,12 @@ static void reset_work(ocfd_handle* h) {
   reset_mu(h);
 }
 
-// (re)builds the runner for LU-SGS tile table v (0: TC = 32, 1: TC = 64); drops a captured graph
-static void select_lu(ocfd_handle* h, int v) {
+// (re)builds the runner for LU-SGS tile table v (0: TC = 32, 1: TC = 64) and wavefront kernel
+// version ver (2, 3 or 4); drops a captured graph
+static void select_lu(ocfd_handle* h, int v, int ver) {
   h->lu = h->lu_var[v];
   h->lu_tc = v == 0 ? 32 : 64;
+  h->info.lu_version = ver;
   h->info.lu = &h->lu;
   h->info.lu_tc = h->lu_tc;
   h->info.lu_grid = std::max(1, std::min(h->lu.ntiles, h->nsm * 8));
@@ -363,17 +367,18 @@ static void select_lu(ocfd_handle* h, int v) {
   else h->run.reset(make_runner_fp64(h->A64, h->info));
 }
 
-// Tile-width autotuner: both tile tables sweep the freshly initialised case (two warm-up and three
-// timed steps each, CUDA events around the two sweeps); the faster is kept.  The state is
-// re-initialised afterwards by the caller, and the choice does not change any result (every
-// tiling gives the hyperplane-order bits).
-static void autotune_lu(ocfd_handle* h) {
+// LU-SGS autotuner: each candidate (tile table v, kernel version ver) sweeps the freshly
+// initialised case (two warm-up and three timed steps, CUDA events around the two sweeps); the
+// fastest is kept.  The state is re-initialised afterwards by the caller, and the choice does not
+// change any result (every tiling and version gives the hyperplane-order bits).
+static void autotune_lu(ocfd_handle* h, const std::vector<std::pair<int, int>>& cand) {
   cudaEvent_t ev[6];
   for (int q = 0; q < 6; q++) cudaEventCreate(&ev[q]);
   float best = 1e30f;
-  int bestv = 0;
-  for (int v = 0; v < 2; v++) {
-    select_lu(h, v);
+  std::pair<int, int> bestv = cand[0];
+  for (const auto& vv : cand) {
+    const int v = vv.first;
+    select_lu(h, v, vv.second);
     h->run->init_flow(h->st);
     for (int s = 0; s < 2; s++) h->run->step(h->st);
     float tot = 0.0f;
@@ -385,14 +390,15 @@ static void autotune_lu(ocfd_handle* h) {
       cudaEventElapsedTime(&b2, ev[2], ev[3]);
       tot += a + b2;
     }
-    if (cudaGetLastError() == cudaSuccess && tot < best) { best = tot; bestv = v; }
+    if (cudaGetLastError() == cudaSuccess && tot < best) { best = tot; bestv = vv; }
   }
   for (int q = 0; q < 6; q++) cudaEventDestroy(ev[q]);
   reset_work(h);
-  select_lu(h, bestv);
+  select_lu(h, bestv.first, bestv.second);
 }
 
 extern "C" int ocfd_lu_tile_width(const ocfd_handle* h) { return h ? h->lu_tc : 0; }
+extern "C" int ocfd_lu_kernel_version(const ocfd_handle* h) { return h ? h->info.lu_version : 0; }
 
 // all solves of a handle share the model switches that select kernels; Mach, angles, Re, CFL,
 // schemes, fluxes and limits may differ per solve
@@ -842,7 +848,6 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   h->info.max_plane = h->max_plane;
   h->info.ncchunk = (int)h->cchunk.size(); h->info.nwchunk = (int)h->wchunk.size();
   h->info.lu_planes = std::getenv("OCFD_LUSGS_PLANES") ? 1 : 0;
-  h->info.lu_version = lu_v2 ? 2 : 3;
   h->info.bc_rounds = h->bc_rounds.data(); h->info.nround = (int)(h->bc_rounds.size() / 3);
   h->info.halo_levels = h->halo_levels.data(); h->info.nhlevel = (int)(h->halo_levels.size() / 3);
   h->info.halo_ent = h->d_halo_ent; h->info.halo_pre = h->d_halo_pre; h->info.halo_stage = h->d_halo_stage;
@@ -876,11 +881,23 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   }
   if (h->prec == OCFD_PREC_MIXED) fill_arena<float>(h, h->A32, h->d_Mf, h->d_volf, h->d_dtmf, h->d_dwf);
   else fill_arena<double>(h, h->A64, h->d_Md, h->d_vold, h->d_dtmd, h->d_dwd);
-  select_lu(h, lu_force ? (lu_force == 64 ? 1 : 0) : 0);
+  // LU-SGS kernel candidates: OCFD_LU_TC fixes the tile width, OCFD_LU_V3 / OCFD_LU_V4 the
+  // wavefront version (OCFD_LU_V2 both); the autotuner picks among the rest
+  const int lu_ver_force = lu_v2 ? 2 : (std::getenv("OCFD_LU_V3") ? 3 : (std::getenv("OCFD_LU_V4") ? 4 : 0));
+  std::vector<std::pair<int, int>> lu_cand;
+  for (int v = 0; v < 2; v++) {
+    if (lu_force && (lu_force == 64) != (v == 1)) continue;
+    for (int ver : {4, 3}) {
+      if (lu_ver_force && ver != lu_ver_force) continue;
+      lu_cand.push_back({v, ver});
+    }
+  }
+  if (lu_ver_force == 2) lu_cand.assign(1, {1, 2});
+  select_lu(h, lu_cand[0].first, lu_cand[0].second);
   if (!h->run) { M.release(); return OCFD_ERR_UNSUPPORTED; }
-  if (!lu_force && !h->info.lu_planes && !std::getenv("OCFD_NO_AUTOTUNE")) {
+  if (lu_cand.size() > 1 && !h->info.lu_planes && !std::getenv("OCFD_NO_AUTOTUNE")) {
     if (h->part) h->part->xchg = false;  // the timed steps are discarded: no exchange with other ranks
-    autotune_lu(h);
+    autotune_lu(h, lu_cand);
     if (h->part) h->part->xchg = true;
   }
   h->run->init_flow(h->st);

@@ -639,4 +639,392 @@ inline void lu_wave3_prepare() {
   cudaFuncSetAttribute(k_lusgs_wave3<T, NV, UPPER, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_wave3_smem<T, NV, UPPER, TC>());
 }
 
+// ============================================================================================
+// Version 4: the version-3 wavefront (same thread roles, barriers, poller and per-cell
+// arithmetic) with its inputs staged by 32-byte sector instead of by element.
+//
+// Every input of a column is a plane read along i, one element per step, so each plane is a
+// stream: its aligned 32-byte sectors land in two 32-byte slots per column, four 16-byte chunks
+// (chunk q = (address >> 4) & 3, so consecutive sectors alternate between the slots), copied by
+// two 16-byte cp.async when the march enters a new sector, LU4_D steps before the step that
+// first reads it.  A stream then costs one copy pair per 4 (FP64) or 8 (FP32) steps instead of
+// one scattered element copy per step: the sweep's global requests fall 2x (FP64) to 4x (FP32),
+// each a whole sector.  That request rate, not HBM bytes, bounded the element-wise staging.
+//
+// Slot lifetime: when step s issues (after barrier B1 of step s) every read of steps < s is done
+// (B1 orders it), and the sectors still to be read cover the elements of steps s .. s+LU4_D,
+// LU4_D+1 <= 5 consecutive elements: at most two sectors of 8-byte elements.  So an issue never
+// lands in a slot that a pending read or an in-flight copy uses.
+//
+// The arena pads every allocation by 32 bytes, so the sector of an array's last element is in
+// bounds.  Bytes of a sector outside the column's own elements are copied and never read.
+// ============================================================================================
+constexpr int LU4_D = 2;
+
+static_assert(LU4_D >= 1 && LU4_D <= 4, "two sector slots hold LU4_D + 1 <= 5 consecutive FP64 elements");
+
+// named barrier ID over NT threads (warp-uniform callers)
+template <int ID, int NT>
+__device__ __forceinline__ void cta_bar_id() { asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(NT) : "memory"); }
+
+__device__ __forceinline__ void cpa16(void* dst, const void* src) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(src) : "memory");
+}
+// the aligned sector holding p into the column's slots (col: the column's chunk 0, CS: chunk stride)
+__device__ __forceinline__ void sec_copy(unsigned char* col, int CS, const void* p) {
+  const size_t a = (size_t)p & ~(size_t)31;
+  unsigned char* dst = col + (int)((a >> 4) & 3) * CS;
+  cpa16(dst, (const void*)a);
+  cpa16(dst + CS, (const void*)(a + 16));
+}
+// stage p's sector when the march enters it at this step (lower sweep: addresses rise, a sector
+// starts at offset 0; upper sweep: they fall, a sector starts at its last element) or when the
+// stream's run starts here (fresh)
+template <bool UPPER, class X>
+__device__ __forceinline__ void sec_stage(unsigned char* col, int CS, const X* p, bool fresh) {
+  const unsigned lo = (unsigned)(size_t)p & 31u;
+  if (fresh || lo == (UPPER ? 32u - (unsigned)sizeof(X) : 0u)) sec_copy(col, CS, p);
+}
+template <class X>
+__device__ __forceinline__ X sec_get(const unsigned char* col, int CS, const X* p) {
+  const size_t a = (size_t)p;
+  return *reinterpret_cast<const X*>(col + (int)((a >> 4) & 3) * CS + (int)(a & 15));
+}
+
+// dynamic shared memory of version 4 (byte offsets); every stream holds four chunks
+template <int NV, int TC>
+struct Lu4Smem {
+  static constexpr int CS = TC * 16;          // chunk stride of the column-indexed streams
+  static constexpr int XN = TC / 2 + 2;       // tile-edge columns: TJ + TK <= TC / 2 + 2 as TK >= 2
+  static constexpr int XS = XN * 16;          // chunk stride of the edge streams
+  static constexpr int NOWN = 2 * NV + 8;     // owner: U[NV], R[NV], vol, dt, Lc[3], Lv[3]
+  static constexpr int NXT = NV + 2;          // edge: the cross-tile neighbour's U[NV], Lc, Lv
+  static constexpr int OWN = 0;
+  static constexpr int DIR = OWN + NOWN * 4 * CS;  // per direction: n1, n2, n3, S
+  static constexpr int XT = DIR + 3 * 4 * 4 * CS;
+  static constexpr int BYTES = XT + NXT * 4 * XS;
+  // owner stream numbers
+  static constexpr int SU = 0, SR = NV, SVOL = 2 * NV, SDT = 2 * NV + 1, SLC = 2 * NV + 2, SLV = 2 * NV + 5;
+};
+
+template <class T, int NV, bool UPPER, int TC>
+__global__ void __launch_bounds__(4 * TC + 64, OCFD_LU_MINB) k_lusgs_wave4(Arena<T> A, LuArgs L) {
+  using SM = Lu4Smem<NV, TC>;
+  constexpr int CS = SM::CS, XS = SM::XS;
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  __shared__ int s_tile;
+  __shared__ double s_acc[3][NV][TC];      // direction terms of the current step
+  __shared__ double s_pub[NV][TC];         // DU of each column's last cell
+  __shared__ double s_diag[2][TC];         // the diagonal of the current step (all variables; the SA variable's)
+  const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
+  const int TJ = L.TJ, TK = L.TK;
+  // thread groups: 0..2 direction threads, 3 owner (TC threads each), 4 the poller warp (waits
+  // for the upstream tiles' progress), 5 the publisher warp (releases this tile's progress).  The
+  // two helper warps take barriers B0 and B1 only; B2 is a separate named barrier of the 4 TC
+  // compute threads, so neither a release fence nor an acquire poll sits inside a step's phase.
+  constexpr int NT = 4 * TC + 64, NC = 4 * TC;
+  const int tid = threadIdx.x, grp = tid < 4 * TC ? tid / TC : (tid < 4 * TC + 32 ? 4 : 5), c = tid % TC;
+  const int lj = c % TJ, lk = c / TJ;
+  const bool owner = grp == 3;
+  const int d = grp;  // direction of a direction thread
+  if (TJ * TK != TC || TJ + TK > SM::XN) {  // tile shape outside the edge-stream table: refuse
+    if (tid == 0) atomicExch(L.err, 1);
+    return;
+  }
+  auto obuf = [&](int s, int cc) { return s_dyn + SM::OWN + s * 4 * CS + cc * 16; };
+  unsigned char* const dbuf = s_dyn + SM::DIR + (d < 3 ? d : 0) * 16 * CS + c * 16;  // stream s at + 4 s CS
+  unsigned char* const xbuf = s_dyn + SM::XT + (d == 1 ? lk : TK + lj) * 16;        // stream s at + 4 s XS
+  using RT = typename std::conditional<UPPER, double, T>::type;  // R: Res (lower) or DU* (upper)
+  for (;;) {
+    if (tid == 0) s_tile = atomicAdd(&L.counter[UPPER ? 1 : 0], 1);
+    __syncthreads();
+    const int q = s_tile;
+    if (q >= L.ntiles) break;
+    const LuTile tl = L.tiles[UPPER ? (L.ntiles - 1 - q) : q];
+    const BlkD& B = A.blk[tl.blk];
+    const SolveP& s = A.sp[B.solve];
+    const int nxm = B.nx - 1, nym = B.ny - 1, nzm = B.nz - 1;
+    const int j = UPPER ? (tl.j0 + TJ - 1 - lj) : (tl.j0 + lj);
+    const int k = UPPER ? (tl.k0 + TK - 1 - lk) : (tl.k0 + lk);
+    const bool active = j >= 1 && j <= nym && k >= 1 && k <= nzm;
+    const int* tb3 = L.tile_of + 3 * tl.blk;
+    const int first = tb3[0], nJ = tb3[1], nK = tb3[2];
+    const int J = (tl.j0 - 1) / TJ, K = (tl.k0 - 1) / TK;
+    int pj = -1, pk = -1;
+    if (!UPPER) {
+      if (J > 0) pj = first + (J - 1) + nJ * K;
+      if (K > 0) pk = first + J + nJ * (K - 1);
+    } else {
+      if (J < nJ - 1) pj = first + (J + 1) + nJ * K;
+      if (K < nK - 1) pk = first + J + nJ * (K + 1);
+    }
+    const int my = first + J + nJ * K;
+    const int nsteps = nxm + TJ + TK - 2;
+    const double w = s.w_lu, gamma = s.gamma;
+    const bool visc = s.viscous == 1;
+    const bool dual = s.time_method == -1;
+    const double sfac1 = dual ? A.sfac[1] : 0.0;
+    const int off = UPPER ? 1 : -1;
+    auto i_of = [&](int t) { int il = t - lj - lk; return UPPER ? (nxm - il) : (il + 1); };
+    auto on_at = [&](int t) { int il = t - lj - lk; return active && il >= 0 && il < nxm; };
+    auto has_at = [&](int t) {
+      const int i = i_of(t);
+      return UPPER ? (d == 0 ? i != nxm : (d == 1 ? j != nym : k != nzm)) : (d == 0 ? i != 1 : (d == 1 ? j != 1 : k != 1));
+    };
+    auto need_dir = [&](int t) { return on_at(t) && has_at(t); };
+    const bool xt = !owner && ((d == 1 && lj == 0) || (d == 2 && lk == 0));
+    const int pubcol = d == 0 ? c : (d == 1 ? c - 1 : c - TJ);
+    const long long cb = B.ocell - 1 + (long long)nxm * ((j - 1) + (long long)nym * (k - 1));
+    const long long bb = B.obox + 3 + (long long)B.NX * ((j + 3) + (long long)B.NY * (k + 3));
+    const long long fb = B.oface - 1 + (long long)B.nx * ((j - 1) + (long long)B.ny * (k - 1));
+    const long long dcn = d == 0 ? off : (d == 1 ? (long long)off * nxm : (long long)off * nxm * nym);
+    const long long dbn = d == 0 ? off : (d == 1 ? (long long)off * B.NX : (long long)off * B.NX * B.NY);
+    const long long dfs = !UPPER ? 0 : (d == 0 ? 1 : (d == 1 ? (long long)B.nx : (long long)B.nx * B.ny));
+    // the planes of the streams (element index: the column base + i)
+    auto Rp = [&](int m, long long ci) {
+      if (UPPER) return (const RT*)(A.DU + m * tc + ci);  // DU* of the lower sweep, read before this column overwrites it
+      return (const RT*)(A.Res + m * tc + ci);
+    };
+    const T* const pn1 = A.M + (M_NI1 + 3 * d) * tf + fb;
+    const T* const pn2 = A.M + (M_NI2 + 3 * d) * tf + fb;
+    const T* const pn3 = A.M + (M_NI3 + 3 * d) * tf + fb;
+    const T* const pS = A.M + (M_SI + d) * tf + fb + dfs;  // the lower face's area, or the upper face's (sub_LU_SGS.f90:96-97)
+
+    auto issue_dir = [&](int u) {
+      if (need_dir(u)) {
+        const bool fresh = !need_dir(u - 1);
+        const int i = i_of(u);
+        sec_stage<UPPER>(dbuf, CS, pn1 + i, fresh);
+        sec_stage<UPPER>(dbuf + 4 * CS, CS, pn2 + i, fresh);
+        sec_stage<UPPER>(dbuf + 8 * CS, CS, pn3 + i, fresh);
+        sec_stage<UPPER>(dbuf + 12 * CS, CS, pS + i, fresh);
+        if (xt) {  // in-tile neighbours read their owner's streams instead
+          const long long bn = bb + i + dbn, cn = cb + i + dcn;
+#pragma unroll
+          for (int m = 0; m < NV; m++) sec_stage<UPPER>(xbuf + m * 4 * XS, XS, A.U + m * tb + bn, fresh);
+          sec_stage<UPPER>(xbuf + NV * 4 * XS, XS, A.Lc + d * tc + cn, fresh);
+          sec_stage<UPPER>(xbuf + (NV + 1) * 4 * XS, XS, A.Lv + d * tc + cn, fresh);
+        }
+      }
+      cpa_commit();
+    };
+    auto issue_own = [&](int u) {
+      if (on_at(u)) {
+        const bool fresh = !on_at(u - 1);
+        const int i = i_of(u);
+        const long long bi = bb + i, ci = cb + i;
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          sec_stage<UPPER>(obuf(SM::SU + m, c), CS, A.U + m * tb + bi, fresh);
+          sec_stage<UPPER>(obuf(SM::SR + m, c), CS, Rp(m, ci), fresh);
+        }
+        sec_stage<UPPER>(obuf(SM::SVOL, c), CS, A.vold + ci, fresh);
+        sec_stage<UPPER>(obuf(SM::SDT, c), CS, A.dt + ci, fresh);
+#pragma unroll
+        for (int q2 = 0; q2 < 3; q2++) {
+          sec_stage<UPPER>(obuf(SM::SLC + q2, c), CS, A.Lc + q2 * tc + ci, fresh);
+          sec_stage<UPPER>(obuf(SM::SLV + q2, c), CS, A.Lv + q2 * tc + ci, fresh);
+        }
+      }
+      cpa_commit();
+    };
+
+    // direction thread state for the current step (as version 3)
+    using DFT = T;
+    DFT un1 = 0, F1[NV], n1 = 0, n2 = 0, n3 = 0, Unb[NV];
+    double S = 0.0, wLc = 0.0, Lvn = 0.0;
+    bool has = false;
+    // comput_DFn's U terms (sub_LU_SGS.f90:135-157) of step t: face data from this thread's
+    // streams; the neighbour's old state from the edge streams (cross-tile) or from its owner's
+    // streams (in tile: the neighbour is the owner column pubcol's cell of step t-1, complete
+    // since that owner's wait in step t-1, ordered before this read by barrier B2 of step t-1)
+    auto prep_dir = [&](int t) {
+      has = need_dir(t);
+      if (!has) return;
+      const int i = i_of(t);
+      n1 = (DFT)sec_get(dbuf, CS, pn1 + i);
+      n2 = (DFT)sec_get(dbuf + 4 * CS, CS, pn2 + i);
+      n3 = (DFT)sec_get(dbuf + 8 * CS, CS, pn3 + i);
+      S = (double)sec_get(dbuf + 12 * CS, CS, pS + i);
+      const long long bn = bb + i + dbn, cn = cb + i + dcn;
+      if (xt) {
+        Lvn = (double)sec_get(xbuf + (NV + 1) * 4 * XS, XS, A.Lv + d * tc + cn);
+        wLc = w * (double)sec_get(xbuf + NV * 4 * XS, XS, A.Lc + d * tc + cn);
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          const double u = sec_get(xbuf + m * 4 * XS, XS, A.U + m * tb + bn);
+          Unb[m] = (DFT)(m >= 5 ? clamp0(u) : u);
+        }
+      } else {
+        Lvn = (double)sec_get(obuf(SM::SLV + d, pubcol), CS, A.Lv + d * tc + cn);
+        wLc = w * (double)sec_get(obuf(SM::SLC + d, pubcol), CS, A.Lc + d * tc + cn);
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          const double u = sec_get(obuf(SM::SU + m, pubcol), CS, A.U + m * tb + bn);
+          Unb[m] = (DFT)(m >= 5 ? clamp0(u) : u);
+        }
+      }
+      const DFT g1 = (DFT)(gamma - 1.0), half = (DFT)0.5;
+      un1 = (Unb[1] * n1 + Unb[2] * n2 + Unb[3] * n3) / Unb[0];
+      const DFT p1 = g1 * (Unb[4] - half * (sq(Unb[1]) + sq(Unb[2]) + sq(Unb[3])) / Unb[0]);
+      F1[0] = Unb[0] * un1;
+      F1[1] = Unb[1] * un1 + p1 * n1;
+      F1[2] = Unb[2] * un1 + p1 * n2;
+      F1[3] = Unb[3] * un1 + p1 * n3;
+      F1[4] = (Unb[4] + p1) * un1;
+#pragma unroll
+      for (int m = 5; m < NV; m++) F1[m] = Unb[m] * un1;
+    };
+    // the diagonal of step t's cell (sub_LU_SGS.f90:50-62, 90-92), as version 3
+    auto diag_own = [&](int t) {
+      const long long ci = cb + i_of(t);
+      const double vol = sec_get(obuf(SM::SVOL, c), CS, A.vold + ci);
+      const double dt = (double)sec_get(obuf(SM::SDT, c), CS, A.dt + ci);
+      const double lc0 = (double)sec_get(obuf(SM::SLC, c), CS, A.Lc + ci);
+      const double lc1 = (double)sec_get(obuf(SM::SLC + 1, c), CS, A.Lc + tc + ci);
+      const double lc2 = (double)sec_get(obuf(SM::SLC + 2, c), CS, A.Lc + 2 * tc + ci);
+      const double a0 = vol / dt + w * (lc0 + lc1 + lc2);
+      double al = a0, als = a0;
+      if (visc) {
+        const double lv0 = (double)sec_get(obuf(SM::SLV, c), CS, A.Lv + ci);
+        const double lv1 = (double)sec_get(obuf(SM::SLV + 1, c), CS, A.Lv + tc + ci);
+        const double lv2 = (double)sec_get(obuf(SM::SLV + 2, c), CS, A.Lv + 2 * tc + ci);
+        const double lv = lv0 + lv1 + lv2;
+        al = al + 2.0 * lv;
+        als = als + 2.0 * lv;
+        if (NV == 6) {  // lower: + (Lv sum); upper: + Lv1 + Lv2 + Lv3 term by term (sub_LU_SGS.f90:60-62, 90-92)
+          if (!UPPER) als = als + lv;
+          else als = als + lv0 + lv1 + lv2;
+        }
+      }
+      if (dual) {  // dual time: + Sfac1 vol (sub_LU_SGS.f90:39, 92)
+        al = al + sfac1 * vol;
+        als = als + sfac1 * vol;
+      }
+      s_diag[0][c] = al;
+      s_diag[1][c] = NV == 6 ? als : al;
+    };
+
+    int seen_j = 0, seen_k = 0;
+    auto poll = [&](int t) {  // upstream tiles far enough for step t
+      bool ok = true;
+      if (pj >= 0 && seen_j < min(t + TJ, nsteps)) ok &= wait_ge(L.progress + pj, min(t + TJ, nsteps), L.spin_limit, seen_j);
+      if (pk >= 0 && seen_k < min(t + TK, nsteps)) ok &= wait_ge(L.progress + pk, min(t + TK, nsteps), L.spin_limit, seen_k);
+      if (!ok) atomicExch(L.err, 1);
+    };
+
+    auto diag_of = [&](int m) { return (NV == 6 && m == 5) ? s_diag[1][c] : s_diag[0][c]; };
+    auto finish = [&](int m, long long ci) {  // sub_LU_SGS.f90:63-72 (lower), 108-117 (upper)
+      const double rm = (double)sec_get(obuf(SM::SR + m, c), CS, Rp(m, ci));
+      double r;
+      if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      A.DU[m * tc + ci] = r;
+      s_pub[m][c] = r;
+    };
+    if (grp == 4) {
+      // poller warp: the upstream tiles' progress for step t+2 during step t (before B1 of step
+      // t+1), so the cross-tile DU of step t+2 can be loaded at the end of step t+1
+      if (tid == 4 * TC) { poll(0); if (1 < nsteps) poll(1); }
+      cta_bar<NT>();  // B0
+      for (int t = 0; t < nsteps; t++) {
+        cta_bar<NT>();  // B1
+        if (tid == 4 * TC && t + 2 < nsteps) poll(t + 2);
+      }
+    } else if (grp == 5) {
+      // publisher warp: after B1 of step t every DU of the steps before t is stored (the barrier
+      // orders the compute threads' stores before this release)
+      cta_bar<NT>();  // B0
+      for (int t = 0; t < nsteps; t++) {
+        cta_bar<NT>();  // B1
+        if (tid == 4 * TC + 32 && t > 0) st_release(L.progress + my, t);
+      }
+    } else if (owner) {
+#pragma unroll
+      for (int u = 0; u < LU4_D; u++) issue_own(u);
+      cta_bar<NT>();  // B0
+      for (int t = 0; t < nsteps; t++) {
+        cta_bar<NT>();  // B1
+        cpa_wait<LU4_D - 1>();  // step t's sectors (only the groups of steps t+1.. may be outstanding)
+        if (on_at(t)) diag_own(t);
+        issue_own(t + LU4_D);
+        cta_bar_id<2, NC>();  // B2: the three direction terms of step t are in shared memory
+        if (on_at(t)) {
+          const long long ci = cb + i_of(t);
+#pragma unroll
+          for (int m = 3; m < NV; m++) finish(m, ci);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < LU4_D; u++) issue_dir(u);
+      cpa_wait<LU4_D - 1>();
+      prep_dir(0);
+      double xdu[NV];  // cross-tile neighbour's DU of the current step, loaded one step early
+      auto load_xdu = [&](int t) {
+        const long long cn = cb + i_of(t) + dcn;
+#pragma unroll
+        for (int m = 0; m < NV; m++) xdu[m] = __ldcg(A.DU + m * tc + cn);
+      };
+      cta_bar<NT>();  // B0: the poller's first waits are done
+      if (xt && has) load_xdu(0);
+      for (int t = 0; t < nsteps; t++) {
+        cta_bar<NT>();  // B1: step t-1 finished (DU in s_pub and in HBM), upstream tiles ready
+        issue_dir(t + LU4_D);
+        if (has) {
+          double DUn[NV];
+          if (!xt) {
+#pragma unroll
+            for (int m = 0; m < NV; m++) DUn[m] = s_pub[m][pubcol];
+          } else {
+#pragma unroll
+            for (int m = 0; m < NV; m++) DUn[m] = xdu[m];
+          }
+          DFT U2[NV];
+#pragma unroll
+          for (int m = 0; m < NV; m++) U2[m] = (DFT)((double)Unb[m] + DUn[m]);
+          const DFT g1 = (DFT)(gamma - 1.0), half = (DFT)0.5;
+          const DFT un2 = (U2[1] * n1 + U2[2] * n2 + U2[3] * n3) / U2[0];
+          const DFT pp2 = g1 * (U2[4] - half * (sq(U2[1]) + sq(U2[2]) + sq(U2[3])) / U2[0]);
+          DFT DF[NV];
+          DF[0] = U2[0] * un2 - F1[0];
+          DF[1] = (U2[1] * un2 + pp2 * n1) - F1[1];
+          DF[2] = (U2[2] * un2 + pp2 * n2) - F1[2];
+          DF[3] = (U2[3] * un2 + pp2 * n3) - F1[3];
+          DF[4] = (U2[4] + pp2) * un2 - F1[4];
+#pragma unroll
+          for (int m = 5; m < NV; m++) DF[m] = U2[m] * un2 - F1[m];
+#pragma unroll
+          for (int m = 0; m < NV; m++) {
+            double v;
+            if (!UPPER) v = 0.5 * ((double)DF[m] * S + wLc * DUn[m]);
+            else v = -(0.5 * ((double)DF[m] * S - wLc * DUn[m]));
+            if (visc) v = v + Lvn * DUn[m];
+            s_acc[d][m][c] = v;
+          }
+        } else if (on_at(t)) {
+#pragma unroll
+          for (int m = 0; m < NV; m++) s_acc[d][m][c] = 0.0;
+        }
+        cta_bar_id<2, NC>();  // B2
+        if (on_at(t)) finish(d, cb + i_of(t));
+        cpa_wait<LU4_D - 1>();  // step t+1's sectors
+        prep_dir(t + 1);
+        if (xt && has) load_xdu(t + 1);  // ready since the poller's wait of step t-1
+      }
+    }
+    cpa_wait<0>();  // no copy of this tile is still landing when the next tile reuses the slots
+    __syncthreads();
+    if (tid == 0) st_release(L.progress + my, nsteps);
+  }
+}
+
+template <class T, int NV, bool UPPER, int TC>
+inline size_t lu_wave4_smem() { return (size_t)Lu4Smem<NV, TC>::BYTES; }
+template <class T, int NV, bool UPPER, int TC>
+inline void lu_wave4_prepare() {
+  cudaFuncSetAttribute(k_lusgs_wave4<T, NV, UPPER, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_wave4_smem<T, NV, UPPER, TC>());
+}
+
 }  // namespace ocfd

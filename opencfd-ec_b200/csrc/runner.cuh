@@ -38,6 +38,10 @@ class RunnerT : public Runner {
     lu_wave3_prepare<T, NV, true, 32>();
     lu_wave3_prepare<T, NV, false, 64>();
     lu_wave3_prepare<T, NV, true, 64>();
+    lu_wave4_prepare<T, NV, false, 32>();
+    lu_wave4_prepare<T, NV, true, 32>();
+    lu_wave4_prepare<T, NV, false, 64>();
+    lu_wave4_prepare<T, NV, true, 64>();
   }
 
   void residual(cudaStream_t st, bool lusgs) override {
@@ -110,6 +114,12 @@ class RunnerT : public Runner {
       if (I_.lu_version == 2) {
         if (!upper) k_lusgs_wave<T, NV, false><<<I_.lu_grid, 64, 0, st>>>(A, L_);
         else k_lusgs_wave<T, NV, true><<<I_.lu_grid, 64, 0, st>>>(A, L_);
+      } else if (I_.lu_version == 4 && I_.lu_tc == 64) {
+        if (!upper) k_lusgs_wave4<T, NV, false, 64><<<I_.lu_grid, 4 * 64 + 64, lu_wave4_smem<T, NV, false, 64>(), st>>>(A, L_);
+        else k_lusgs_wave4<T, NV, true, 64><<<I_.lu_grid, 4 * 64 + 64, lu_wave4_smem<T, NV, true, 64>(), st>>>(A, L_);
+      } else if (I_.lu_version == 4) {
+        if (!upper) k_lusgs_wave4<T, NV, false, 32><<<I_.lu_grid, 4 * 32 + 64, lu_wave4_smem<T, NV, false, 32>(), st>>>(A, L_);
+        else k_lusgs_wave4<T, NV, true, 32><<<I_.lu_grid, 4 * 32 + 64, lu_wave4_smem<T, NV, true, 32>(), st>>>(A, L_);
       } else if (I_.lu_tc == 64) {
         if (!upper) k_lusgs_wave3<T, NV, false, 64><<<I_.lu_grid, 4 * 64 + 32, lu_wave3_smem<T, NV, false, 64>(), st>>>(A, L_);
         else k_lusgs_wave3<T, NV, true, 64><<<I_.lu_grid, 4 * 64 + 32, lu_wave3_smem<T, NV, true, 64>(), st>>>(A, L_);

@@ -17,7 +17,7 @@ struct RunInfo {
   int lu_planes;          // 1: one launch per hyperplane (reference order); 0: pipelined wavefront
   const LuArgs* lu;       // wavefront tables (host copy of the kernel argument)
   int lu_grid;            // CTAs of the wavefront kernel
-  int lu_version;         // 2: one thread per column; 3: four thread groups per column
+  int lu_version;         // 2: one thread per column; 3: four thread groups per column, staged by element; 4: staged by sector
   int lu_tc;              // columns per tile (32 or 64)
   int recon_prim;         // 1: every solve reconstructs primitive variables
   const int* bc_rounds;   // per boundary round: first entry, end entry, cells

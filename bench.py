@@ -365,7 +365,9 @@ def main():
     bmodel = BYTES[(prec, s.nvar)]
     single = [k for k in ("lusgs_lower", "lusgs_upper") if ph[k] > 0.0]
     dom = max(single, key=lambda k: ph[k]) if single else "residual"
-    kernel_name = {"lusgs_lower": "k_lusgs_wave<lower>", "lusgs_upper": "k_lusgs_wave<upper>",
+    luv, lutc = s.lu_kernel_version(), s.lu_tile_width()
+    kernel_name = {"lusgs_lower": "k_lusgs_wave%d<lower, %d columns>" % (luv, lutc),
+                   "lusgs_upper": "k_lusgs_wave%d<upper, %d columns>" % (luv, lutc),
                    "residual": "residual phase (all flux/source kernels)"}[dom]
     t_dom = ph[dom] / 3.0 * 1e-3
     achieved = bmodel[dom] * ncell / t_dom / 1e9

@@ -150,7 +150,8 @@ def aggregate_rate(world, units_per_rank, ms):
 def cpu_sample(args, min_seconds=10.0, max_steps=50):
     """Times the CPU oracle (restatement of the reference algorithm, all host threads) on the same
     workload: full mesh, one warm-up step, then steps until min_seconds of CPU work (at most
-    max_steps).  Returns (cell-updates/s, threads, description)."""
+    max_steps), and one more step on a single host thread.  Returns (cell-updates/s, threads,
+    description, the single-thread sample or None)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
     p, case = make_case(args, 0)
@@ -163,9 +164,19 @@ def cpu_sample(args, min_seconds=10.0, max_steps=50):
         el = time.time() - t0
         if el >= min_seconds or n >= max_steps:
             break
+    threads = oracle_py.threads()
+    # one more step of the same (warm) case on a single host thread
+    single = None
+    if threads > 1:
+        oracle_py.set_threads(1)
+        t1 = time.time()
+        o.advance(1)
+        e1 = time.time() - t1
+        oracle_py.set_threads(threads)
+        single = {"value": case.ncells / e1, "unit": "cell-updates/s", "cores": 1,
+                  "sample": "%s, 1 LU-SGS step on 1 host thread after the %d above, %.1f s" % (case.name, n + 1, e1)}
     o.close()
-    threads = int(os.environ.get("OCFD_ORACLE_THREADS", os.cpu_count() or 1))
-    return case.ncells * n / el, threads, "%s, %d LU-SGS step(s) after 1 warm-up, %.1f s on %d host threads" % (case.name, n, el, threads)
+    return case.ncells * n / el, threads, "%s, %d LU-SGS step(s) after 1 warm-up, %.1f s on %d host threads" % (case.name, n, el, threads), single
 
 
 def event_ms(s, nsteps):
@@ -281,7 +292,7 @@ def run_reference(args, budget_s=150.0):
             break
     el = time.time() - t0
     o.close()
-    threads = int(os.environ.get("OCFD_ORACLE_THREADS", os.cpu_count() or 1))
+    threads = oracle_py.threads()
     v = case.ncells * n / el
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": 1, "steps": args.steps,
@@ -423,8 +434,10 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            v, cores, desc = cpu_sample(args)
+            v, cores, desc, single = cpu_sample(args)
             cpu = {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port", "sample": desc}
+            if single:
+                cpu["single_thread"] = single
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "port", "sample": "failed: %s" % e}
 

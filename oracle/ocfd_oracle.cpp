@@ -2335,6 +2335,14 @@ using namespace orc;
 
 extern "C" {
 
+// host threads of the oracle's loop pool (OCFD_ORACLE_THREADS or all hardware threads at load);
+// returns the count in use
+int oracle_set_threads(int n) {
+  orc::Pool::get().set_threads(n);
+  return orc::Pool::get().size();
+}
+int oracle_threads() { return orc::Pool::get().size(); }
+
 int oracle_create(const ocfd_params* p, int nblk, const int* nijk, const double* const* xyz, const int* nsub, const int* inc,
                   const double* const* dw, void** out) {
   if (!p || nblk <= 0 || !nijk || !xyz || !nsub || !inc || !out) return OCFD_ERR_ARG;

@@ -32,6 +32,7 @@ def lib():
         vp, ip, dp, cp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.c_char_p
         L.oracle_create.argtypes = [vp, ctypes.c_int, ip, ctypes.POINTER(dp), ip, ip, ctypes.POINTER(dp), ctypes.POINTER(vp)]
         L.oracle_destroy.argtypes = [vp]
+        L.oracle_set_threads.argtypes = [ctypes.c_int]
         L.oracle_last_error.argtypes = [vp]
         L.oracle_last_error.restype = cp
         L.oracle_advance.argtypes = [vp, ctypes.c_int, ip, dp]
@@ -144,6 +145,15 @@ class OracleCase:
         out = np.empty(shape)
         self._check(lib().oracle_get_array(self.h, b, name.encode(), _dp(out)), "get_array " + name)
         return out, tuple(lo), tuple(hi)
+
+
+def set_threads(n):
+    """Host threads of the oracle's loop pool; returns the count in use."""
+    return int(lib().oracle_set_threads(int(n)))
+
+
+def threads():
+    return int(lib().oracle_threads())
 
 
 def flux_1d(QL, QR, gamma, iflux):

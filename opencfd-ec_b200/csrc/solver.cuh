@@ -1497,17 +1497,21 @@ __global__ void k_norms(Arena<T> A, double* part, unsigned long long* nan_at) {
   double mx[NV], sm[NV];
 #pragma unroll
   for (int m = 0; m < NV; m++) { mx[m] = 0.0; sm[m] = 0.0; }
+  // the first NaN position of this thread's cells, published by one atomic after the loop (an
+  // atomic inside it would order every later load behind the NaN test of the previous value)
+  unsigned long long nan_first = ~0ULL;
 #pragma unroll 4
   for (int l = threadIdx.x; l < ch.z; l += blockDim.x) {  // unrolled: loads of 4 cells in flight, sums in order
     long long g = B.ocell + ch.y + l;
 #pragma unroll
     for (int m = 0; m < NV; m++) {
-      double r = (double)A.Res[m * tc + g];
-      if (isnan(r)) atomicMin(nan_at, (unsigned long long)(g * 8 + m));
+      double r = (double)__ldg(A.Res + m * tc + g);
+      if (isnan(r)) nan_first = min(nan_first, (unsigned long long)(g * 8 + m));
       mx[m] = fmax(mx[m], fabs(r));
       sm[m] = sm[m] + r * r;
     }
   }
+  if (nan_first != ~0ULL) atomicMin(nan_at, nan_first);
 #pragma unroll
   for (int m = 0; m < NV; m++) { smax[m][threadIdx.x] = mx[m]; ssum[m][threadIdx.x] = sm[m]; }
   __syncthreads();

@@ -70,17 +70,21 @@ def test_nan_reported_with_location(gpu):
     g.close()
 
 
-def test_lusgs_wait_bound_reports_timeout(gpu, oracle):
+@pytest.mark.parametrize("version", ["OCFD_LU_V3", "OCFD_LU_V4"])
+def test_lusgs_wait_bound_reports_timeout(gpu, oracle, version):
     """With the LU-SGS wait bound at zero every cross-tile wait that is not already satisfied gives
     up at once: the sweep finishes, the step reports OCFD_ERR_TIMEOUT, and a new handle on the
-    same context runs correctly."""
+    same context runs correctly (each wavefront kernel version)."""
     from ocfd_b200 import cases
     p, case = cases.config2_small()
     os.environ["OCFD_LU_SPIN_LIMIT"] = "0"
+    os.environ[version] = "1"
     try:
         g = gpu.Solver(p, case)
     finally:
         os.environ.pop("OCFD_LU_SPIN_LIMIT", None)
+        os.environ.pop(version, None)
+    assert g.lu_kernel_version() == int(version[-1])
     seen = False
     for _ in range(3):
         g.advance(1)

@@ -752,6 +752,9 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
     dec_cell(B, g - B.ocell, i, j, k);
     long long f = fix_(B, i, j, k), fi1 = fix_(B, i + 1, j, k), fj1 = fix_(B, i, j + 1, k), fk1 = fix_(B, i, j, k + 1);
     bool visc = s.viscous == 1 && A.flags[b] != 1;
+    // all loads and arithmetic first, the stores (Res, Lc, Lv, dt) at the end: a store inside the
+    // loop would keep every later load (the planes may alias for the compiler) behind it
+    T Rm[5];
 #pragma unroll
     for (int m = 0; m < 5; m++) {
       const T* F0 = A.Fi + (0 * 5 + m) * tf;
@@ -768,7 +771,7 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
         R = R + V1[fj1] - V1[f];
         R = R + V2[fk1] - V2[f];
       }
-      A.Res[m * tc + g] = R;
+      Rm[m] = R;
     }
     long long c = bix(B, i, j, k);
     T D0 = T(0);
@@ -791,8 +794,6 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
       T S0 = (Sd[f] + Sd[fo]) * T(0.5);
       L[d] = (dabs(un) + cc) * S0;
       L[3 + d] = D0 * S0 * S0 * vol1;
-      A.Lc[d * tc + g] = L[d];
-      A.Lv[d * tc + g] = L[3 + d];
     }
     T dtv;
     if (s.local_dt == 1) {
@@ -804,6 +805,10 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
     } else {
       dtv = T(s.dt_global);
     }
+#pragma unroll
+    for (int m = 0; m < 5; m++) A.Res[m * tc + g] = Rm[m];
+#pragma unroll
+    for (int d = 0; d < 3; d++) { A.Lc[d * tc + g] = L[d]; A.Lv[d * tc + g] = L[3 + d]; }
     A.dt[g] = dtv;
   }
 }
@@ -996,6 +1001,8 @@ __global__ void k_update(Arena<T> A) {
     int i, j, k;
     dec_cell(B, g - B.ocell, i, j, k);
     long long c = bix(B, i, j, k);
+    // every variable's new value first, then the stores: a store of U inside the loop would keep
+    // the next variable's loads (U and DU may alias for the compiler) behind it
     double Un[NV];
 #pragma unroll
     for (int m = 0; m < NV; m++) {
@@ -1018,9 +1025,10 @@ __global__ void k_update(Arena<T> A) {
         if (m >= 5) cur = clamp0(cur);
         u = Ra * A.Un[m * tb + c] + Rg * cur + (double)A.dt[g] * Rb * du;
       }
-      A.U[m * tb + c] = u;
       Un[m] = u;
     }
+#pragma unroll
+    for (int m = 0; m < NV; m++) A.U[m * tb + c] = Un[m];
     if (s.limit_flow == 1) {
       double d1 = Un[0], u1 = Un[1] / d1, v1 = Un[2] / d1, w1 = Un[3] / d1;
       double p1 = (Un[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1)) * (s.gamma - 1.0);

@@ -128,9 +128,9 @@ __global__ void k_sa_pre(Arena<T> A) {
     if (i < 0 || i > B.nx || j < 0 || j > B.ny || k < 0 || k > B.nz) continue;
     const SolveP& s = A.sp[B.solve];
     T mu = T((double)A.mu[g] * s.re);
-    A.mu[g] = mu;
     T vt = T(clamp0(A.U[5 * tb + g]));
     T d = A.P[P_D * tb + g];
+    A.mu[g] = mu;  // after the loads: a store before them would hold them back
     T X = d * vt / mu;
     T fv1 = cube(X) / (cube(X) + T(sa::Cv1_3));
     T mut = fv1 * d * vt;
@@ -1377,8 +1377,11 @@ __global__ void k_halo(Arena<T> A) {
     int s = find_blk(A.pre_halo, A.nsub, g);
     long long cs, ct;
     halo_map(A, A.sub[s], g - A.pre_halo[s], cs, ct);
+    double v[NV];  // all loads before the stores (a store in between would hold the next load back)
 #pragma unroll
-    for (int m = 0; m < NV; m++) A.U[m * tb + ct] = A.U[m * tb + cs];
+    for (int m = 0; m < NV; m++) v[m] = A.U[m * tb + cs];
+#pragma unroll
+    for (int m = 0; m < NV; m++) A.U[m * tb + ct] = v[m];
   }
 }
 
@@ -1393,10 +1396,13 @@ __global__ void k_halo_level(Arena<T> A, const int* ent, const long long* pre, i
     int e = e0 + find_blk(pre + e0, e1 - e0, g);
     long long cs, ct;
     halo_map(A, A.sub[ent[e]], g - pre[e], cs, ct);
+    double v[NV];  // all loads before the stores
+#pragma unroll
+    for (int m = 0; m < NV; m++) v[m] = PHASE == 0 ? A.U[m * tb + cs] : stage[m * cells + g];
 #pragma unroll
     for (int m = 0; m < NV; m++) {
-      if (PHASE == 0) stage[m * cells + g] = A.U[m * tb + cs];
-      else A.U[m * tb + ct] = stage[m * cells + g];
+      if (PHASE == 0) stage[m * cells + g] = v[m];
+      else A.U[m * tb + ct] = v[m];
     }
   }
 }
@@ -1416,8 +1422,11 @@ __global__ void k_halo_pack(Arena<T> A, const int* ent, const long long* pre, in
     int src[3], dst[3];
     halo_idx(S, g - pre[e], src, dst);
     const long long cs = bix(A.blk[S.blk], src[0], src[1], src[2]);
+    double v[NV];  // all loads before the stores
 #pragma unroll
-    for (int m = 0; m < NV; m++) buf[g * NV + m] = A.U[m * tb + cs];
+    for (int m = 0; m < NV; m++) v[m] = A.U[m * tb + cs];
+#pragma unroll
+    for (int m = 0; m < NV; m++) buf[g * NV + m] = v[m];
   }
 }
 template <class T, int NV>
@@ -1429,8 +1438,11 @@ __global__ void k_halo_unpack(Arena<T> A, const SubD* sub, const long long* pre,
     int src[3], dst[3];
     halo_idx(S, g - pre[e], src, dst);
     const long long ct = bix(A.blk[S.nb1], dst[0], dst[1], dst[2]);
+    double v[NV];  // all loads before the stores
 #pragma unroll
-    for (int m = 0; m < NV; m++) A.U[m * tb + ct] = buf[g * NV + m];
+    for (int m = 0; m < NV; m++) v[m] = buf[g * NV + m];
+#pragma unroll
+    for (int m = 0; m < NV; m++) A.U[m * tb + ct] = v[m];
   }
 }
 

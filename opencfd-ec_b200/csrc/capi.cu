@@ -473,6 +473,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     B.obox = h->pre_box[b]; B.oface = h->pre_face[b]; B.ocell = h->pre_cell[b]; B.ocol = h->pre_col[b]; B.onode = onode;
     B.obci = obci; B.obcj = obcj; B.obck = obck;
     long long box = (long long)B.NX * B.NY * B.NZ;
+    if (box >= (1LL << 31)) return OCFD_ERR_ARG;  // the kernels decode block-local indices in 32 bits
     h->max_box_b = std::max(h->max_box_b, box);
     h->pre_box[b + 1] = h->pre_box[b] + box;
     h->pre_face[b + 1] = h->pre_face[b] + (long long)B.nx * B.ny * B.nz;

@@ -48,16 +48,22 @@ __device__ __forceinline__ long long nix(const BlkD& B, int i, int j, int k) {
 __device__ __forceinline__ double clamp0(double v) { return v < 0.0 ? 0.0 : v; }
 template <class T> __device__ __forceinline__ T ld(const T* p, long long i) { return p[i]; }
 
-// decode helpers: global index -> block + (i,j,k)
+// decode helpers: index within a block -> (i,j,k).  A block's ghost box holds fewer than 2^31
+// cells (ocfd_create checks it), so the decode divides in 32 bits instead of 64.
 __device__ __forceinline__ void dec_cell(const BlkD& B, long long l, int& i, int& j, int& k) {
-  int nxm = B.nx - 1, nym = B.ny - 1;
-  i = (int)(l % nxm) + 1; long long t = l / nxm; j = (int)(t % nym) + 1; k = (int)(t / nym) + 1;
+  const unsigned u = (unsigned)l, nxm = (unsigned)(B.nx - 1), nym = (unsigned)(B.ny - 1);
+  const unsigned t = u / nxm;
+  i = (int)(u - t * nxm) + 1; j = (int)(t % nym) + 1; k = (int)(t / nym) + 1;
 }
 __device__ __forceinline__ void dec_face(const BlkD& B, long long l, int& i, int& j, int& k) {
-  i = (int)(l % B.nx) + 1; long long t = l / B.nx; j = (int)(t % B.ny) + 1; k = (int)(t / B.ny) + 1;
+  const unsigned u = (unsigned)l, nx = (unsigned)B.nx, ny = (unsigned)B.ny;
+  const unsigned t = u / nx;
+  i = (int)(u - t * nx) + 1; j = (int)(t % ny) + 1; k = (int)(t / ny) + 1;
 }
 __device__ __forceinline__ void dec_box(const BlkD& B, long long l, int& i, int& j, int& k) {
-  i = (int)(l % B.NX) - 3; long long t = l / B.NX; j = (int)(t % B.NY) - 3; k = (int)(t / B.NY) - 3;
+  const unsigned u = (unsigned)l, NX = (unsigned)B.NX, NY = (unsigned)B.NY;
+  const unsigned t = u / NX;
+  i = (int)(u - t * NX) - 3; j = (int)(t % NY) - 3; k = (int)(t / NY) - 3;
 }
 
 // ============================================================================================
@@ -448,9 +454,10 @@ __global__ void k_mu_finish(Arena<T> A) {
 // decode a face cell of a subface (transverse ranges b..e-1)
 __device__ __forceinline__ void subcell_ijk(const SubD& S, long long l, int& i, int& j, int& k) {
   int f = S.face;
-  if (f == 1 || f == 4) { int nj = S.je - S.jb; j = S.jb + (int)(l % nj); k = S.kb + (int)(l / nj); i = f == 1 ? 1 : S.ie - 1; }
-  else if (f == 2 || f == 5) { int ni = S.ie - S.ib; i = S.ib + (int)(l % ni); k = S.kb + (int)(l / ni); j = f == 2 ? 1 : S.je - 1; }
-  else { int ni = S.ie - S.ib; i = S.ib + (int)(l % ni); j = S.jb + (int)(l / ni); k = f == 3 ? 1 : S.ke - 1; }
+  const unsigned u = (unsigned)l;  // a subface's cell count is below 2^31
+  if (f == 1 || f == 4) { unsigned nj = (unsigned)(S.je - S.jb); j = S.jb + (int)(u % nj); k = S.kb + (int)(u / nj); i = f == 1 ? 1 : S.ie - 1; }
+  else if (f == 2 || f == 5) { unsigned ni = (unsigned)(S.ie - S.ib); i = S.ib + (int)(u % ni); k = S.kb + (int)(u / ni); j = f == 2 ? 1 : S.je - 1; }
+  else { unsigned ni = (unsigned)(S.ie - S.ib); i = S.ib + (int)(u % ni); j = S.jb + (int)(u / ni); k = f == 3 ? 1 : S.ke - 1; }
 }
 __device__ __forceinline__ void ghost_of(const SubD& S, int i, int j, int k, int& gi, int& gj, int& gk) {
   gi = i; gj = j; gk = k;
@@ -618,8 +625,8 @@ __global__ void k_inv_kbc(Arena<T> A) {
     const BlkD& B = A.blk[S.blk];
     const SolveP& sp = A.sp[B.solve];
     long long l = g - A.pre_subcell[s];
-    int ni = S.ie - S.ib;
-    int i = S.ib + (int)(l % ni), j = S.jb + (int)(l / ni), k = S.kb;
+    const unsigned ni = (unsigned)(S.ie - S.ib), u = (unsigned)l;
+    int i = S.ib + (int)(u % ni), j = S.jb + (int)(u / ni), k = S.kb;
     long long c0 = bix(B, i, j, k), c1 = bix(B, i, j, k - 1);
     T gm = T(sp.gamma);
     T d0 = (A.P[P_D * tb + c0] + A.P[P_D * tb + c1]) * T(0.5), uu0 = (A.P[P_U * tb + c0] + A.P[P_U * tb + c1]) * T(0.5);
@@ -913,7 +920,8 @@ __global__ void k_lusgs(Arena<T> A, int plane) {
     int b = find_blk(A.pre_col, A.nblk, g);
     const BlkD& B = A.blk[b];
     long long l = g - B.ocol;
-    int j = (int)(l % (B.ny - 1)) + 1, k = (int)(l / (B.ny - 1)) + 1;
+    const unsigned nym = (unsigned)(B.ny - 1), u = (unsigned)l;
+    int j = (int)(u % nym) + 1, k = (int)(u / nym) + 1;
     int i = plane - k - j;
     if (i < 1 || i > B.nx - 1) continue;
     const SolveP& s = A.sp[B.solve];
@@ -1254,8 +1262,8 @@ __device__ __forceinline__ void bc_cell(Arena<T>& A, const SubD& S, const BlkD& 
     wall_bound_d<NV>(s, U, tb, c1, bix(B, gi, gj, gk), (double)A.mu[c1], dwv);
   } else if (S.bc == 4 || S.bc == 5 || S.bc == 6 || S.bc == 401) {  // far field / inflow / outflow / extrapolate (152-283, 458-504)
     const int Flag = S.bc == 5 ? 2 : (S.bc == 6 ? 1 : 0);
-    int ni = S.ie - S.ib + 1, nj = S.je - S.jb + 1;
-    int i = S.ib + (int)(l % ni), j = S.jb + (int)((l / ni) % nj), k = S.kb + (int)(l / ((long long)ni * nj));
+    const unsigned ni = (unsigned)(S.ie - S.ib + 1), nj = (unsigned)(S.je - S.jb + 1), u = (unsigned)l, t = u / ni;
+    int i = S.ib + (int)(u - t * ni), j = S.jb + (int)(t % nj), k = S.kb + (int)(t / nj);
     int i1 = i, j1 = j, k1 = k, i2 = i, j2 = j, k2 = k;
     double n1, n2, n3, sg = (f <= 3) ? -1.0 : 1.0;
     if (f == 1) i2 = i - 1; else if (f == 2) j2 = j - 1; else if (f == 3) k2 = k - 1;
@@ -1350,8 +1358,9 @@ __device__ __forceinline__ void halo_idx(const SubD& S, long long l, int* src, i
   int d1 = (S.face1 - 1) % 3;
   if (S.face1 <= 3) kb1[d1] = kb1[d1] - LAP;
   ke1[d1] = kb1[d1] + LAP - 1;
-  int n0 = ke1[0] - kb1[0] + 1, n1 = ke1[1] - kb1[1] + 1;
-  int ka[3] = {(int)(l % n0), (int)((l / n0) % n1), (int)(l / ((long long)n0 * n1))};
+  const unsigned n0 = (unsigned)(ke1[0] - kb1[0] + 1), n1 = (unsigned)(ke1[1] - kb1[1] + 1);
+  const unsigned u = (unsigned)l, t = u / n0;  // a copy's cell count is below 2^31
+  int ka[3] = {(int)(u - t * n0), (int)(t % n1), (int)(t / n1)};
   int L[3] = {abs(S.L1), abs(S.L2), abs(S.L3)};
   int P[3] = {S.L1 >= 0 ? 1 : -1, S.L2 >= 0 ? 1 : -1, S.L3 >= 0 ? 1 : -1};
 #pragma unroll

@@ -521,11 +521,15 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
     //     variable d, the owner the variables 3..NV-1; direction threads then prepare the next
     //     step's old-state terms, and thread 0 completes the poll of the upstream tiles.
     auto diag_of = [&](int m) { return (NV == 6 && m == 5) ? s_diag[1][c] : s_diag[0][c]; };
-    auto finish = [&](int m, int t, long long ci) {  // sub_LU_SGS.f90:63-72 (lower), 108-117 (upper)
+    auto finish_val = [&](int m, int t) {  // sub_LU_SGS.f90:63-72 (lower), 108-117 (upper)
       const double rm = (double)R.oR[t % LU_RING][m][c];
       double r;
       if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
       else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      return r;
+    };
+    auto finish = [&](int m, int t, long long ci) {
+      const double r = finish_val(m, t);
       A.DU[m * tc + ci] = r;
       s_pub[m][c] = r;
     };
@@ -555,8 +559,11 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
         cta_bar<NT>();  // B2: the three direction terms of step t are in shared memory
         if (on_at(t)) {
           const long long ci = cb + i_of(t);
+          double r[NV];  // every value before the stores, so the divisions overlap
 #pragma unroll
-          for (int m = 3; m < NV; m++) finish(m, t, ci);
+          for (int m = 3; m < NV; m++) r[m] = finish_val(m, t);
+#pragma unroll
+          for (int m = 3; m < NV; m++) { A.DU[m * tc + ci] = r[m]; s_pub[m][c] = r[m]; }
         }
       }
     } else {

@@ -268,10 +268,11 @@ __global__ void k_sst_pre(Arena<T> A) {
     dec_box(B, g - B.obox, i, j, k);
     if (i < 0 || i > B.nx || j < 0 || j > B.ny || k < 0 || k > B.nz) continue;
     const SolveP& s = A.sp[B.solve];
-    A.mu[g] = T((double)A.mu[g] * s.re);
-    double d = A.U[g];
-    A.Kt[g] = T(clamp0(A.U[5 * tb + g]) / d);
-    A.Wt[g] = T(clamp0(A.U[6 * tb + g]) / d);
+    const T mu = T((double)A.mu[g] * s.re);
+    const double d = A.U[g], u5 = A.U[5 * tb + g], u6 = A.U[6 * tb + g];  // loads before the stores
+    A.mu[g] = mu;
+    A.Kt[g] = T(clamp0(u5) / d);
+    A.Wt[g] = T(clamp0(u6) / d);
   }
 }
 
@@ -304,6 +305,7 @@ __global__ void k_sst_src(Arena<T> A) {
     T Ktz = Kti * iz + Ktj * jz + Ktk * kz, wtz = wti * iz + wtj * jz + wtk * kz;
     T omega = dsqrt(sq(wy - vz) + sq(uz - wx) + sq(vx - uy));
     T Re = T(s.re), dw = A.dw[g], K = A.Kt[c], Wv = A.Wt[c], dd = A.P[P_D * tb + c], mu = A.mu[c];
+    const T volg = A.vol[g];  // before the stores below
     const T c009 = T((double)0.09f);  // `0.09` default-real literal (SST.f90:108, 120)
     T arg2 = fmax_(T(2) * dsqrt(dabs(K)) / (c009 * Wv * dw * Re), T(500) * mu / (dd * Wv * sq(dw) * Re * Re));
     T f2 = dtanh(sq(arg2));
@@ -320,8 +322,8 @@ __global__ void k_sst_src(Arena<T> A) {
     T Cw = f1 * T(sst::Cw1) + (T(1) - f1) * T(sst::Cw2);
     T beta = f1 * T(sst::beta1) + (T(1) - f1) * T(sst::beta2);
     T Qw = Cw * dd * omega * omega / Re - Re * beta * dd * sq(Wv) + (T(1) - f1) * Kws / Re;
-    A.Res[5 * tc + g] = Qk * A.vol[g];
-    A.Res[6 * tc + g] = Qw * A.vol[g];
+    A.Res[5 * tc + g] = Qk * volg;
+    A.Res[6 * tc + g] = Qw * volg;
   }
 }
 
@@ -422,13 +424,17 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sst_res(Arena<T> A) {
     int i, j, k;
     dec_cell(B, g - B.ocell, i, j, k);
     long long f = fix_(B, i, j, k), fi1 = fix_(B, i + 1, j, k), fj1 = fix_(B, i, j + 1, k), fk1 = fix_(B, i, j, k + 1);
+    T Rq[2];  // both values before the stores
+#pragma unroll
     for (int q = 0; q < 2; q++) {
       T R = A.Res[(5 + q) * tc + g];
       R = R + A.Ft[(0 + q) * tf + fi1] - A.Ft[(0 + q) * tf + f];
       R = R + A.Ft[(2 + q) * tf + fj1] - A.Ft[(2 + q) * tf + f];
       R = R + A.Ft[(4 + q) * tf + fk1] - A.Ft[(4 + q) * tf + f];
-      A.Res[(5 + q) * tc + g] = R;
+      Rq[q] = R;
     }
+    A.Res[5 * tc + g] = Rq[0];
+    A.Res[6 * tc + g] = Rq[1];
   }
 }
 

@@ -875,6 +875,12 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   }
   h->info.recon_prim = 1;
   for (int q = 0; q < nsolve; q++) if (ps[q].iflag_reconstruction != 0) h->info.recon_prim = 0;
+  h->info.int_scheme = ps[0].iflag_scheme;
+  h->info.int_flux = ps[0].iflag_flux;
+  for (int q = 1; q < nsolve; q++) {
+    if (ps[q].iflag_scheme != h->info.int_scheme) h->info.int_scheme = -1;
+    if (ps[q].iflag_flux != h->info.int_flux) h->info.int_flux = -1;
+  }
   {
     int dev = 0;
     cudaGetDevice(&dev);

@@ -20,6 +20,8 @@ struct RunInfo {
   int lu_version;         // 2: one thread per column; 3: four thread groups per column, staged by element; 4: staged by sector
   int lu_tc;              // columns per tile (32 or 64)
   int recon_prim;         // 1: every solve reconstructs primitive variables
+  int int_scheme;         // the interior scheme (Iflag_Scheme) if every solve uses the same one, else -1
+  int int_flux;           // the flux (Iflag_Flux) if every solve uses the same one, else -1
   const int* bc_rounds;   // per boundary round: first entry, end entry, cells
   int nround;
   // ordered interface-copy levels (empty: all copies independent, one launch); per level the

@@ -505,8 +505,11 @@ __global__ void k_amut(Arena<T> A) {
 template <class T>
 struct InvFluxOcc { static constexpr int value = sizeof(T) == 8 ? 3 : INV_FLUX_MIXED_MINB; };
 // PRIM: every solve of the handle reconstructs the primitive variables (IFlag_Reconstruction = 0),
-// so the conservative / characteristic branches are compiled out
-template <class T, int DIR, bool PRIM = false>
+// so the conservative / characteristic branches are compiled out.  ISCH / IFLUX (>= 0): every
+// solve uses this interior scheme / flux, so the faces that use the interior scheme take a
+// straight-line path (the five reconstructions without a switch between them, free to interleave)
+// and the flux switch folds; boundary faces keep the general path.
+template <class T, int DIR, bool PRIM = false, int ISCH = -1, int IFLUX = -1>
 __global__ void __launch_bounds__(256, InvFluxOcc<T>::value) k_inv_flux(Arena<T> A) {
   const long long tb = A.tot_box, tf = A.tot_face;
   OCFD_GRID_STRIDE(g, tf) {
@@ -532,7 +535,16 @@ __global__ void __launch_bounds__(256, InvFluxOcc<T>::value) k_inv_flux(Arena<T>
     long long c0 = bix(B, i - 4 * di, j - 4 * dj, k - 4 * dk);
     const long long st = DIR == 0 ? 1 : (DIR == 1 ? (long long)B.NX : (long long)B.NX * B.NY);
     T UL[5], UR[5];
-    if (PRIM || s.recon == 0) {
+    if ((PRIM || s.recon == 0) && ISCH >= 0 && scheme == ISCH) {
+#pragma unroll
+      for (int m = 0; m < 5; m++) {
+        const int pl = m == 4 ? P_P : m;
+        T u[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) u[q] = A.P[pl * tb + c0 + q * st];
+        scheme_LR(u, ISCH < 0 ? 0 : ISCH, UL[m], UR[m]);
+      }
+    } else if (PRIM || s.recon == 0) {
       T u[8];
 #pragma unroll
       for (int m = 0; m < 5; m++) {
@@ -609,7 +621,7 @@ __global__ void __launch_bounds__(256, InvFluxOcc<T>::value) k_inv_flux(Arena<T>
     QL[3] = UL[1] * s3x + UL[2] * s3y + UL[3] * s3z; QL[4] = UL[4];
     QR[0] = UR[0]; QR[1] = UR[1] * s1x + UR[2] * s1y + UR[3] * s1z; QR[2] = UR[1] * s2x + UR[2] * s2y + UR[3] * s2z;
     QR[3] = UR[1] * s3x + UR[2] * s3y + UR[3] * s3z; QR[4] = UR[4];
-    flux_1d(QL, QR, F0, T(s.gamma), s.flux);
+    flux_1d(QL, QR, F0, T(s.gamma), IFLUX >= 0 ? IFLUX : s.flux);
     T S = A.M[(M_SI + DIR) * tf + g];
     T* Fo = A.Fi + (long long)DIR * 5 * tf + g;
     Fo[0] = -F0[0] * S;

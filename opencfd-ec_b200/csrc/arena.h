@@ -58,12 +58,17 @@ enum : int {
 // primitive planes in the box arrays
 enum : int { P_D = 0, P_U, P_V, P_W, P_P, P_T, P_C, P_COUNT };
 
+constexpr int HINT_SHIFT = 10;  // 1024 elements per block-hint chunk
+
 template <class T>
 struct Arena {
   // layout
   const BlkD* blk;
   int nblk;
   const long long* pre_box;   // nblk+1 prefix sums of box sizes
+  // block of element q << HINT_SHIFT of the box, cell and face index spaces (a lookup start for
+  // the block of any element: at most a few block starts lie inside one chunk)
+  const int *hint_box, *hint_cell, *hint_face;
   const long long* pre_cell;  // nblk+1
   const long long* pre_face;  // nblk+1
   const long long* pre_col;   // nblk+1, (ny-1)(nz-1) columns per block

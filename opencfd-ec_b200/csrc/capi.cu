@@ -97,6 +97,7 @@ struct ocfd_handle {
   SubD* d_sub = nullptr;
   SolveP* d_sp = nullptr;
   long long *d_pre_box = nullptr, *d_pre_cell = nullptr, *d_pre_face = nullptr, *d_pre_col = nullptr, *d_pre_subcell = nullptr, *d_pre_halo = nullptr;
+  int *d_hint_box = nullptr, *d_hint_cell = nullptr, *d_hint_face = nullptr;
   long long *d_pre_lnj = nullptr, *d_pre_lnk = nullptr;  // j-line and k-line prefix sums (residual smoothing)
   int4 *d_cchunk = nullptr, *d_wchunk = nullptr;
   int* d_cspre = nullptr;
@@ -289,6 +290,7 @@ template <class T>
 static void fill_arena(ocfd_handle* h, Arena<T>& A, const T* M, const T* vol, const T* dtm, const T* dw) {
   A.blk = h->d_blk; A.nblk = h->nblk;
   A.pre_box = h->d_pre_box; A.pre_cell = h->d_pre_cell; A.pre_face = h->d_pre_face; A.pre_col = h->d_pre_col;
+  A.hint_box = h->d_hint_box; A.hint_cell = h->d_hint_cell; A.hint_face = h->d_hint_face;
   A.pre_lnj = h->d_pre_lnj; A.pre_lnk = h->d_pre_lnk; A.tot_lnj = h->pre_lnj[h->nblk]; A.tot_lnk = h->pre_lnk[h->nblk];
   A.sub = h->d_sub; A.nsub = (int)h->sub.size();
   A.pre_subcell = h->d_pre_subcell; A.pre_halo = h->d_pre_halo;
@@ -695,6 +697,21 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   h->d_blk = M.alloc<BlkD>(nblk, e);
   h->d_sub = M.alloc<SubD>(std::max(1, ns), e);
   h->d_sp = M.alloc<SolveP>(nsolve, e);
+  // block hints of the box, cell and face index spaces (find_blk_h)
+  auto hints = [&](const std::vector<long long>& pre) {
+    std::vector<int> hv((size_t)(pre[nblk] >> HINT_SHIFT) + 1);
+    int b = 0;
+    for (size_t q = 0; q < hv.size(); q++) {
+      const long long g = (long long)q << HINT_SHIFT;
+      while (b + 1 < nblk && pre[b + 1] <= g) b++;
+      hv[q] = b;
+    }
+    return hv;
+  };
+  const std::vector<int> hint_box = hints(h->pre_box), hint_cell = hints(h->pre_cell), hint_face = hints(h->pre_face);
+  h->d_hint_box = M.alloc<int>(hint_box.size(), e);
+  h->d_hint_cell = M.alloc<int>(hint_cell.size(), e);
+  h->d_hint_face = M.alloc<int>(hint_face.size(), e);
   h->d_pre_box = M.alloc<long long>(nblk + 1, e); h->d_pre_cell = M.alloc<long long>(nblk + 1, e);
   h->d_pre_face = M.alloc<long long>(nblk + 1, e); h->d_pre_col = M.alloc<long long>(nblk + 1, e);
   h->d_pre_lnj = M.alloc<long long>(nblk + 1, e); h->d_pre_lnk = M.alloc<long long>(nblk + 1, e);
@@ -765,6 +782,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "allocation"); }
   // ---- uploads
   if ((e = up(h->d_blk, h->blk)) || (e = up(h->d_sub, h->sub)) || (e = up(h->d_sp, h->sps)) ||
+      (e = up(h->d_hint_box, hint_box)) || (e = up(h->d_hint_cell, hint_cell)) || (e = up(h->d_hint_face, hint_face)) ||
       (e = up(h->d_pre_box, h->pre_box)) || (e = up(h->d_pre_cell, h->pre_cell)) || (e = up(h->d_pre_face, h->pre_face)) ||
       (e = up(h->d_pre_col, h->pre_col)) || (e = up(h->d_pre_subcell, h->pre_subcell)) || (e = up(h->d_pre_halo, h->pre_halo)) ||
       (e = up(h->d_pre_lnj, h->pre_lnj)) || (e = up(h->d_pre_lnk, h->pre_lnk)) ||

@@ -145,6 +145,8 @@ int ocfd_finalize_params(ocfd_params* p);
  * Geometry (coordinate ghosts sub_update_buffer_mpi.f90:230-512, metrics sub_geometry.f90:6-346,
  * mesh-quality dt factor sub_geometry.f90:361-515) is computed on the device.  The flow is set
  * to freestream (init_flow_zero, sub_init.f90:302-410) with BC + halo applied.
+ * OCFD_ERR_ARG for a block with fewer than 2 nodes in a direction or whose ghost box
+ * (nx+7)(ny+7)(nz+7) reaches 2^31 cells (the kernels index within a block in 32 bits).
  */
 int ocfd_create(const ocfd_params* p, int nblk, const int* nijk, const double* const* xyz,
                 const int* nsub, const int* inc, const double* const* dw, ocfd_handle** out);

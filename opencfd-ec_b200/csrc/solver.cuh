@@ -685,11 +685,9 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_visc_flux(Arena<T> A) {
     if (DIR == 1 && (i == B.nx || k == B.nz)) continue;
     if (DIR == 2 && (i == B.nx || j == B.ny)) continue;
     T* Fo = A.Fv + (long long)DIR * 4 * tf + g;
-    if (A.flags[b] == 1) {  // OverLimit: no viscous flux, Surf = 0 (734-750)
-      int idx = DIR == 0 ? i : (DIR == 1 ? j : k), nd = DIR == 0 ? B.nx : (DIR == 1 ? B.ny : B.nz);
-      if (idx == 1 || idx == nd) { Fo[0] = T(0); Fo[tf] = T(0); Fo[2 * tf] = T(0); }
-      continue;
-    }
+    // the block's OverLimit flag is tested after the stencil loads below (a branch on it here
+    // would hold every load of the face behind the flag's load)
+    const int overlimit = A.flags[b];
     const SolveP& s = A.sp[B.solve];
     const T *Pu = A.P + P_U * tb, *Pv = A.P + P_V * tb, *Pw = A.P + P_W * tb, *PT = A.P + P_T * tb;
     auto avg = [&](const T* a, int i1, int j1, int k1, int i2, int j2, int k2) -> T { return T(0.5) * (a[bix(B, i1, j1, k1)] + a[bix(B, i2, j2, k2)]); };
@@ -742,6 +740,11 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_visc_flux(Arena<T> A) {
       }
       ui = T(0.5) * (ui2 - ui1); vi = T(0.5) * (vi2 - vi1); wi = T(0.5) * (wi2 - wi1); Ti = T(0.5) * (Ti2 - Ti1);
       uj = T(0.5) * (uj2 - uj1); vj = T(0.5) * (vj2 - vj1); wj = T(0.5) * (wj2 - wj1); Tj = T(0.5) * (Tj2 - Tj1);
+    }
+    if (overlimit == 1) {  // OverLimit: no viscous flux, Surf = 0 (734-750)
+      int idx = DIR == 0 ? i : (DIR == 1 ? j : k), nd = DIR == 0 ? B.nx : (DIR == 1 ? B.ny : B.nz);
+      if (idx == 1 || idx == nd) { Fo[0] = T(0); Fo[tf] = T(0); Fo[2 * tf] = T(0); }
+      continue;
     }
     const int J = DIR == 0 ? M_J1 : (DIR == 1 ? M_J2 : M_J3);
     T ix = A.M[(J + 0) * tf + g], iy = A.M[(J + 1) * tf + g], iz = A.M[(J + 2) * tf + g];

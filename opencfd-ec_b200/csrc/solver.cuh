@@ -516,8 +516,12 @@ struct InvFluxOcc { static constexpr int value = sizeof(T) == 8 ? 3 : INV_FLUX_M
 // solve uses this interior scheme / flux, so the faces that use the interior scheme take a
 // straight-line path (the five reconstructions without a switch between them, free to interleave)
 // and the flux switch folds; boundary faces keep the general path.
+// CTAs per SM: FP64 3 (80 registers); the FP64 MUSCL3 specialisation 2 (about 120 registers, no
+// spills: config 1 residual phase 0.099 -> 0.094 ms; WENO5 is faster at 3, 1.85 against 2.00 ms)
+template <class T, int ISCH>
+struct InvFluxOccS { static constexpr int value = (sizeof(T) == 8 && ISCH == S_MUSCL3) ? 2 : InvFluxOcc<T>::value; };
 template <class T, int DIR, bool PRIM = false, int ISCH = -1, int IFLUX = -1>
-__global__ void __launch_bounds__(256, InvFluxOcc<T>::value) k_inv_flux(Arena<T> A) {
+__global__ void __launch_bounds__(256, InvFluxOccS<T, ISCH>::value) k_inv_flux(Arena<T> A) {
   const long long tb = A.tot_box, tf = A.tot_face;
   OCFD_GRID_STRIDE(g, tf) {
     int b = find_blk_h(A.pre_face, A.hint_face, A.nblk, g);

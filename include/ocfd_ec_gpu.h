@@ -244,9 +244,13 @@ int ocfd_synchronize(ocfd_handle* h);
  * ocfd_residual for solve 0 that allocates nothing, neither device nor host heap memory: for
  * callers that must not allocate inside their iteration loop (a driver whose device memory is
  * fully committed to resident solves, or a monitor that must not touch an allocator while the
- * solver runs).  Its scratch is one static device area per device, shared by all handles of the
- * process: at most 33,554,432 interior cells (4096 chunks of 8192) and 256 solves per handle;
- * larger handles get OCFD_ERR_ARG with a message (use ocfd_residual).  The first call on a device
+ * solver runs).  Its error paths allocate nothing either: their messages are formatted on the
+ * stack into the handle's preallocated error string.  Its scratch is one static device area per
+ * device, shared by all handles of the process: at most 4096 norm chunks and 256 solves per
+ * handle.  Every block's interior cells are cut into chunks of at most 8192 cells, so the limit is
+ * 33,554,432 cells for large blocks and fewer for many small ones (256 solves of 17 small blocks
+ * already make 4352 chunks); larger handles get OCFD_ERR_ARG with their chunk count in the
+ * message (use ocfd_residual).  The first call on a device
  * looks the area up (cudaGetSymbolAddress) with that device current; make that first call before
  * any stream capture.  Calls that overlap in time (other threads, other handles on the same
  * device) race on the shared area and must be serialised by the caller.  On a NaN it returns

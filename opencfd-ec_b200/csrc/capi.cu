@@ -150,6 +150,18 @@ static int fail(ocfd_handle* h, int code, const std::string& msg) {
 static int cuda_fail(ocfd_handle* h, cudaError_t e, const char* where) {
   return fail(h, e == cudaErrorMemoryAllocation ? OCFD_ERR_OOM : OCFD_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
+// error paths that allocate nothing (ocfd_residual_static): the message is formatted on the
+// stack and copied into the handle's error string, whose capacity (512 bytes) every handle
+// reserves at creation, so the copy never reallocates
+static int fail_c(ocfd_handle* h, int code, const char* msg) {
+  if (h) h->err.assign(msg, std::min<size_t>(std::strlen(msg), 511));
+  return code;
+}
+static int cuda_fail_c(ocfd_handle* h, cudaError_t e, const char* where) {
+  char buf[256];
+  std::snprintf(buf, sizeof buf, "%s: %s", where, cudaGetErrorString(e));
+  return fail_c(h, e == cudaErrorMemoryAllocation ? OCFD_ERR_OOM : OCFD_ERR_CUDA, buf);
+}
 
 extern "C" const char* ocfd_version(void) { return "ocfd-b200 abi 1 sm_100a (FP64 + mixed FP32/FP64)"; }
 
@@ -1419,7 +1431,10 @@ extern "C" int ocfd_residual_all(ocfd_handle* h, double* rmax, double* rrms) {
 // of the process: per-chunk partial max / sum of squares, per-solve totals, and the NaN location.
 // Each call overwrites all partials and totals it reads; only the NaN location must start at its
 // sentinel (all ones), which the call resets on the handle's stream before the norm kernels.
-constexpr int kStaticNormChunks = 4096;  // 8192 cells per chunk: up to 33,554,432 interior cells
+// each block's interior cells are cut into norm chunks of at most 8192 cells, so 4096 chunks hold
+// 33,554,432 cells only when the blocks are large; a handle of many small blocks reaches 4096
+// chunks with fewer cells
+constexpr int kStaticNormChunks = 4096;
 constexpr int kStaticNormSolves = 256;
 static __device__ __align__(256) double g_static_norm[(kStaticNormChunks + kStaticNormSolves) * 14];
 static __device__ __align__(256) unsigned long long g_static_nan;
@@ -1441,15 +1456,15 @@ std::mutex g_static_mu;
 static int static_norm_area(ocfd_handle* h, StaticNormArea& a) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return cuda_fail(h, e, "residual_static: cudaGetDevice");
-  if (dev < 0 || dev >= kMaxDevices) return fail(h, OCFD_ERR_ARG, "residual_static: device ordinal beyond 63");
+  if (e != cudaSuccess) return cuda_fail_c(h, e, "residual_static: cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail_c(h, OCFD_ERR_ARG, "residual_static: device ordinal beyond 63");
   std::lock_guard<std::mutex> lk(g_static_mu);
   StaticNormArea& c = g_static_area[dev];
   if (!c.part) {
     void* p = nullptr;
     void* n = nullptr;
-    if ((e = cudaGetSymbolAddress(&p, g_static_norm)) != cudaSuccess) return cuda_fail(h, e, "residual_static: cudaGetSymbolAddress");
-    if ((e = cudaGetSymbolAddress(&n, g_static_nan)) != cudaSuccess) return cuda_fail(h, e, "residual_static: cudaGetSymbolAddress");
+    if ((e = cudaGetSymbolAddress(&p, g_static_norm)) != cudaSuccess) return cuda_fail_c(h, e, "residual_static: cudaGetSymbolAddress");
+    if ((e = cudaGetSymbolAddress(&n, g_static_nan)) != cudaSuccess) return cuda_fail_c(h, e, "residual_static: cudaGetSymbolAddress");
     c.part = (double*)p;
     c.out = (double*)p + (size_t)kStaticNormChunks * 14;
     c.nan = (unsigned long long*)n;
@@ -1460,10 +1475,15 @@ static int static_norm_area(ocfd_handle* h, StaticNormArea& a) {
 
 extern "C" int ocfd_residual_static(ocfd_handle* h, double* rmax, double* rrms) {
   if (!h || !rmax || !rrms) return OCFD_ERR_ARG;
-  if (h->part) return fail(h, OCFD_ERR_UNSUPPORTED, "residual_static: not for sharded handles (the norms are all-reduced); use ocfd_residual");
-  if ((long long)h->cchunk.size() > kStaticNormChunks)
-    return fail(h, OCFD_ERR_ARG, "residual_static: the handle has more than 33,554,432 interior cells (4096 chunks); use ocfd_residual");
-  if (h->nsolve > kStaticNormSolves) return fail(h, OCFD_ERR_ARG, "residual_static: the handle has more than 256 solves; use ocfd_residual");
+  if (h->part) return fail_c(h, OCFD_ERR_UNSUPPORTED, "residual_static: not for sharded handles (the norms are all-reduced); use ocfd_residual");
+  if ((long long)h->cchunk.size() > kStaticNormChunks) {
+    char buf[256];
+    std::snprintf(buf, sizeof buf,
+                  "residual_static: the handle has %lld norm chunks (each block's interior cells in chunks of at most 8192), "
+                  "more than 4096; use ocfd_residual", (long long)h->cchunk.size());
+    return fail_c(h, OCFD_ERR_ARG, buf);
+  }
+  if (h->nsolve > kStaticNormSolves) return fail_c(h, OCFD_ERR_ARG, "residual_static: the handle has more than 256 solves; use ocfd_residual");
   StaticNormArea a;
   if (int rc = static_norm_area(h, a)) return rc;
   k_static_nan_reset<<<1, 1, 0, h->st>>>(a.nan);
@@ -1475,7 +1495,7 @@ extern "C" int ocfd_residual_static(ocfd_handle* h, double* rmax, double* rrms) 
   cudaMemcpyAsync(&nan_at, a.nan, 8, cudaMemcpyDeviceToHost, h->st);
   cudaMemcpyAsync(&lu_err, h->d_lu_err, 4, cudaMemcpyDeviceToHost, h->st);
   cudaError_t e = cudaStreamSynchronize(h->st);
-  if (e != cudaSuccess) return cuda_fail(h, e, "residual_static");
+  if (e != cudaSuccess) return cuda_fail_c(h, e, "residual_static");
   for (int m = 0; m < 7; m++) {
     rmax[m] = m < h->nvar ? out[m] : 0.0;
     rrms[m] = m < h->nvar ? std::sqrt(out[7 + m] / (double)h->ncell_s[0]) : 0.0;
@@ -1483,9 +1503,9 @@ extern "C" int ocfd_residual_static(ocfd_handle* h, double* rmax, double* rrms) 
   if (lu_err) {
     cudaMemsetAsync(h->d_lu_err, 0, 4, h->st);
     cudaStreamSynchronize(h->st);
-    return fail(h, OCFD_ERR_TIMEOUT, "LU-SGS wavefront: a bounded wait between tiles timed out");
+    return fail_c(h, OCFD_ERR_TIMEOUT, "LU-SGS wavefront: a bounded wait between tiles timed out");
   }
-  if (nan_at != ~0ULL) return fail(h, OCFD_ERR_NAN, "NaN in residual (location: ocfd_residual)");
+  if (nan_at != ~0ULL) return fail_c(h, OCFD_ERR_NAN, "NaN in residual (location: ocfd_residual)");
   return OCFD_OK;
 }
 

@@ -10,6 +10,11 @@ converges (density-residual RMS down by ``drop`` from its first iteration, or |d
 ``dcl`` over the last ``dcl_window`` iterations) or reaches ``max_iters``; its memory is
 released for the next admission.
 
+A request whose solve fails (a NaN in its residual, a device wait that ran out, a CUDA error on
+its handle) ends with ``converged == "error"`` and the message; its handle is closed and its
+memory released, and the other solves go on.  If the loop itself is left by an exception, every
+handle still open is closed.
+
 The sequence of operations on one handle does not depend on the other solves in flight, so a
 request's result is the same alone and in the mix (bit for bit).  No counterpart in the
 reference, which runs one case per MPI job.
@@ -30,6 +35,7 @@ class Request:
     case: object
     arrival: float = 0.0            # seconds after the loop starts
     max_iters: int = 5000
+    state: Optional[list] = None    # initial state per block (Fortran layout, as a restart reads it)
 
 
 @dataclass
@@ -40,12 +46,13 @@ class Result:
     admitted: float
     finished: float
     iters: int
-    converged: str                  # "residual", "cl", or "max_iters"
+    converged: str                  # "residual", "cl", "max_iters", or "error"
     rms0: float
     rms: np.ndarray
     cl: float
     cd: float
     cl_hist: List[float] = field(default_factory=list)
+    error: str = ""
 
     @property
     def latency(self):
@@ -78,6 +85,19 @@ class Server:
         free, _ = torch.cuda.mem_get_info()
         return int(free * 0.9)
 
+    def _start(self, r):
+        """Handle, restart state and first iteration of request r."""
+        s = capi.Solver(r.params, r.case)
+        try:
+            if r.state is not None:
+                for b, U in enumerate(r.state):
+                    s.set_state(b, U)
+            s.advance(1)
+        except Exception:
+            s.close()
+            raise
+        return s
+
     def _done(self, a):
         _, rms = a.s.residual()
         _, cl, cd, _ = a.s.forces()
@@ -101,52 +121,71 @@ class Server:
         used = 0
         fp = {}
         t0 = self.clock()
-        while pending or queue or active:
-            now = self.clock() - t0
-            while pending and pending[0].arrival <= now:
-                queue.append(pending.pop(0))
-            # admission: FIFO, by free slot and device footprint
-            while queue and len(active) < self.max_active:
-                r = queue[0]
-                need = fp.setdefault(r.rid, capi.footprint(r.params, r.case))
-                if used + need > budget:
-                    if not active:
-                        raise MemoryError("request %d needs %d bytes, budget %d" % (r.rid, need, budget))
-                    break
-                queue.pop(0)
-                s = capi.Solver(r.params, r.case)
-                used += need
-                a = _Active(r, s, self.clock() - t0)
-                s.advance(1)
-                a.iters = 1
-                active.append(a)
-            if not active:
-                if pending:
-                    time.sleep(max(0.0, min(0.05, pending[0].arrival - (self.clock() - t0))))
-                continue
-            # every solve whose queued chunk has finished is read back and given its next chunk;
-            # the others keep running
-            still, progressed = [], False
+
+        def failed(r, admitted, iters, err, a=None):
+            nan = float("nan")
+            results.append(Result(r.rid, r.case.ncells, r.arrival, admitted, self.clock() - t0, iters, "error",
+                                  nan if a is None or a.rms0 is None else float(a.rms0), np.full(7, nan), nan, nan,
+                                  [] if a is None else [c for _, c in a.cl_hist], str(err)))
+
+        try:
+            while pending or queue or active:
+                now = self.clock() - t0
+                while pending and pending[0].arrival <= now:
+                    queue.append(pending.pop(0))
+                # admission: FIFO, by free slot and device footprint
+                while queue and len(active) < self.max_active:
+                    r = queue[0]
+                    need = fp.setdefault(r.rid, capi.footprint(r.params, r.case))
+                    if used + need > budget:
+                        if not active:
+                            raise MemoryError("request %d needs %d bytes, budget %d" % (r.rid, need, budget))
+                        break
+                    queue.pop(0)
+                    admitted = self.clock() - t0
+                    try:
+                        s = self._start(r)
+                    except (capi.OcfdError, FloatingPointError) as e:
+                        failed(r, admitted, 0, e)
+                        continue
+                    used += need
+                    a = _Active(r, s, admitted)
+                    a.iters = 1
+                    active.append(a)
+                if not active:
+                    if pending:
+                        time.sleep(max(0.0, min(0.05, pending[0].arrival - (self.clock() - t0))))
+                    continue
+                # every solve whose queued chunk has finished is read back and given its next chunk;
+                # the others keep running
+                still, progressed = [], False
+                for a in active:
+                    if not a.stream.query():
+                        still.append(a)
+                        continue
+                    progressed = True
+                    try:
+                        why, rms, cl, cd = self._done(a)
+                        if why is None:
+                            n = min(self.chunk, a.req.max_iters - a.iters)
+                            a.s.advance(n)
+                            a.iters += n
+                            still.append(a)
+                            continue
+                    except (capi.OcfdError, FloatingPointError) as e:
+                        failed(a.req, a.admitted, a.iters, e, a)
+                    else:
+                        fin = self.clock() - t0
+                        results.append(Result(a.req.rid, a.req.case.ncells, a.req.arrival, a.admitted, fin, a.iters, why,
+                                              float(a.rms0), rms.copy(), cl, cd, [c for _, c in a.cl_hist]))
+                    a.s.close()
+                    used -= fp[a.req.rid]
+                active = still
+                if not progressed:
+                    time.sleep(0.0002)
+        finally:
             for a in active:
-                if not a.stream.query():
-                    still.append(a)
-                    continue
-                progressed = True
-                why, rms, cl, cd = self._done(a)
-                if why is None:
-                    n = min(self.chunk, a.req.max_iters - a.iters)
-                    a.s.advance(n)
-                    a.iters += n
-                    still.append(a)
-                    continue
-                fin = self.clock() - t0
-                results.append(Result(a.req.rid, a.req.case.ncells, a.req.arrival, a.admitted, fin, a.iters, why,
-                                      float(a.rms0), rms.copy(), cl, cd, [c for _, c in a.cl_hist]))
                 a.s.close()
-                used -= fp[a.req.rid]
-            active = still
-            if not progressed:
-                time.sleep(0.0002)
         return sorted(results, key=lambda r: r.rid)
 
 
@@ -165,4 +204,4 @@ def summarize(results, wall_s):
     cells = sum(r.cells * r.iters for r in results)
     return {"requests": len(results), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "cell_updates_per_s": cells / wall_s, "wall_s": wall_s,
-            "converged": {k: sum(1 for r in results if r.converged == k) for k in ("residual", "cl", "max_iters")}}
+            "converged": {k: sum(1 for r in results if r.converged == k) for k in ("residual", "cl", "max_iters", "error")}}

@@ -29,6 +29,14 @@ def small_cases():
         "foil_sa_lusgs_smooth": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=4, turb=2, if_residual_smoothing=1),
         "foil_lam_rk3_smooth": lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=4, turb=0, time_method=3, cfl=1.5,
                                                      if_residual_smoothing=1),
+        # the schemes no other case uses as the interior scheme (sub_scheme.f90:6-96): UD1, NND2,
+        # UD3, MUSCL2U, UD5, and UD1 as the boundary scheme
+        "foil_sa_ud1_roe": lambda: cases.airfoil(ni=65, nj=17, scheme=0, flux=4, turb=2),
+        "foil_lam_nnd2_vl": lambda: cases.airfoil(ni=65, nj=17, scheme=1, flux=5, turb=0),
+        "bump_ud3_roe": lambda: cases.config1(scale=0.25, iflag_scheme=2),
+        "foil_sa_muscl2u_sw": lambda: cases.airfoil(ni=65, nj=17, scheme=3, flux=1, turb=2),
+        "bump_ud5_ausmpw": lambda: cases.config1(scale=0.25, iflag_scheme=8, iflag_flux=6),
+        "foil_sa_ud3_bound_ud1": lambda: cases.airfoil(ni=65, nj=17, scheme=2, flux=4, turb=2, bound_scheme=0),
         "bump_dual_smooth": lambda: cases.config1(scale=0.25, cuts_i=(12,), time_method=-1, dt_global=0.2, step_inner_limit=3,
                                                   res_inner_limit=1e-14, if_residual_smoothing=1),
     }

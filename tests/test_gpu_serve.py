@@ -46,3 +46,35 @@ def test_admission_by_footprint(gpu):
         peak = max(peak, live)
     assert peak <= 2
     assert all(r.iters == 150 or r.converged != "max_iters" for r in out)
+
+
+def test_failing_request_leaves_the_others_untouched(gpu):
+    """A request whose restart state holds a NaN fails on its first read-back (OCFD_ERR_NAN); it
+    ends as an "error" result with the message, its handle is closed and its memory released,
+    and every other request of the mix gives the same result as alone (bit for bit)."""
+    import copy
+
+    import torch
+    from ocfd_b200 import capi
+    from ocfd_b200.serve import Request, Server
+    base = reqs()
+    p, c = base[1].params, base[1].case
+    s = capi.Solver(p, c)
+    s.advance(3)
+    state = [s.get_state(b) for b in range(s.nblk)]
+    s.close()
+    state[0][3 + 1, 3 + 5, 3 + 7, 0] = float("nan")
+    bad = Request(9, p, c, 0.02, 300, state)
+    free0 = torch.cuda.mem_get_info()[0]
+    mix = Server(chunk=50).run(copy.copy(base) + [bad])
+    assert len(mix) == 5
+    r_bad = [r for r in mix if r.rid == 9][0]
+    assert r_bad.converged == "error" and "NaN" in r_bad.error, r_bad.error
+    for r in mix:
+        if r.rid == 9:
+            continue
+        alone = Server(chunk=50).run([x for x in reqs() if x.rid == r.rid])[0]
+        assert r.converged != "error"
+        assert np.array_equal(alone.rms, r.rms) and alone.cl == r.cl and alone.cd == r.cd
+    # every handle of the run was closed: the device memory is back
+    assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)

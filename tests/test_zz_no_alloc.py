@@ -1,7 +1,9 @@
 """ocfd_residual_static: the allocation-free residual norms agree bit for bit with
-ocfd_residual, on two calls in a row, across handles sharing the static scratch, and refuse
-handles larger than the static area with a clear error.  Collected last on purpose: it must pass
-alone and after every other test in the process."""
+ocfd_residual, on two calls in a row, across handles sharing the static scratch; a fresh handle
+whose first read-back is this call leaves the device's free memory unchanged; handles larger than
+the static area (in solves or in norm chunks) are refused with a clear error, and a NaN gives
+OCFD_ERR_NAN.  Collected last on purpose: it must pass alone and after every other test in the
+process."""
 import numpy as np
 import pytest
 
@@ -37,3 +39,55 @@ def test_static_residual_rejects_oversize_handle(gpu):
         b.residual_static()
     assert e.value.code == gpu.OCFD_ERR_ARG and "256 solves" in str(e.value)
     b.close()
+
+
+def test_static_residual_first_call_allocates_nothing(gpu):
+    """A fresh handle calls ocfd_residual_static before any other read-back (so the pinned
+    read-back area of ocfd_residual is never set up): the device's free memory stays the same
+    over repeated calls, and the norms equal ocfd_residual's afterwards."""
+    import torch
+    from ocfd_b200 import cases
+    p, case = cases.airfoil(ni=65, nj=17)
+    s = gpu.Solver(p, case)
+    s.advance(2)
+    s.synchronize()
+    first = s.residual_static()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        again = s.residual_static()
+        assert all(np.array_equal(x, y) for x, y in zip(first, again))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert all(np.array_equal(x, y) for x, y in zip(s.residual(), first))
+    s.close()
+
+
+def test_static_residual_rejects_too_many_chunks(gpu):
+    """241 solves of 17 small blocks each: 4097 norm chunks (one per block) with only 262,208
+    cells and fewer than 256 solves; refused with OCFD_ERR_ARG and the chunk count."""
+    from meshes import wavy_box
+    from ocfd_b200.params import make_params
+    case = wavy_box(nx=69, ny=5, nz=5, cuts=tuple(range(5, 69, 4)))
+    assert len(case.dims) == 17
+    p = make_params(ma=0.5, if_viscous=0, iflag_scheme=5, iflag_flux=4, cfl=2.0)
+    b = gpu.Batch([(p, case)] * 241)
+    with pytest.raises(gpu.OcfdError) as e:
+        b.residual_static()
+    assert e.value.code == gpu.OCFD_ERR_ARG and "4097 norm chunks" in str(e.value), str(e.value)
+    b.close()
+
+
+def test_static_residual_reports_nan(gpu):
+    from ocfd_b200 import cases
+    p, case = cases.airfoil(ni=65, nj=17)
+    s = gpu.Solver(p, case)
+    s.advance(2)
+    U = s.get_state(0)
+    U[3 + 1, 3 + 6, 3 + 20, 0] = float("nan")
+    s.set_state(0, U)
+    s.advance(1)
+    with pytest.raises(FloatingPointError) as e:
+        s.residual_static()
+    assert "NaN" in str(e.value)
+    s.close()

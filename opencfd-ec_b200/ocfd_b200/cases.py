@@ -32,24 +32,37 @@ def config2(ni=257, nj=97, nk_wing=61, nk_tip=26, i_cut=49, **over):
     return make_params(**raw), case
 
 
+FUSELAGE = dict(length=4.0, fineness=8.0, xc=0.5)   # ellipsoid: 4 root chords long, fineness 8, centred at mid-chord
+
+
 def config3(ni=449, nj=129, nk_wing=97, nk_tip=41, i_cut=86, j_cuts=(33, 73), **over):
-    """Config 3 stand-in: the swept wing refined to ~7.8 M cells in 24 uneven blocks (4 around
-    the section x 3 wall-normal x 2 spanwise), RANS-SST, MUSCL3, LU-SGS, M 0.75, AoA 2 deg, Re 3e6,
-    mixed precision by default (the FP64 run of the same case is precision=0).  Two deviations:
-    the ellipsoidal fuselage is not modelled (only the wing, root on a symmetry plane), and the
-    flux is Roe: HLLC as the reference implements it (the right star state carries v into the
-    w-momentum, sub_flux_split.f90:67) diverges within 5 steps on this 3-D wing, in the CPU
-    restatement as on the GPU; iflag_flux=3 selects it.  LU-SGS runs at CFL 1 (at 2 and above the
-    wall cell at the root trailing edge diverges within 15 steps at this resolution with SST).
-    The RK3 variant (time_method=3) runs at
-    CFL 0.5: at the configuration's 1.5, explicit RK3 with the SST sources diverges in the first
-    steps on this mesh (wall spacing 4.5e-6 chord), again in both implementations."""
-    case = meshgen.swept_wing(ni=ni, nj=nj, nk_wing=nk_wing, nk_tip=nk_tip, i_cut=i_cut, j_cuts=j_cuts,
-                              name="config3_wing_%dx%dx%d_24blk" % (ni, nj, nk_wing + nk_tip - 1))
+    """Config 3: the swept wing with an ellipsoidal fuselage (length 4 chords, fineness 8) at its
+    root, ~7.8 M cells in 24 uneven blocks (4 around the section x 3 wall-normal x 2 spanwise),
+    RANS-SST, MUSCL3, LU-SGS, M 0.75, AoA 2 deg, Re 3e6, mixed precision by default (the FP64 run
+    of the same case is precision=0).  The fuselage is the root surface lifted onto the half
+    ellipsoid (meshgen.swept_wing); it keeps the root plane's symmetry condition, so it is a slip
+    surface and its pressure is not in the integrated forces.
+
+    The flux defaults to Roe, a stand-in: with HLLC as the configuration states (iflag_flux=3),
+    the reference algorithm diverges in the first iterations on this wing-body, in the CPU
+    restatement as on the GPU (its right star state carries v into the w-momentum,
+    sub_flux_split.f90:67); config3_as_specified() builds that case.  LU-SGS runs at CFL 1.  The
+    RK3 variant (time_method=3) of the configuration is at CFL 1.5, where explicit RK3 with the SST
+    model diverges at the first step in the far field beyond the tip (at CFL 0.8 too; Euler,
+    laminar and SA run); the stand-in uses CFL 0.5."""
+    case = meshgen.swept_wing(ni=ni, nj=nj, nk_wing=nk_wing, nk_tip=nk_tip, i_cut=i_cut, j_cuts=j_cuts, fuselage=FUSELAGE,
+                              name="config3_wingbody_%dx%dx%d_24blk" % (ni, nj, nk_wing + nk_tip - 1))
     raw = dict(ma=0.75, aoa=2.0, re=3.0e6, if_viscous=1, iflag_turbulence_model=3, iflag_scheme=5, iflag_flux=4,
                time_method=0, cfl=1.0, precision=1, kt_inf=1e-8, wt_inf=1e-5, ref_s=meshgen.wing_ref_area(), ref_l=1.0)
     raw.update(over)
     return make_params(**raw), case
+
+
+def config3_as_specified(rk3=False, **over):
+    """Config 3 exactly as stated: HLLC + MUSCL3, LU-SGS, or the RK3 variant at CFL 1.5."""
+    if rk3:
+        return config3(iflag_flux=3, time_method=3, cfl=1.5, **over)
+    return config3(iflag_flux=3, **over)
 
 
 def config3_small(**over):

@@ -7,7 +7,8 @@ reference's case files, whose meshes are not shipped (.MISSING_LARGE_BLOBS:1).
 
 * ``channel_bump``   -- config 1: 129x65x17 channel with a sin^2 bump, optionally cut in i.
 * ``airfoil_omesh``  -- NACA 4-digit O-mesh extruded over k (config 4's 2-D airfoils).
-* ``swept_wing``     -- config 2: O-H mesh around a tapered, swept NACA 0012 wing (8 blocks).
+* ``swept_wing``     -- config 2: O-H mesh around a tapered, swept NACA 0012 wing (8 blocks);
+                        config 3 adds an ellipsoidal fuselage at the root (24 blocks).
 """
 import math
 from dataclasses import dataclass, field
@@ -192,8 +193,16 @@ def airfoil_omesh(ni=129, nj=33, nk=3, m=0.0, p=0.0, t=0.12, radius=20.0, ds=2e-
     return Case(name, [X], [B], meta=dict(kind="airfoil", ni=ni, nj=nj, nk=nk, m=m, p=p, t=t))
 
 
+def fuselage_lift(x, y, length=4.0, fineness=8.0, xc=0.5):
+    """Height above the symmetry plane of a half ellipsoid of revolution about the x axis
+    (length `length`, maximum diameter length / fineness, centred at x = xc), 0 outside it."""
+    a, b = 0.5 * length, 0.5 * length / fineness
+    q = 1.0 - ((x - xc) / a) ** 2 - (y / b) ** 2
+    return b * np.sqrt(np.maximum(q, 0.0))
+
+
 def swept_wing(ni=257, nj=97, nk_wing=61, nk_tip=26, i_cut=49, sweep_deg=30.0, taper=0.56,
-               semi_span=1.5, radius=20.0, ds=4.5e-6, tip_far=15.0, name="wing", j_cuts=()):
+               semi_span=1.5, radius=20.0, ds=4.5e-6, tip_far=15.0, name="wing", j_cuts=(), fuselage=None):
     """Config 2 stand-in: O-H mesh around a swept, tapered NACA 0012 wing.
 
     i runs around each spanwise section (O-type, periodic trailing-edge seam), j from the wall
@@ -204,6 +213,12 @@ def swept_wing(ni=257, nj=97, nk_wing=61, nk_tip=26, i_cut=49, sweep_deg=30.0, t
     upper sides (an inner boundary i <-> ni+1-i).  Blocks: i cut at i_cut, the leading edge and
     ni+1-i_cut; k cut at the tip -> 8 uneven blocks; optional wall-normal cuts at the node
     indices j_cuts multiply that by len(j_cuts)+1.
+
+    fuselage (dict of fuselage_lift's arguments, or None): the root surface k = 1 is lifted onto a
+    half ellipsoid of revolution about the x axis (a wing-body configuration: the wing root sits on
+    the body's side); every k line (i, j) is lifted by the ellipsoid's height above its root node,
+    fading linearly to zero at 60 % of the semi-span, so every node keeps its order in k.  The root face keeps its symmetry condition, which on the lifted part makes the
+    body a slip (inviscid) surface.
     """
     assert ni % 2 == 1
     mid = (ni + 1) // 2
@@ -235,6 +250,11 @@ def swept_wing(ni=257, nj=97, nk_wing=61, nk_tip=26, i_cut=49, sweep_deg=30.0, t
         X[0, k] = X2
         X[1, k] = Y2
         X[2, k] = z[k]
+    if fuselage is not None:
+        # one lift per (i, j) line, from the root plane's node: z stays monotone along every k line
+        zb = 0.6 * semi_span
+        lift = fuselage_lift(X[0, 0], X[1, 0], **fuselage)
+        X[2] = X[2] + lift[None] * np.maximum(0.0, 1.0 - X[2] / zb)
     kt = nk_wing  # node index of the tip plane
     ibnd = [1, i_cut, mid, ni + 1 - i_cut, ni]
     jbnd = [1] + list(j_cuts) + [nj]

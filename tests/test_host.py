@@ -10,7 +10,9 @@ import pytest
 from conftest import ROOT
 
 HEADER = os.path.join(ROOT, "include", "ocfd_ec_gpu.h")
-REF_CASES = "/root/reference/cases"
+# the reference's case folder (M6-wing, M6-wing-SEC, DLR-F4 with their bc3d.inp decks), when a
+# checkout of the reference is at hand: OCFD_REF_CASES=<reference>/cases
+REF_CASES = os.environ.get("OCFD_REF_CASES", "")
 
 
 @pytest.fixture(scope="module")
@@ -137,8 +139,8 @@ def test_convert_reference_bc3d_inp(name):
     """.inp -> .inc conversion (sub_convert_inp.f90:25-248) of the reference's own case decks:
     every inner subface finds its partner and the orientation maps are mutually inverse."""
     path = os.path.join(REF_CASES, name, "bc3d.inp")
-    if not os.path.exists(path):
-        pytest.skip("reference case decks not present on this machine")
+    if not REF_CASES or not os.path.exists(path):
+        pytest.skip("set OCFD_REF_CASES to the reference's cases folder to run this test")
     from ocfd_b200.connectivity import convert_inp_inc, read_bc3d_inp
     inp = read_bc3d_inp(path)
     inc = convert_inp_inc(inp)

@@ -19,6 +19,7 @@
 #include "../../include/ocfd_ec_gpu.h"
 #include "arena.h"
 #include "lusgs.cuh"
+#include "lusgs5.cuh"
 #include "runner.h"
 #include "setup.h"
 
@@ -130,6 +131,9 @@ struct ocfd_handle {
   LuArgs lu{};
   LuArgs lu_var[2]{};          // LU-SGS tile tables for TC = 32, 64
   int lu_tc = 32;              // the tile width in use
+  LuStream lus{};              // version-5 sweep records (built for the 64-column tile table)
+  int lus_v = -1;              // tile table the records were built for (-1: none)
+  bool lus_geo = false;        // static geometry records packed
   RunInfo info{};
   int nsm = 148;
   int* d_lu_err = nullptr;
@@ -366,19 +370,48 @@ static void reset_work(ocfd_handle* h) {
   reset_mu(h);
 }
 
+// version-5 record layout for the handle's precision and NVAR
+static void lu5_layout_for(int prec, int NV, LuStream& S, int TC, int E) {
+  if (prec == OCFD_PREC_MIXED) {
+    if (NV == 5) lu5_layout<float, 5>(S, TC, E);
+    else if (NV == 6) lu5_layout<float, 6>(S, TC, E);
+    else lu5_layout<float, 7>(S, TC, E);
+  } else {
+    if (NV == 5) lu5_layout<double, 5>(S, TC, E);
+    else if (NV == 6) lu5_layout<double, 6>(S, TC, E);
+    else lu5_layout<double, 7>(S, TC, E);
+  }
+}
+
 // (re)builds the runner for LU-SGS tile table v (0: TC = 32, 1: TC = 64) and wavefront kernel
 // version ver (2, 3 or 4); drops a captured graph
 static void select_lu(ocfd_handle* h, int v, int ver) {
+  if (ver == 5 && h->lus_v != v) ver = 4;   // records exist for one tile table only
   h->lu = h->lu_var[v];
   h->lu_tc = v == 0 ? 32 : 64;
   h->info.lu_version = ver;
   h->info.lu = &h->lu;
   h->info.lu_tc = h->lu_tc;
   h->info.lu_grid = std::max(1, std::min(h->lu.ntiles, h->nsm * 8));
+  h->info.lus = ver == 5 ? &h->lus : nullptr;
+  if (ver == 5) {
+    // resident CTAs per SM from the shared memory a CTA takes (ring + exchange arrays + margin)
+    const int TC = h->lu_tc;
+    for (int up = 0; up < 2; up++) {
+      const long long ring = (long long)h->lus.nstage * (h->lus.dyn_bytes + h->lus.geo_bytes + (up ? h->lus.dus_bytes : 0)) + 16 * h->lus.nstage;
+      const long long per = ring + 40LL * h->nvar * TC + 16LL * TC + 2048;
+      const int occ = (int)std::max(1LL, std::min(233472LL / per, 2048LL / (4 * TC + 32)));
+      h->info.lu5_grid[up] = std::max(1, std::min(h->lu.ntiles, h->nsm * occ));
+    }
+  }
   if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
   if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
   if (h->prec == OCFD_PREC_MIXED) h->run.reset(make_runner_mixed(h->A32, h->info));
   else h->run.reset(make_runner_fp64(h->A64, h->info));
+  if (ver == 5 && h->run && !h->lus_geo) {
+    h->run->lu5_pack_geo(h->st);
+    h->lus_geo = true;
+  }
 }
 
 // LU-SGS autotuner: each candidate (tile table v, kernel version ver) sweeps the freshly
@@ -872,6 +905,36 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     L.tile_of = d_tile_of; L.err = h->d_lu_err; L.TJ = TJ; L.TK = TK;
     L.spin_limit = 4000000;  // x ~64 ns: a few hundred ms before a stuck wait gives up
     if (const char* sl = std::getenv("OCFD_LU_SPIN_LIMIT")) L.spin_limit = std::max(0LL, std::atoll(sl));
+    // version-5 records for the 64-column table: tiles in block order and their first records
+    if (v == 1 && !h->part && !std::getenv("OCFD_NO_LU5")) {
+      std::vector<LuTile> tmy(first);
+      std::vector<long long> rec0(first + 1, 0);
+      for (int b = 0; b < nblk; b++) {
+        const BlkD& B = h->blk[b];
+        const int nJ = tile_of[3 * b + 1], nK = tile_of[3 * b + 2];
+        for (int K = 0; K < nK; K++)
+          for (int J = 0; J < nJ; J++) {
+            const int q = tile_of[3 * b] + J + nJ * K;
+            tmy[q] = LuTile{b, 1 + J * TJ, 1 + K * TK, 0};
+            rec0[q + 1] = (B.nx - 1 + TJ + TK - 2) + 2;
+          }
+      }
+      for (int q = 0; q < first; q++) rec0[q + 1] += rec0[q];
+      LuStream& S = h->lus;
+      lu5_layout_for(h->prec, NV, S, TJ * TK, (TJ + 2) * (TK + 2));
+      const long long nrec = rec0[first];
+      LuTile* d_tmy = M.alloc<LuTile>(tmy.size(), e);
+      long long* d_rec0 = M.alloc<long long>(rec0.size(), e);
+      S.dyn = M.alloc<unsigned char>((size_t)nrec * S.dyn_bytes, e);
+      S.geo = M.alloc<unsigned char>((size_t)nrec * S.geo_bytes, e);
+      S.dus = (double*)M.alloc<unsigned char>((size_t)nrec * S.dus_bytes, e);
+      if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "lu records"); }
+      cudaMemcpy(d_tmy, tmy.data(), tmy.size() * sizeof(LuTile), cudaMemcpyHostToDevice);
+      cudaMemcpy(d_rec0, rec0.data(), rec0.size() * sizeof(long long), cudaMemcpyHostToDevice);
+      S.tmy = d_tmy;
+      S.rec0 = d_rec0;
+      h->lus_v = 1;
+    }
   }
   // ---- runner
   h->info.nvar = NV; h->info.time_method = p->time_method; h->info.viscous = p->if_viscous; h->info.turb = turb;
@@ -920,15 +983,17 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   else fill_arena<double>(h, h->A64, h->d_Md, h->d_vold, h->d_dtmd, h->d_dwd);
   // LU-SGS kernel candidates: OCFD_LU_TC fixes the tile width, OCFD_LU_V3 / OCFD_LU_V4 the
   // wavefront version (OCFD_LU_V2 both); the autotuner picks among the rest
-  const int lu_ver_force = lu_v2 ? 2 : (std::getenv("OCFD_LU_V3") ? 3 : (std::getenv("OCFD_LU_V4") ? 4 : 0));
+  const int lu_ver_force = lu_v2 ? 2 : (std::getenv("OCFD_LU_V3") ? 3 : (std::getenv("OCFD_LU_V4") ? 4 : (std::getenv("OCFD_LU_V5") ? 5 : 0)));
   std::vector<std::pair<int, int>> lu_cand;
   for (int v = 0; v < 2; v++) {
     if (lu_force && (lu_force == 64) != (v == 1)) continue;
-    for (int ver : {4, 3}) {
+    for (int ver : {5, 4, 3}) {
       if (lu_ver_force && ver != lu_ver_force) continue;
+      if (ver == 5 && (h->lus_v != v || lu_ver_force != 5)) continue;
       lu_cand.push_back({v, ver});
     }
   }
+  if (lu_cand.empty()) lu_cand.push_back({1, 4});
   if (lu_ver_force == 2) lu_cand.assign(1, {1, 2});
   select_lu(h, lu_cand[0].first, lu_cand[0].second);
   if (!h->run) { M.release(); return OCFD_ERR_UNSUPPORTED; }
@@ -1190,6 +1255,19 @@ extern "C" long long ocfd_footprint(const ocfd_params* p, int nblk, const int* n
   if (tm == 3) bytes += ts * (2 * tb + tf);
   if (p->precision == OCFD_PREC_MIXED) bytes += 4 * (M_COUNT * tf + 3 * tc);
   bytes += NV * maxbox * 8;                                                       // state staging
+  if (!std::getenv("OCFD_NO_LU5")) {                                              // LU-SGS version-5 records
+    int min_nzm = 1 << 30;
+    for (int b = 0; b < nblk; b++) min_nzm = std::min(min_nzm, nijk[3 * b + 2] - 1);
+    const int TK = min_nzm <= 2 ? 2 : (min_nzm <= 4 ? 4 : 8), TJ = 64 / TK;
+    LuStream S{};
+    lu5_layout_for(p->precision, (int)NV, S, 64, (TJ + 2) * (TK + 2));
+    long long nrec = 0;
+    for (int b = 0; b < nblk; b++) {
+      const long long nJ = (nijk[3 * b + 1] - 1 + TJ - 1) / TJ, nK = (nijk[3 * b + 2] - 1 + TK - 1) / TK;
+      nrec += nJ * nK * (nijk[3 * b] - 1 + TJ + TK);
+    }
+    bytes += nrec * (S.dyn_bytes + S.geo_bytes + S.dus_bytes);
+  }
   return bytes + bytes / 20 + (16LL << 20);                                       // tables, chunks, margin
 }
 

@@ -1,6 +1,7 @@
 // Kernel sequencing of one time step, templated on the flux precision T and NVAR.
 #pragma once
 #include "lusgs.cuh"
+#include "lusgs5.cuh"
 #include "runner.h"
 #include "solver.cuh"
 
@@ -42,6 +43,11 @@ class RunnerT : public Runner {
     lu_wave4_prepare<T, NV, true, 32>();
     lu_wave4_prepare<T, NV, false, 64>();
     lu_wave4_prepare<T, NV, true, 64>();
+    if (I.lus) {
+      S_ = *I.lus;
+      if (L_.TJ * L_.TK == 64) { lu_wave5_prepare<T, NV, false, 64>(S_); lu_wave5_prepare<T, NV, true, 64>(S_); }
+      else { lu_wave5_prepare<T, NV, false, 32>(S_); lu_wave5_prepare<T, NV, true, 32>(S_); }
+    }
   }
 
   void residual(cudaStream_t st, bool lusgs) override {
@@ -119,7 +125,18 @@ class RunnerT : public Runner {
     } else {
       if (!upper) cudaMemsetAsync(L_.counter, 0, 2 * sizeof(int), st);
       cudaMemsetAsync(L_.progress, 0, sizeof(int) * L_.ntiles, st);
-      if (I_.lu_version == 2) {
+      if (I_.lu_version == 5) {
+        const int TC = L_.TJ * L_.TK;
+        const int g = I_.lu5_grid[upper ? 1 : 0];
+        if (!upper) k_lu_pack_dyn<T, NV><<<dim3(8, L_.ntiles), 256, 0, st>>>(A, S_, L_.TJ, L_.TK);
+        if (TC == 64) {
+          if (!upper) k_lusgs_wave5<T, NV, false, 64><<<g, 4 * 64 + 32, lu5_smem<T, NV, 64>(S_, false), st>>>(A, L_, S_);
+          else k_lusgs_wave5<T, NV, true, 64><<<g, 4 * 64 + 32, lu5_smem<T, NV, 64>(S_, true), st>>>(A, L_, S_);
+        } else {
+          if (!upper) k_lusgs_wave5<T, NV, false, 32><<<g, 4 * 32 + 32, lu5_smem<T, NV, 32>(S_, false), st>>>(A, L_, S_);
+          else k_lusgs_wave5<T, NV, true, 32><<<g, 4 * 32 + 32, lu5_smem<T, NV, 32>(S_, true), st>>>(A, L_, S_);
+        }
+      } else if (I_.lu_version == 2) {
         if (!upper) k_lusgs_wave<T, NV, false><<<I_.lu_grid, 64, 0, st>>>(A, L_);
         else k_lusgs_wave<T, NV, true><<<I_.lu_grid, 64, 0, st>>>(A, L_);
       } else if (I_.lu_version == 4 && I_.lu_tc == 64) {
@@ -162,10 +179,10 @@ class RunnerT : public Runner {
   void limit(cudaStream_t st) {
     const Arena<T>& A = A_;
     k_limit_fix<T><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
-    if (NV == 6) {
+    if (NV == 6) {  // order: the cells above LSAmax first, then the clamp of all others
       k_sa_limit_check<T><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
+      k_sa_limit_serial<T><<<A.nblk, SAL_THREADS, 0, st>>>(A);
       k_sa_limit_par<T><<<grid_of(A.tot_cell), 256, 0, st>>>(A);
-      k_sa_limit_serial<T><<<A.nblk, 32, 0, st>>>(A);
     }
   }
 
@@ -231,7 +248,7 @@ class RunnerT : public Runner {
       if (I_.turb == 2) res += 6;
       else if (I_.turb == 3) res += 11;
     }
-    int lu = I_.lu_planes ? 2 * (I_.max_plane - 2) : 2;
+    int lu = I_.lu_planes ? 2 * (I_.max_plane - 2) : (I_.lu_version == 5 ? 3 : 2);
     int upd = 1 + 1 + (NV == 6 ? 3 : 0);
     int nbc = 0;
     for (int r = 0; r < I_.nround; r++) nbc += I_.bc_rounds[3 * r + 2] > 0;
@@ -243,6 +260,10 @@ class RunnerT : public Runner {
     else n = 1 + 3 * (res + upd + bch);
     if (NV >= 6) n += 1;
     return n;
+  }
+
+  void lu5_pack_geo(cudaStream_t st) override {
+    if (I_.lus) k_lu_pack_geo<T><<<dim3(8, L_.ntiles), 256, 0, st>>>(A_, S_, L_.TJ, L_.TK);
   }
 
   void dual_init(cudaStream_t st) override { k_dual_init<T, NV><<<grid_of((long long)NV * A_.tot_box), 256, 0, st>>>(A_); }
@@ -276,6 +297,7 @@ class RunnerT : public Runner {
   Arena<T> A_;
   RunInfo I_;
   LuArgs L_{};
+  LuStream S_{};
 };
 
 template <class T>

@@ -8,6 +8,7 @@
 namespace ocfd {
 
 struct LuArgs;
+struct LuStream;
 
 struct RunInfo {
   int nvar, time_method, viscous, turb;
@@ -17,7 +18,10 @@ struct RunInfo {
   int lu_planes;          // 1: one launch per hyperplane (reference order); 0: pipelined wavefront
   const LuArgs* lu;       // wavefront tables (host copy of the kernel argument)
   int lu_grid;            // CTAs of the wavefront kernel
-  int lu_version;         // 2: one thread per column; 3: four thread groups per column, staged by element; 4: staged by sector
+  int lu_version;         // 2: one thread per column; 3: four thread groups per column, staged by element; 4: staged by sector;
+                          // 5: inputs packed in sweep order, one bulk copy per step (lus)
+  const LuStream* lus;    // version 5: record layout and buffers (host copy of the kernel argument)
+  int lu5_grid[2];        // version 5: CTAs of the lower / upper sweep (resident CTAs, at most the tiles)
   int lu_tc;              // columns per tile (32 or 64)
   int recon_prim;         // 1: every solve reconstructs primitive variables
   int int_scheme;         // the interior scheme (Iflag_Scheme) if every solve uses the same one, else -1
@@ -70,6 +74,8 @@ class Runner {
   virtual void norms(cudaStream_t st, double* part, double* out, unsigned long long* nan_at) = 0;
   // force partial sums: 9 doubles per wall chunk
   virtual void forces(cudaStream_t st, double* part) = 0;
+  // version-5 LU-SGS: the static geometry records (once, after the geometry is computed)
+  virtual void lu5_pack_geo(cudaStream_t st) = 0;
   // AoS Fortran U(NV, box) of one block <-> device planes
   virtual void scatter_state(cudaStream_t st, int blk, const double* aos, long long box_b) = 0;
   virtual void gather_state(cudaStream_t st, int blk, double* aos, long long box_b) = 0;

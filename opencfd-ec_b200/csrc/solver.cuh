@@ -1165,9 +1165,15 @@ __global__ void k_limit_fix(Arena<T> A) {
   }
 }
 
-// limit_flow_SA (sub_limitflow.f90:182-231): the averaging branch depends on the serial loop order,
-// so a block with any U6 > LSAmax is done by one thread in that order; otherwise the clamp to SAmin
-// is pointwise.
+// limit_flow_SA (sub_limitflow.f90:182-231).  The reference visits the interior cells in (k, j, i)
+// order and limits each in place: U6 < SAmin becomes SAmin; U6 > LSAmax becomes the average of the
+// 3x3x3 neighbours whose value lies in [SAmin, LSAmax] at that moment (LSAmax if none).  So a
+// neighbour earlier in the order holds its limited value and a later one its original value.
+// Every limited value is at least SAmin, and an earlier cell's limited value is max(v, SAmin) of
+// what it holds in the array before the clamp pass, whether it was above LSAmax (replaced by an
+// average in [SAmin, LSAmax]) or not.  That makes the order matter only among the cells above
+// LSAmax, which k_sa_limit_serial visits in order (reading earlier neighbours as max(v, SAmin) and
+// later ones as they are); k_sa_limit_par then clamps every other cell to SAmin in parallel.
 template <class T>
 __global__ void k_sa_limit_check(Arena<T> A) {
   const long long tb = A.tot_box;
@@ -1184,7 +1190,6 @@ __global__ void k_sa_limit_par(Arena<T> A) {
   const long long tb = A.tot_box;
   OCFD_GRID_STRIDE(g, A.tot_cell) {
     int b = find_blk_h(A.pre_cell, A.hint_cell, A.nblk, g);
-    if (A.flags[2 * A.nblk + b] != 0) continue;
     const BlkD& B = A.blk[b];
     if (A.sp[B.solve].limit_flow != 1) continue;
     int i, j, k;
@@ -1193,33 +1198,68 @@ __global__ void k_sa_limit_par(Arena<T> A) {
     if (A.U[c] < 1.e-8) A.U[c] = 1.e-8;
   }
 }
+// one CTA per block with a cell above LSAmax: the block is scanned in chunks of SAL_CHUNK cells in
+// the reference's order (warp ballots find the chunk's cells above LSAmax), and thread 0 replaces
+// those cells, in order, by the average of their neighbours
+constexpr int SAL_THREADS = 512, SAL_PER = 8, SAL_CHUNK = SAL_THREADS * SAL_PER;
 template <class T>
-__global__ void k_sa_limit_serial(Arena<T> A) {
-  int b = blockIdx.x;
-  if (threadIdx.x != 0 || b >= A.nblk || A.flags[2 * A.nblk + b] == 0) return;
+__global__ void __launch_bounds__(SAL_THREADS) k_sa_limit_serial(Arena<T> A) {
+  __shared__ unsigned s_bad[SAL_CHUNK / 32];
+  const int b = blockIdx.x;
+  if (b >= A.nblk || A.flags[2 * A.nblk + b] == 0) return;   // the same for every thread of the CTA
   const BlkD& B = A.blk[b];
   const double SAmin = 1.e-8, LSAmax = A.sp[B.solve].lsamax;
   double* U6 = A.U + 5 * A.tot_box;
-  for (int k = 1; k <= B.nz - 1; k++)
-    for (int j = 1; j <= B.ny - 1; j++)
-      for (int i = 1; i <= B.nx - 1; i++) {
-        long long c = bix(B, i, j, k);
-        if (U6[c] < SAmin) U6[c] = SAmin;
-        if (U6[c] > LSAmax) {
+  const int nxm = B.nx - 1, nym = B.ny - 1, nzm = B.nz - 1;
+  const long long ncl = (long long)nxm * nym * nzm;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  auto cell = [&](long long l, int& i, int& j, int& k) {
+    const unsigned u = (unsigned)l, t = u / (unsigned)nxm;
+    i = (int)(u - t * (unsigned)nxm) + 1; j = (int)(t % (unsigned)nym) + 1; k = (int)(t / (unsigned)nym) + 1;
+  };
+  for (long long base = 0; base < ncl; base += SAL_CHUNK) {
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < SAL_PER; q++) {
+      const long long l = base + q * SAL_THREADS + tid;   // word (q * SAL_THREADS + tid) / 32 = q * 16 + warp
+      bool bad = false;
+      if (l < ncl) {
+        int i, j, k;
+        cell(l, i, j, k);
+        bad = U6[bix(B, i, j, k)] > LSAmax;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, bad);
+      if (lane == 0) s_bad[q * (SAL_THREADS / 32) + warp] = m;
+      any |= bad;
+    }
+    if (__syncthreads_or(any) && tid == 0) {
+      for (int w = 0; w < SAL_CHUNK / 32; w++) {
+        unsigned m = s_bad[w];
+        while (m) {
+          const int bit = __ffs(m) - 1;
+          m &= m - 1;
+          const long long l = base + w * 32 + bit;
+          int i, j, k;
+          cell(l, i, j, k);
           double s0 = 0.0;
           int kn = 0;
           for (int ka = -1; ka <= 1; ka++)
             for (int ja = -1; ja <= 1; ja++)
               for (int ia = -1; ia <= 1; ia++) {
-                int k1 = k + ka, j1 = j + ja, i1 = i + ia;
+                const int k1 = k + ka, j1 = j + ja, i1 = i + ia;
                 if (i1 > 0 && i1 < B.nx && j1 > 0 && j1 < B.ny && k1 > 0 && k1 < B.nz) {
+                  const long long l1 = (long long)(i1 - 1) + (long long)nxm * ((j1 - 1) + (long long)nym * (k1 - 1));
                   double q = U6[bix(B, i1, j1, k1)];
+                  if (l1 < l && q < SAmin) q = SAmin;   // an earlier cell holds its limited value
                   if (q >= SAmin && q <= LSAmax) { s0 = s0 + q; kn++; }
                 }
               }
-          U6[c] = kn == 0 ? LSAmax : s0 / kn;
+          U6[bix(B, i, j, k)] = kn == 0 ? LSAmax : s0 / kn;
         }
       }
+    }
+    __syncthreads();   // this chunk's averages are written before the next chunk's scan reads them
+  }
 }
 
 // force_vt_kw (sub_time_advance.f90:27-61)

@@ -4,9 +4,13 @@ committed histories (tests/golden/history_*.npz, written by tests/golden/make_hi
 Config 1 (the channel bump, 131,072 cells, MUSCL3 + Roe, LU-SGS CFL 5) is compared over its
 full 2000 iterations, as Residual.dat and force.log would record them: every iteration's residual
 norms within 1e-10 relative and CL / CD within 1e-10 relative (plus 1e-14 absolute), and the final
-state's checksums.
-The first iteration that leaves the tolerance, if any, is named in the failure message.  Two SA
-cases (an airfoil over 600 iterations, the 8-block wing over 200) cover the turbulence path.
+state's checksums.  The first iteration that leaves the tolerance, if any, is named in the failure
+message.  Two SA cases (an airfoil over 600 iterations, the 8-block wing over 200) cover the
+turbulence path with the same bounds, except the max norm of the SA cases at 1e-9: the SA source
+evaluates exp and pow (the ft2 and fw functions, sub_turbulence_SA.f90:188-249), whose CUDA and
+C-library results may differ in the last unit, and the max norm, one cell's value, magnifies that
+more than the RMS (measured: 2.2e-10 on the airfoil after 540 iterations, RMS 1.7e-11).  Euler has
+only additions, products, divisions and square roots, correctly rounded on both sides.
 """
 import os
 
@@ -18,6 +22,7 @@ from conftest import GOLDEN
 pytestmark = pytest.mark.gpu
 
 RTOL = 1e-10
+RTOL_MAX = {"config1": 1e-10, "foil_sa": 1e-9, "wing8_sa": 1e-9}
 
 
 def first_bad(got, ref, rtol, atol=0.0):
@@ -41,8 +46,8 @@ def test_history_matches_oracle(gpu, name):
     nv = p.nvar
     k = first_bad(rrms[:, :nv], gd["res_rms"][:, :nv], RTOL)
     assert k is None, "res_rms leaves %.0e at iteration %d: %s vs %s" % (RTOL, k + 1, rrms[k, :nv], gd["res_rms"][k, :nv])
-    k = first_bad(rmax[:, :nv], gd["res_max"][:, :nv], RTOL)
-    assert k is None, "res_max leaves %.0e at iteration %d" % (RTOL, k + 1)
+    k = first_bad(rmax[:, :nv], gd["res_max"][:, :nv], RTOL_MAX[name])
+    assert k is None, "res_max leaves %.0e at iteration %d" % (RTOL_MAX[name], k + 1)
     # CL / CD: config 1's pass through ~2e-6 (a symmetric bump at AoA 0), where the wall sums'
     # order alone moves the last bits of O(1) terms; hence the absolute floor
     k = first_bad(coef[:, :2], gd["clcdcs"][:, :2], RTOL, 1e-14)

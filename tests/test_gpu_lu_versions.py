@@ -1,8 +1,9 @@
 """Every LU-SGS wavefront variant gives the hyperplane-order bits.
 
 The creation-time autotuner picks a tile width (32 or 64 columns) and a wavefront kernel version
-(3: inputs staged by element; 4: staged by 32-byte sector, helper warps off the step phases) per
-case; the choice must never change a result.  Each variant is forced here through its switches and
+(3: inputs staged by element; 4: staged by 32-byte sector, helper warps off the step phases; 5:
+inputs packed in sweep order and fetched by one bulk copy per step, 64-column tiles) per case; the
+choice must never change a result.  Each variant is forced here through its switches and
 compared bit for bit with the one-launch-per-hyperplane sweep (OCFD_LUSGS_PLANES=1), on cases that
 cover NV = 5, 6 and 7, dual time, block edges that cut tiles, blocks thinner than a tile, and both
 precisions (in the mixed form the wavefront's flux difference is FP32 while the hyperplane form's
@@ -15,7 +16,8 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SWITCHES = ("OCFD_LU_V3", "OCFD_LU_V4", "OCFD_LU_TC", "OCFD_LUSGS_PLANES", "OCFD_NO_AUTOTUNE")
+SWITCHES = ("OCFD_LU_V3", "OCFD_LU_V4", "OCFD_LU_V5", "OCFD_LU_TC", "OCFD_LUSGS_PLANES", "OCFD_NO_AUTOTUNE")
+VARIANTS = (("3", "32"), ("3", "64"), ("4", "32"), ("4", "64"), ("5", "64"))
 
 
 def run(gpu, p, case, env, nsteps):
@@ -66,35 +68,44 @@ NAMES = ["config2_small_sa", "config3_small_sst", "config1_euler_2blk", "config2
 def test_every_wavefront_variant_equals_hyperplanes(gpu, name):
     p, case = case_list()[name]
     refU, refDU, _, _ = run(gpu, p, case, {"OCFD_LUSGS_PLANES": "1"}, 3)
-    for ver in ("3", "4"):
-        for tc in ("32", "64"):
-            U, DU, v, t = run(gpu, p, case, {"OCFD_LU_V" + ver: "1", "OCFD_LU_TC": tc}, 3)
-            assert (v, t) == (int(ver), int(tc))
-            assert bits_equal(U, refU), (name, ver, tc)
-            assert bits_equal(DU, refDU), (name, ver, tc)
+    for ver, tc in VARIANTS:
+        U, DU, v, t = run(gpu, p, case, {"OCFD_LU_V" + ver: "1", "OCFD_LU_TC": tc}, 3)
+        assert (v, t) == (int(ver), int(tc))
+        assert bits_equal(U, refU), (name, ver, tc)
+        assert bits_equal(DU, refDU), (name, ver, tc)
 
 
 @pytest.mark.parametrize("name", ["config2_small_sa", "config3_small_sst"])
 def test_mixed_wavefront_versions_agree(gpu, name):
+    """Versions 3 and 4 agree bit for bit in the mixed form.  Version 5's mixed form takes the
+    off-diagonal products in FP32 and multiplies by the diagonal's FP64 reciprocal (the north star
+    keeps only the diagonal inverse and the accumulation in FP64), and the compiler may contract
+    its FP32 operations differently: the FP32 flux difference F(U+DU) - F(U) is a cancellation
+    that keeps ~1e-4 of DU's digits, so the state after three steps agrees to 1e-5 of each
+    variable's scale (the converged state, where Res = 0, does not depend on the sweep's
+    rounding)."""
     p, case = case_list()[name]
     p = p.copy()
     p.precision = 1
     base = None
-    for ver in ("3", "4"):
-        for tc in ("32", "64"):
-            U, DU, v, t = run(gpu, p, case, {"OCFD_LU_V" + ver: "1", "OCFD_LU_TC": tc}, 3)
-            assert (v, t) == (int(ver), int(tc))
-            if base is None:
-                base = (U, DU)
-            else:
-                assert bits_equal(U, base[0]), (name, ver, tc)
-                assert bits_equal(DU, base[1]), (name, ver, tc)
+    for ver, tc in VARIANTS:
+        U, DU, v, t = run(gpu, p, case, {"OCFD_LU_V" + ver: "1", "OCFD_LU_TC": tc}, 3)
+        assert (v, t) == (int(ver), int(tc))
+        if base is None:
+            base = (U, DU)
+        elif ver != "5":
+            assert bits_equal(U, base[0]), (name, ver, tc)
+            assert bits_equal(DU, base[1]), (name, ver, tc)
+        else:
+            for a, b in zip(U, base[0]):
+                scale = np.maximum(np.abs(b).max(axis=(0, 1, 2)), 1e-30)
+                assert (np.abs(a - b).max(axis=(0, 1, 2)) / scale).max() <= 1e-5, (name, ver, tc)
 
 
 def test_autotuner_picks_a_known_variant(gpu):
     from ocfd_b200 import cases
     p, case = cases.config2_small()
     _, _, v, t = run(gpu, p, case, {}, 1)
-    assert v in (3, 4) and t in (32, 64)
+    assert v in (3, 4, 5) and t in (32, 64)
     _, _, v, t = run(gpu, p, case, {"OCFD_NO_AUTOTUNE": "1"}, 1)
     assert (v, t) == (4, 32)

@@ -400,7 +400,7 @@ static void select_lu(ocfd_handle* h, int v, int ver) {
     for (int up = 0; up < 2; up++) {
       const long long ring = (long long)h->lus.nstage * (h->lus.dyn_bytes + h->lus.geo_bytes + (up ? h->lus.dus_bytes : 0)) + 16 * h->lus.nstage;
       const long long per = ring + 40LL * h->nvar * TC + 16LL * TC + 2048;
-      const int occ = (int)std::max(1LL, std::min(233472LL / per, 2048LL / (4 * TC + 32)));
+      const int occ = (int)std::max(1LL, std::min(233472LL / (per + 1024), std::min(2LL, 2048LL / (4 * TC + 32))));
       h->info.lu5_grid[up] = std::max(1, std::min(h->lu.ntiles, h->nsm * occ));
     }
   }

@@ -66,10 +66,11 @@ inline void lu5_layout(LuStream& S, int TC, int E) {
   S.geo_bytes = o;
   S.dus_bytes = lu5_align16(8 * NV * TC);
   S.E = E;
-  // ring depth: as many stages as fit next to the kernel's static arrays in 227 KB (at least 4)
+  // ring depth: as many stages as fit next to the kernel's static arrays in half of the SM's
+  // 228 KB (two CTAs per SM: every tile of a 2 M-cell case resident at once), 4 at the least
   const int stat = (2 + 3) * NV * TC * 8 + 2 * TC * 8 + 16 + 1024;
   const int stg = S.dyn_bytes + S.geo_bytes + S.dus_bytes + 16;
-  S.nstage = (232448 - stat) / stg;
+  S.nstage = (233472 / 2 - 1024 - stat) / stg;
   if (S.nstage > 8) S.nstage = 8;
   if (S.nstage < 4) S.nstage = 4;
 }
@@ -212,6 +213,10 @@ __device__ __forceinline__ bool lu5_mbar_wait(uint64_t* bar, unsigned parity, lo
   return true;
 }
 
+// barrier 1 of the compute groups alone (warp-uniform callers; barrier 0 is __syncthreads)
+template <int NT>
+__device__ __forceinline__ void lu5_bar_compute() { asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory"); }
+
 template <class T, int NV, bool UPPER>
 __host__ __device__ inline int lu5_stage_bytes(const LuStream& S) { return S.dyn_bytes + S.geo_bytes + (UPPER ? S.dus_bytes : 0); }
 
@@ -230,7 +235,7 @@ constexpr size_t lu5_static_smem() { return (2 + 3) * NV * TC * 8 + 2 * TC * 8 +
 // variable d), then one helper warp.  Two CTA barriers per step: B1 (the previous step's DU is in
 // shared memory; a ring stage is free), B2 (the three terms and the diagonal are in shared memory).
 template <class T, int NV, bool UPPER, int TC>
-__global__ void __launch_bounds__(4 * TC + 32) k_lusgs_wave5(Arena<T> A, LuArgs L, LuStream S) {
+__global__ void __launch_bounds__(4 * TC + 32, 2) k_lusgs_wave5(Arena<T> A, LuArgs L, LuStream S) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   __shared__ double s_du[2][NV][TC];     // DU of each column's cell of the last two steps
   __shared__ double s_acc[3][NV][TC];    // the direction terms of the current step
@@ -344,13 +349,13 @@ __global__ void __launch_bounds__(4 * TC + 32) k_lusgs_wave5(Arena<T> A, LuArgs 
       }
       __syncthreads();   // B0
       for (int t = 0; t < nsteps; t++) {
-        __syncthreads();   // B1
+        __syncthreads();   // B1 (the compute groups' B2 is a named barrier without the helper, so
+                           // the release fence and the upstream wait below overlap their step)
         if (tid == HT) {
           if (t > 0) st_release(L.progress + my, t);
           issue(t + NS - 1);   // into the stage of load t-1, last read before B1
+          poll(t + 2);
         }
-        __syncthreads();   // B2
-        if (tid == HT) poll(t + 2);
       }
     } else if (grp == 3) {
       // ---- owner: diagonal (sub_LU_SGS.f90:29-39, 82-92), finish of variables 3..NV-1 ----
@@ -384,7 +389,7 @@ __global__ void __launch_bounds__(4 * TC + 32) k_lusgs_wave5(Arena<T> A, LuArgs 
           s_diag[0][c] = MIXED ? 1.0 / al : al;
           s_diag[1][c] = MIXED ? 1.0 / als : als;
         }
-        __syncthreads();   // B2
+        lu5_bar_compute<4 * TC>();   // B2
         if (on) {
           double r[NV];
 #pragma unroll
@@ -500,7 +505,7 @@ __global__ void __launch_bounds__(4 * TC + 32) k_lusgs_wave5(Arena<T> A, LuArgs 
 #pragma unroll
           for (int m = 0; m < NV; m++) s_acc[d][m][c] = 0.0;
         }
-        __syncthreads();   // B2: the terms and the diagonal of step t are in shared memory
+        lu5_bar_compute<4 * TC>();   // B2: the terms and the diagonal of step t are in shared memory
         if (on_at(t)) store(d, t, finish(d, t));
         if (t + 1 < nsteps) {
           if (on_at(t + 1) && !wait_rec(seq0 + t + 2)) atomicExch(L.err, 1);

@@ -52,8 +52,13 @@ def test_history_matches_oracle(gpu, name):
     # order alone moves the last bits of O(1) terms; hence the absolute floor
     k = first_bad(coef[:, :2], gd["clcdcs"][:, :2], RTOL, 1e-14)
     assert k is None, "CL/CD leave %.0e at iteration %d: %s vs %s" % (RTOL, k + 1, coef[k], gd["clcdcs"][k])
+    # final state: sums and sums of squares of each variable over each block's interior, against
+    # the largest of the block's sums of that kind (a nearly cancelling sum, like the w-momentum's,
+    # keeps only the absolute accuracy of the others)
     chk = np.stack([interior_checksums(g.get_state(b), case.dims[b]) for b in range(g.nblk)])
-    np.testing.assert_allclose(chk, gd["state_checksums"], rtol=1e-11, atol=1e-13)
+    ref = gd["state_checksums"]
+    scale = np.abs(ref).max(axis=2, keepdims=True)
+    assert np.all(np.abs(chk - ref) <= RTOL_MAX[name] * 0.1 * scale), np.abs(chk - ref).max() / scale.max()
     if name == "config1":   # the whole run of the configuration: the residual falls ~70x
         assert rrms[-1, 0] < 0.05 * rrms[0, 0]
     g.close()

@@ -906,7 +906,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     L.spin_limit = 4000000;  // x ~64 ns: a few hundred ms before a stuck wait gives up
     if (const char* sl = std::getenv("OCFD_LU_SPIN_LIMIT")) L.spin_limit = std::max(0LL, std::atoll(sl));
     // version-5 records for the 64-column table: tiles in block order and their first records
-    if (v == 1 && !h->part && !std::getenv("OCFD_NO_LU5")) {
+    if (v == 1 && !h->part && std::getenv("OCFD_LU_V5")) {
       std::vector<LuTile> tmy(first);
       std::vector<long long> rec0(first + 1, 0);
       for (int b = 0; b < nblk; b++) {
@@ -1255,7 +1255,7 @@ extern "C" long long ocfd_footprint(const ocfd_params* p, int nblk, const int* n
   if (tm == 3) bytes += ts * (2 * tb + tf);
   if (p->precision == OCFD_PREC_MIXED) bytes += 4 * (M_COUNT * tf + 3 * tc);
   bytes += NV * maxbox * 8;                                                       // state staging
-  if (!std::getenv("OCFD_NO_LU5")) {                                              // LU-SGS version-5 records
+  if (std::getenv("OCFD_LU_V5")) {                                                // LU-SGS version-5 records
     int min_nzm = 1 << 30;
     for (int b = 0; b < nblk; b++) min_nzm = std::min(min_nzm, nijk[3 * b + 2] - 1);
     const int TK = min_nzm <= 2 ? 2 : (min_nzm <= 4 ? 4 : 8), TJ = 64 / TK;

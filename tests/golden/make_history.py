@@ -15,6 +15,9 @@ Runs:
                CFL 5, inviscid, 2000 iterations: the whole run of the configuration
   foil_sa      SA airfoil 65x17 (WENO5 + Roe, LU-SGS), 600 iterations
   wing8_sa     the reduced swept wing (8 blocks, SA, WENO5 + Roe), 200 iterations
+  foil_sst_rk3 SST airfoil 65x17 (MUSCL3 + HLLC), three-stage RK3 at CFL 1.0, 300 steps
+  bump_dual    the channel bump at a quarter size, dual time (dt 0.2, 3 inner LU-SGS iterations
+               per physical step), 60 physical steps
 """
 import os
 import sys
@@ -36,6 +39,10 @@ def runs():
         "config1": (lambda: cases.config1(), 2000),
         "foil_sa": (lambda: cases.airfoil(ni=65, nj=17, scheme=7, flux=4, turb=2), 600),
         "wing8_sa": (lambda: cases.config2_small(), 200),
+        "foil_sst_rk3": (lambda: cases.airfoil(ni=65, nj=17, scheme=5, flux=3, turb=3, time_method=3, cfl=1.0,
+                                               kt_inf=1e-8, wt_inf=1e-5), 300),
+        "bump_dual": (lambda: cases.config1(scale=0.25, time_method=-1, dt_global=0.2, step_inner_limit=3,
+                                            res_inner_limit=1e-14), 60),
     }
 
 

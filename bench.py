@@ -115,13 +115,31 @@ def rank_aoa(rank):
     return 3.0 + 0.25 * rank
 
 
-WORKLOADS = ("config2", "config2_medium", "config1")
+WORKLOADS = ("config2", "config2_medium", "config1", "config4")
+
+
+class BatchItems:
+    """The 64 config-4 airfoils as one workload (one batch handle)."""
+
+    def __init__(self, items):
+        self.items = items
+        self.name = "config4_64_naca_airfoils"
+        self.dims = [d for _, c in items for d in c.dims]
+        self.ncells = sum(c.ncells for _, c in items)
 
 
 def make_case(args, rank):
     from ocfd_b200 import cases
     prec = 1 if args.precision == "mixed" else 0
+    if args.workload == "config4":
+        items = cases.config4_batch(n=64, precision=prec)
+        return items[0][0], BatchItems(items)
     return getattr(cases, args.workload)(precision=prec, aoa=rank_aoa(rank))
+
+
+def open_solver(p, case):
+    from ocfd_b200 import capi
+    return capi.Batch(case.items) if isinstance(case, BatchItems) else capi.Solver(p, case)
 
 
 def describe(p, case):
@@ -358,7 +376,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--workload", choices=WORKLOADS, default="config2",
-                    help="config2 (the headline case); the others are for profiler captures")
+                    help="config2 (the headline case); the others are for profiler captures (config4: the "
+                         "64-airfoil batch in one handle)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-extra", action="store_true", help="skip the mixed-precision, batch and serving legs")
@@ -386,7 +405,7 @@ def main():
         build.build()
 
     p, case = make_case(args, rank)
-    s = capi.Solver(p, case)
+    s = open_solver(p, case)
     stream = torch.cuda.ExternalStream(s.stream())
     s.advance(args.warmup)
     s.residual()

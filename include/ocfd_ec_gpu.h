@@ -230,6 +230,18 @@ int ocfd_residual_all(ocfd_handle* h, double* res_max, double* res_rms);
 /* ocfd_forces for every solve: ft holds 9*nsolve doubles, cl / cd / cs nsolve each (may be
  * NULL); each solve uses its own Ref_S, Ref_L, AoA and Cood_Y_UP. */
 int ocfd_forces_all(ocfd_handle* h, double* ft, double* cl, double* cd, double* cs);
+/*
+ * Solve q of a batch starts over with new parameters on its own mesh (a new Mach number, angle,
+ * Reynolds number, CFL, scheme, ...; the same NVAR, if_viscous, time_method and precision as the
+ * other solves, OCFD_ERR_ARG otherwise): its constants are replaced, the arrays that carry history
+ * between steps (mu, mu_t, the SST k / omega planes, the limiter flags) return to their state
+ * after allocation, and its flow is set to the new freestream with BC, halo and corners on its
+ * blocks, exactly as a new handle holding this case alone starts.  The other solves keep their
+ * state, and the next ocfd_advance steps all of them together (the captured step graph stays
+ * valid).  This is how a serving loop admits a new request into a free slot of a running batch.
+ * Not for sharded handles or dual time (OCFD_ERR_UNSUPPORTED).  Synchronous.
+ */
+int ocfd_reset_solve(ocfd_handle* h, int q, const ocfd_params* p);
 /* Upper estimate of the device bytes ocfd_create would allocate for these blocks and
  * parameters (admission control by HBM footprint); -1 on bad arguments.  No device call. */
 long long ocfd_footprint(const ocfd_params* p, int nblk, const int* nijk);

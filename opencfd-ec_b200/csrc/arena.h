@@ -116,6 +116,9 @@ struct Arena {
   T* Fv;       // viscous face fluxes: plane dir*4+(m-1), m = 1..4 for Res(2..5); boundary entries are Surf1..6
   T* Ft;       // turbulence face fluxes: plane dir*2+q
   int* flags;  // 4 planes of nblk ints: IF_OverLimit, limited-cell count, SA above LSAmax, BC error
+  // -1: kernels cover every solve; q >= 0: the initialisation, BC, halo and corner kernels touch
+  // only solve q's blocks (a solve of a batch re-initialised while the others keep their state)
+  int only_solve;
 };
 
 }  // namespace ocfd

@@ -323,6 +323,7 @@ static void fill_arena(ocfd_handle* h, Arena<T>& A, const T* M, const T* vol, co
   A.U = h->d_U; A.Un = h->d_Un; A.Un1 = h->d_Un1; A.sfac = h->d_sfac; A.P = (T*)h->d_P; A.mu = (T*)h->d_mu; A.mut = (T*)h->d_mut; A.Kt = (T*)h->d_Kt; A.Wt = (T*)h->d_Wt;
   A.f1 = (T*)h->d_f1; A.Res = (T*)h->d_Res; A.DU = h->d_DU; A.dt = (T*)h->d_dt; A.Lc = (T*)h->d_Lc; A.Lv = (T*)h->d_Lv;
   A.Fi = (T*)h->d_Fi; A.Fv = (T*)h->d_Fv; A.Ft = (T*)h->d_Ft; A.flags = h->d_flags;
+  A.only_solve = -1;
 }
 
 template <class T>
@@ -1319,6 +1320,43 @@ extern "C" int ocfd_get_state(ocfd_handle* h, int b, double* U) {
   cudaError_t e = cudaMemcpyAsync(U, h->d_stage, (size_t)h->nvar * box * 8, cudaMemcpyDeviceToHost, h->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "get_state");
+  return OCFD_OK;
+}
+
+// a slot of a batch given a new case on the same mesh: the solve's constants, its arrays that carry
+// history from step to step (mu and mu_t with their never-recomputed edge ghosts, the SST k, omega
+// and f1 planes, the limiter flags) back to their state after allocation, then freestream, BC,
+// halo and corners on its blocks; the other solves and the captured step graph are untouched
+extern "C" int ocfd_reset_solve(ocfd_handle* h, int q, const ocfd_params* p) {
+  if (!h || !p || q < 0 || q >= h->nsolve) return OCFD_ERR_ARG;
+  if (h->part) return fail(h, OCFD_ERR_UNSUPPORTED, "reset_solve: not for sharded handles");
+  if (p->time_method == -1) return fail(h, OCFD_ERR_UNSUPPORTED, "reset_solve: dual time keeps per-handle history (use a new handle)");
+  std::vector<ocfd_params> ps = h->Ps;
+  ps[q] = *p;
+  if (int rc = check_params(ps.data(), h->nsolve)) return fail(h, rc, "reset_solve: parameters incompatible with the handle's other solves");
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "reset_solve");
+  h->Ps[q] = *p;
+  fill_solve(*p, h->nvar, h->sps[q]);
+  const int b0 = h->sblk0[q], b1 = h->sblk0[q + 1];
+  const long long x0 = h->pre_box[b0], x1 = h->pre_box[b1], f0 = h->pre_face[b0], f1 = h->pre_face[b1];
+  const size_t ts = h->prec == OCFD_PREC_MIXED ? sizeof(float) : sizeof(double);
+  std::vector<char> mu((size_t)(x1 - x0) * ts);
+  for (long long l = 0; l < x1 - x0; l++) {
+    if (ts == 4) ((float*)mu.data())[l] = (float)(1.0 / p->re);
+    else ((double*)mu.data())[l] = 1.0 / p->re;
+  }
+  if (!e) e = cudaMemcpy(h->d_sp + q, &h->sps[q], sizeof(SolveP), cudaMemcpyHostToDevice);
+  if (!e) e = cudaMemcpy((char*)h->d_mu + x0 * ts, mu.data(), mu.size(), cudaMemcpyHostToDevice);
+  if (!e) e = cudaMemset((char*)h->d_mut + x0 * ts, 0, (x1 - x0) * ts);
+  if (!e && h->d_Kt) e = cudaMemset((char*)h->d_Kt + x0 * ts, 0, (x1 - x0) * ts);
+  if (!e && h->d_Wt) e = cudaMemset((char*)h->d_Wt + x0 * ts, 0, (x1 - x0) * ts);
+  if (!e && h->d_f1) e = cudaMemset((char*)h->d_f1 + f0 * ts, 0, (f1 - f0) * ts);
+  for (int pl = 0; pl < 4 && !e; pl++) e = cudaMemset(h->d_flags + pl * h->nblk + b0, 0, sizeof(int) * (b1 - b0));
+  if (e != cudaSuccess) return cuda_fail(h, e, "reset_solve");
+  h->run->reset_solve(h->st, q);
+  e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "reset_solve");
   return OCFD_OK;
 }
 

@@ -155,8 +155,17 @@ class RunnerT : public Runner {
     }
   }
 
-  void bc_halo(cudaStream_t st) override {
-    const Arena<T>& A = A_;
+  void bc_halo(cudaStream_t st) override { bc_halo_with(st, A_); }
+
+  // freestream + BC + halo + corners of solve q's blocks only (the other solves keep their state)
+  void reset_solve(cudaStream_t st, int q) override {
+    Arena<T> A = A_;
+    A.only_solve = q;
+    k_init_flow<T, NV><<<grid_of(A.tot_box), 256, 0, st>>>(A);
+    bc_halo_with(st, A);
+  }
+
+  void bc_halo_with(cudaStream_t st, const Arena<T>& A) {
     for (int r = 0; r < I_.nround; r++) {
       const int* R = I_.bc_rounds + 3 * r;
       if (R[2] > 0) k_bc_round<T, NV><<<grid_of(R[2]), 256, 0, st>>>(A, R[0], R[1], (long long)R[2]);

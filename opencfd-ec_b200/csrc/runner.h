@@ -70,6 +70,8 @@ class Runner {
   virtual void dual_end(cudaStream_t st) = 0;
   // BC + halo + corners only
   virtual void bc_halo(cudaStream_t st) = 0;
+  // freestream + BC + halo + corners of solve q's blocks only (a batch slot re-initialised)
+  virtual void reset_solve(cudaStream_t st, int q) = 0;
   // residual norms: 14 doubles per solve into out (max[7], sum of squares[7])
   virtual void norms(cudaStream_t st, double* part, double* out, unsigned long long* nan_at) = 0;
   // force partial sums: 9 doubles per wall chunk

@@ -1410,6 +1410,7 @@ __global__ void k_bc_round(Arena<T> A, int e0, int e1, long long ncell) {
     const int e = e0 + find_blk(A.bc_pre + e0, e1 - e0, gg);
     const SubD S = A.sub[A.bc_ent[e]];
     const BlkD& B = A.blk[S.blk];
+    if (A.only_solve >= 0 && B.solve != A.only_solve) continue;
     bc_cell<T, NV>(A, S, B, A.sp[B.solve], gg - A.bc_pre[e]);
   }
 }
@@ -1456,6 +1457,7 @@ __global__ void k_halo(Arena<T> A) {
   const long long tb = A.tot_box;
   OCFD_GRID_STRIDE(g, A.tot_halo) {
     int s = find_blk(A.pre_halo, A.nsub, g);
+    if (A.only_solve >= 0 && A.blk[A.sub[s].nb1].solve != A.only_solve) continue;
     long long cs, ct;
     halo_map(A, A.sub[s], g - A.pre_halo[s], cs, ct);
     double v[NV];  // all loads before the stores (a store in between would hold the next load back)
@@ -1475,6 +1477,7 @@ __global__ void k_halo_level(Arena<T> A, const int* ent, const long long* pre, i
   const long long tb = A.tot_box;
   OCFD_GRID_STRIDE(g, cells) {
     int e = e0 + find_blk(pre + e0, e1 - e0, g);
+    if (A.only_solve >= 0 && A.blk[A.sub[ent[e]].nb1].solve != A.only_solve) continue;
     long long cs, ct;
     halo_map(A, A.sub[ent[e]], g - pre[e], cs, ct);
     double v[NV];  // all loads before the stores
@@ -1533,6 +1536,7 @@ __global__ void k_corner(Arena<T> A) {  // edges: grid (blocks, CTAs per block)
   const int b = blockIdx.x;
   if (b >= A.nblk) return;
   const BlkD& B = A.blk[b];
+  if (A.only_solve >= 0 && B.solve != A.only_solve) return;
   const long long tb = A.tot_box;
   const int nx = B.nx, ny = B.ny, nz = B.nz;
   double* U = A.U;
@@ -1573,6 +1577,7 @@ __global__ void k_corner_vtx(Arena<T> A) {
   if (g >= (long long)A.nblk * NV * 8) return;
   const int b = (int)(g / (NV * 8));
   const BlkD& B = A.blk[b];
+  if (A.only_solve >= 0 && B.solve != A.only_solve) return;
   const int nx = B.nx, ny = B.ny, nz = B.nz;
   double* U = A.U;
   auto u = [&](int m, int i, int j, int k) -> double& { return U[m * tb + bix(B, i, j, k)]; };
@@ -1716,6 +1721,7 @@ __global__ void k_init_flow(Arena<T> A) {
   const long long tb = A.tot_box;
   OCFD_GRID_STRIDE(g, tb) {
     int b = find_blk_h(A.pre_box, A.hint_box, A.nblk, g);
+    if (A.only_solve >= 0 && A.blk[b].solve != A.only_solve) continue;
     const SolveP& s = A.sp[A.blk[b].solve];
     double d0 = 1.0, u0 = s.u_inf, v0 = s.v_inf, w0 = s.w_inf, p0 = 1.0 / (s.gamma * s.ma * s.ma);
     A.U[g] = d0; A.U[tb + g] = d0 * u0; A.U[2 * tb + g] = d0 * v0; A.U[3 * tb + g] = d0 * w0;

@@ -20,7 +20,7 @@ EXPORTED = [
     "ocfd_default_params", "ocfd_finalize_params", "ocfd_create", "ocfd_destroy", "ocfd_last_error", "ocfd_state_size",
     "ocfd_set_state", "ocfd_get_state", "ocfd_init_flow", "ocfd_advance", "ocfd_residual", "ocfd_forces",
     "ocfd_limiter_status", "ocfd_array_shape", "ocfd_get_array", "ocfd_version", "ocfd_compute_residual",
-    "ocfd_stream", "ocfd_profile", "ocfd_launches_per_step", "ocfd_create_batch", "ocfd_nsolve",
+    "ocfd_stream", "ocfd_profile", "ocfd_launches_per_step", "ocfd_create_batch", "ocfd_nsolve", "ocfd_reset_solve",
     "ocfd_residual_all", "ocfd_forces_all", "ocfd_footprint", "ocfd_synchronize", "ocfd_residual_static",
     "ocfd_lu_tile_width", "ocfd_lu_kernel_version", "ocfd_create_part", "ocfd_part_blocks", "ocfd_part_plan",
 ]
@@ -65,6 +65,7 @@ def lib():
         L.ocfd_launches_per_step.argtypes = [vp]
         L.ocfd_create_batch.argtypes = [pp, ctypes.c_int, ip, ip, ctypes.POINTER(dp), ip, ip, ctypes.POINTER(dp), ctypes.POINTER(vp)]
         L.ocfd_nsolve.argtypes = [vp]
+        L.ocfd_reset_solve.argtypes = [vp, ctypes.c_int, vp]
         L.ocfd_residual_all.argtypes = [vp, dp, dp]
         L.ocfd_forces_all.argtypes = [vp, dp, dp, dp, dp]
         L.ocfd_footprint.argtypes = [pp, ctypes.c_int, ip]
@@ -259,6 +260,10 @@ class Batch(Solver):
 
     def __init__(self, items, dw=None):
         self._create(list(items), dw)
+
+    def reset_solve(self, q, params):
+        """Solve q starts over with new parameters on its own mesh (ocfd_reset_solve)."""
+        self._check(lib().ocfd_reset_solve(self.h, int(q), ctypes.byref(params)), "reset_solve")
 
 
 def version():

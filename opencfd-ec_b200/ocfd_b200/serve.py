@@ -189,6 +189,142 @@ class Server:
         return sorted(results, key=lambda r: r.rid)
 
 
+def mesh_key(case):
+    """Identity of a request's mesh (block sizes and node coordinates): requests with the same key
+    can share the slots of one batch handle."""
+    import hashlib
+    h = hashlib.sha1()
+    for d, x in zip(case.dims, case.xyz):
+        h.update(np.asarray(d, dtype=np.int64).tobytes())
+        h.update(np.ascontiguousarray(x).tobytes())
+    return h.hexdigest()
+
+
+class _Pool:
+    """One batch handle whose solves are slots for requests on one mesh."""
+
+    def __init__(self, req, slots, admitted):
+        import torch
+        self.b = capi.Batch([(req.params, req.case)] * slots)
+        self.stream = torch.cuda.ExternalStream(self.b.stream())
+        self.req = [None] * slots           # the request in each slot (None: free)
+        self.iters = [0] * slots
+        self.rms0 = [None] * slots
+        self.cl_hist = [[] for _ in range(slots)]
+        self.admitted = [0.0] * slots
+        self.req[0] = req
+        self.admitted[0] = admitted
+        self.busy = False                   # a chunk is queued
+
+
+class SlotServer:
+    """Continuous batching inside batched steps: requests on the same mesh (Mach / AoA / Re
+    sweeps on one geometry) are admitted into free slots of one batch handle, whose step graph
+    advances all of them in the same launches; a new request takes a free slot through
+    ocfd_reset_solve while the other slots keep iterating.  A mesh seen for the first time gets
+    a handle of `slots` solves (admission by device footprint, as Server); idle slots are stepped
+    along with the others.  Every request is checked at the same points (every `chunk` of its
+    own iterations) with the same convergence tests as Server, so its result is the same alone
+    and in the mix (bit for bit)."""
+
+    def __init__(self, slots=8, chunk=50, hbm_budget: Optional[int] = None, drop: float = 1e-6, dcl: float = 1e-4,
+                 dcl_window: int = 200, clock=time.perf_counter):
+        self.slots, self.chunk, self.hbm_budget = slots, chunk, hbm_budget
+        self.drop, self.dcl, self.dcl_window = drop, dcl, dcl_window
+        self.clock = clock
+
+    def _check(self, P, q, rms, cl):
+        P.cl_hist[q].append((P.iters[q], cl))
+        if P.rms0[q] is None:
+            P.rms0[q] = rms[0]
+        if rms[0] <= self.drop * P.rms0[q]:
+            return "residual"
+        it, hist = P.iters[q], P.cl_hist[q]
+        old = [c for i, c in hist if i <= it - self.dcl_window]
+        if old and it >= self.dcl_window and abs(cl - old[-1]) < self.dcl and \
+                all(abs(cl - c) < self.dcl for i, c in hist if i >= it - self.dcl_window):
+            return "cl"
+        if it >= P.req[q].max_iters:
+            return "max_iters"
+        return None
+
+    def run(self, requests: List[Request]) -> List[Result]:
+        pending = sorted(requests, key=lambda r: r.arrival)
+        queue, results, pools, keys = [], [], {}, {}
+        budget = self.hbm_budget
+        if budget is None:
+            import torch
+            budget = int(torch.cuda.mem_get_info()[0] * 0.9)
+        used = 0
+        t0 = self.clock()
+
+        def finish(P, q, why, rms, cl, cd, err=""):
+            r = P.req[q]
+            results.append(Result(r.rid, r.case.ncells, r.arrival, P.admitted[q], self.clock() - t0, P.iters[q], why,
+                                  float("nan") if P.rms0[q] is None else float(P.rms0[q]), rms, cl, cd,
+                                  [c for _, c in P.cl_hist[q]], err))
+            P.req[q] = None
+
+        try:
+            while pending or queue or any(any(r is not None for r in P.req) for P in pools.values()):
+                now = self.clock() - t0
+                while pending and pending[0].arrival <= now:
+                    r = pending.pop(0)
+                    keys[r.rid] = mesh_key(r.case)
+                    queue.append(r)
+                # a mesh seen for the first time: a new handle of `slots` solves, by footprint
+                for r in list(queue):
+                    k = keys[r.rid]
+                    if k in pools:
+                        continue
+                    need = self.slots * capi.footprint(r.params, r.case)
+                    if used + need > budget:
+                        continue
+                    pools[k] = _Pool(r, self.slots, self.clock() - t0)
+                    used += need
+                    queue.remove(r)
+                progressed = False
+                for k, P in pools.items():
+                    if P.busy and not P.stream.query():
+                        continue
+                    if P.busy:   # a chunk has finished: read back and check every occupied slot
+                        progressed = True
+                        _, rms = P.b.residual_all()
+                        _, cl, cd, _ = P.b.forces_all()
+                        for q in range(self.slots):
+                            if P.req[q] is None:
+                                continue
+                            if not np.isfinite(rms[q][0]):
+                                finish(P, q, "error", rms[q].copy(), float("nan"), float("nan"), "NaN in the residual")
+                                continue
+                            why = self._check(P, q, rms[q], cl[q])
+                            if why is not None:
+                                finish(P, q, why, rms[q].copy(), float(cl[q]), float(cd[q]))
+                        P.busy = False
+                    # queued requests on this mesh take the free slots
+                    for r in list(queue):
+                        if keys[r.rid] != k or None not in P.req:
+                            continue
+                        q = P.req.index(None)
+                        P.b.reset_solve(q, r.params)
+                        P.req[q], P.iters[q], P.rms0[q], P.cl_hist[q] = r, 0, None, []
+                        P.admitted[q] = self.clock() - t0
+                        queue.remove(r)
+                    if any(r is not None for r in P.req):
+                        P.b.advance(self.chunk)
+                        for q in range(self.slots):
+                            if P.req[q] is not None:
+                                P.iters[q] += self.chunk
+                        P.busy = True
+                        progressed = True
+                if not progressed:
+                    time.sleep(0.0002)
+        finally:
+            for P in pools.values():
+                P.b.close()
+        return sorted(results, key=lambda r: r.rid)
+
+
 def poisson_requests(items, rate=2.0, seed=2024, max_iters=5000):
     """Requests for the given (params, case) items with exponential inter-arrival times."""
     rng = np.random.default_rng(seed)

@@ -82,3 +82,35 @@ def test_config4_batch_runs(gpu):
     _, cl, cd, _ = b.forces_all()
     assert np.all(np.isfinite(rrms)) and np.all(np.isfinite(cl)) and np.all(np.isfinite(cd))
     b.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_reset_solve_starts_over_like_a_new_handle(gpu, precision):
+    """ocfd_reset_solve: a slot of a running batch takes a new case on its mesh (other Mach, AoA,
+    Re); after it, that solve's states, norms and forces equal a new handle holding the case alone
+    bit for bit, and the other solve is exactly where it would be without the reset."""
+    from ocfd_b200 import cases
+    a = cases.airfoil(ni=65, nj=17, ma=0.6, aoa=1.0, precision=precision)
+    b = cases.airfoil(ni=81, nj=21, ma=0.7, aoa=2.5, m=0.03, precision=precision)
+    c = cases.airfoil(ni=81, nj=21, ma=0.5, aoa=4.0, m=0.03, re=3.0e6, precision=precision)   # b's mesh
+    assert all(np.array_equal(x, y) for x, y in zip(b[1].xyz, c[1].xyz))
+    bt = gpu.Batch([a, b])
+    bt.advance(30)
+    bt.reset_solve(1, c[0])
+    bt.advance(20)
+    alone = gpu.Solver(*c)
+    alone.advance(20)
+    nb0 = len(a[1].dims)
+    for k in range(alone.nblk):
+        assert np.array_equal(bt.get_state(nb0 + k), alone.get_state(k))
+    (mx, rm), (amx, arm) = bt.residual_all(), alone.residual()
+    assert np.array_equal(rm[1], arm) and np.array_equal(mx[1], amx)
+    ft, cl, cd, cs = bt.forces_all()
+    _, acl, acd, _ = alone.forces()
+    assert cl[1] == acl and cd[1] == acd
+    ref = gpu.Batch([a, b])
+    ref.advance(50)
+    for k in range(nb0):
+        assert np.array_equal(bt.get_state(k), ref.get_state(k))
+    for s in (bt, alone, ref):
+        s.close()

@@ -78,3 +78,27 @@ def test_failing_request_leaves_the_others_untouched(gpu):
         assert np.array_equal(alone.rms, r.rms) and alone.cl == r.cl and alone.cd == r.cd
     # every handle of the run was closed: the device memory is back
     assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
+
+
+def sweep_reqs(max_iters=300):
+    """Four Mach / AoA points on one airfoil mesh and one request on another mesh."""
+    from ocfd_b200 import cases
+    from ocfd_b200.serve import Request
+    its = [cases.airfoil(ni=65, nj=17, ma=ma, aoa=aoa, precision=1) for ma, aoa in ((0.5, 1.0), (0.6, 2.0), (0.7, 0.0), (0.55, 3.0))]
+    its.append(cases.airfoil(ni=81, nj=21, m=0.03, ma=0.6, aoa=1.5, precision=1))
+    arr = [0.0, 0.0, 0.05, 0.3, 0.1]
+    return [Request(q, p, c, arr[q], max_iters) for q, (p, c) in enumerate(its)]
+
+
+def test_slot_server_same_alone_and_in_the_mix(gpu):
+    """Continuous batching inside batched steps (SlotServer): with two slots per mesh, the third
+    and fourth requests on the first mesh wait for a slot and enter a running batch through
+    ocfd_reset_solve; every result equals the same request run alone, bit for bit."""
+    from ocfd_b200.serve import SlotServer
+    mix = SlotServer(slots=2, chunk=50).run(sweep_reqs())
+    assert len(mix) == 5 and all(r.converged != "error" for r in mix)
+    for r in mix:
+        alone = SlotServer(slots=2, chunk=50).run([x for x in sweep_reqs() if x.rid == r.rid])[0]
+        assert alone.iters == r.iters and alone.converged == r.converged
+        assert np.array_equal(alone.rms, r.rms)
+        assert alone.cl == r.cl and alone.cd == r.cd

@@ -358,6 +358,81 @@ def serving_leg(max_iters=5000, n=14, rate=2.0):
     return out
 
 
+def bench_config(p, case, prec, world):
+    """The `config` object of the JSON line, the same for both arms of one workload."""
+    return {"workload": describe(p, case), "cells": case.ncells, "blocks": len(case.dims), "precision": prec,
+            "parallelism": "replicas x%d (independent solves, no collective)" % world,
+            "l2": "working set %.1f GB > 126 MB L2 (no flush needed)" % (case.ncells * 1200 / 1e9)}
+
+
+
+def converged_leg(args):
+    """CL / CD / final-residual error of the mixed form against FP64 at convergence, per
+    configuration (1 count = 1e-4), and config 1's FP64 history against the oracle's.
+    config 2: both precisions over the configuration's 5000 iterations; config 4: the 64 airfoils
+    over 8000 iterations, errors over those whose FP64 CL moved < 0.1 count in the last 400;
+    config 3 (stand-in): 1000 iterations; config 1: the FP64 GPU run of 2000 iterations against
+    the committed history of the CPU restatement (tests/golden/history_config1.npz)."""
+    import numpy as np
+    from ocfd_b200 import capi, cases
+    out = {}
+
+    def final(p, case, n, chunk=500):
+        s = capi.Solver(p, case)
+        for _ in range(n // chunk):
+            s.advance(chunk)
+        _, cl, cd, _ = s.forces()
+        rms = s.residual()[1][0]
+        s.close()
+        return cl, cd, rms
+
+    for name, mk, n in (("config2", cases.config2, 5000), ("config3", cases.config3, 1000)):
+        a = final(*mk(precision=0), n)
+        b = final(*mk(precision=1), n)
+        out[name] = {"iterations": n, "cl_fp64": a[0], "cd_fp64": a[1], "dCL_counts": abs(b[0] - a[0]) * 1e4,
+                     "dCD_counts": abs(b[1] - a[1]) * 1e4, "rms_rho_fp64": a[2], "rms_rho_mixed": b[2],
+                     "rms_rel_err": abs(b[2] - a[2]) / a[2]}
+    hist = {}
+    for prec in (0, 1):
+        bt = capi.Batch(cases.config4_batch(n=64, precision=prec))
+        cl = []
+        for _ in range(40):
+            bt.advance(200)
+            cl.append(bt.forces_all())
+        bt.close()
+        hist[prec] = cl
+    cl64 = np.array([h[1] for h in hist[0]])
+    cd64 = np.array([h[2] for h in hist[0]])
+    cl32, cd32 = hist[1][-1][1], hist[1][-1][2]
+    settled = np.abs(cl64[-1] - cl64[-3]) < 1e-5
+    dcl, dcd = np.abs(cl32 - cl64[-1]) * 1e4, np.abs(cd32 - cd64[-1]) * 1e4
+    out["config4"] = {"iterations": 8000, "solves": 64, "settled": int(settled.sum()),
+                      "dCL_counts_settled_max": float(dcl[settled].max()) if settled.any() else None,
+                      "dCD_counts_settled_max": float(dcd[settled].max()) if settled.any() else None,
+                      "dCL_counts_all_median": float(np.median(dcl)), "dCL_counts_all_max": float(dcl.max()),
+                      "dCD_counts_all_max": float(dcd.max())}
+    gd = np.load(os.path.join(ROOT, "tests", "golden", "history_config1.npz"))
+    p, case = cases.config1()
+    s = capi.Solver(p, case)
+    rms, mx, co = [], [], []
+    for _ in range(int(gd["steps"])):
+        s.advance(1)
+        a, b = s.residual()
+        rms.append(b[:5])
+        mx.append(a[:5])
+        co.append(s.forces()[1:3])
+    s.close()
+    d_rms = np.abs(np.array(rms) - gd["res_rms"][:, :5]) / np.abs(gd["res_rms"][:, :5])
+    d_max = np.abs(np.array(mx) - gd["res_max"][:, :5]) / np.abs(gd["res_max"][:, :5])
+    d_co = np.abs(np.array(co) - gd["clcdcs"][:, :2])
+    bad = np.any(d_rms > 1e-10, axis=1) | np.any(d_max > 1e-10, axis=1)
+    out["config1_fp64_vs_oracle"] = {"iterations": int(gd["steps"]), "res_rms_max_rel": float(d_rms.max()),
+                                     "res_max_max_rel": float(d_max.max()), "clcd_max_abs": float(d_co.max()),
+                                     "first_iteration_beyond_1e-10": int(np.argmax(bad)) + 1 if bad.any() else None}
+    return out
+
+
+
 def run_reference(args, budget_s=150.0):
     """The reference arm: the CPU restatement of the reference algorithm (oracle/, FP64, all host
     threads) on the same workload, rank 0 only.  Times args.steps full steps, or as many as fit

@@ -501,8 +501,10 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
         al = al + sfac1 * vol;
         als = als + sfac1 * vol;
       }
-      s_diag[0][c] = al;
-      s_diag[1][c] = NV == 6 ? als : al;
+      // the mixed form multiplies by the diagonal's FP64 reciprocal (taken here, off the chain);
+      // the FP64 form divides as the reference does
+      s_diag[0][c] = sizeof(T) == 4 ? 1.0 / al : al;
+      s_diag[1][c] = sizeof(T) == 4 ? 1.0 / (NV == 6 ? als : al) : (NV == 6 ? als : al);
     };
 
     int seen_j = 0, seen_k = 0;
@@ -524,8 +526,13 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
     auto finish_val = [&](int m, int t) {  // sub_LU_SGS.f90:63-72 (lower), 108-117 (upper)
       const double rm = (double)R.oR[t % LU_RING][m][c];
       double r;
-      if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
-      else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      if (sizeof(T) == 4) {
+        if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) * diag_of(m);
+        else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) * diag_of(m);
+      } else {
+        if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+        else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      }
       return r;
     };
     auto finish = [&](int m, int t, long long ci) {
@@ -612,9 +619,18 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
 #pragma unroll
           for (int m = 0; m < NV; m++) {
             double v;
-            if (!UPPER) v = 0.5 * ((double)DF[m] * S + wLc * DUn[m]);
-            else v = -(0.5 * ((double)DF[m] * S - wLc * DUn[m]));
-            if (visc) v = v + Lvn * DUn[m];
+            if (sizeof(T) == 4) {   // the mixed form: off-diagonal products in FP32, the sum stays FP64
+              const float du = (float)DUn[m];
+              float x;
+              if (!UPPER) x = 0.5f * ((float)DF[m] * (float)S + (float)wLc * du);
+              else x = -(0.5f * ((float)DF[m] * (float)S - (float)wLc * du));
+              if (visc) x = x + (float)Lvn * du;
+              v = (double)x;
+            } else {
+              if (!UPPER) v = 0.5 * ((double)DF[m] * S + wLc * DUn[m]);
+              else v = -(0.5 * ((double)DF[m] * S - wLc * DUn[m]));
+              if (visc) v = v + Lvn * DUn[m];
+            }
             s_acc[d][m][c] = v;
           }
         } else if (on_at(t)) {
@@ -913,8 +929,10 @@ __global__ void __launch_bounds__(4 * TC + 64, OCFD_LU_MINB) k_lusgs_wave4(Arena
         al = al + sfac1 * vol;
         als = als + sfac1 * vol;
       }
-      s_diag[0][c] = al;
-      s_diag[1][c] = NV == 6 ? als : al;
+      // the mixed form multiplies by the diagonal's FP64 reciprocal (taken here, off the chain);
+      // the FP64 form divides as the reference does
+      s_diag[0][c] = sizeof(T) == 4 ? 1.0 / al : al;
+      s_diag[1][c] = sizeof(T) == 4 ? 1.0 / (NV == 6 ? als : al) : (NV == 6 ? als : al);
     };
 
     int seen_j = 0, seen_k = 0;
@@ -929,8 +947,13 @@ __global__ void __launch_bounds__(4 * TC + 64, OCFD_LU_MINB) k_lusgs_wave4(Arena
     auto finish_val = [&](int m, long long ci) {  // sub_LU_SGS.f90:63-72 (lower), 108-117 (upper)
       const double rm = (double)sec_get(obuf(SM::SR + m, c), CS, Rp(m, ci));
       double r;
-      if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
-      else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      if (sizeof(T) == 4) {
+        if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) * diag_of(m);
+        else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) * diag_of(m);
+      } else {
+        if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+        else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
+      }
       return r;
     };
     auto finish = [&](int m, long long ci) {
@@ -1016,9 +1039,18 @@ __global__ void __launch_bounds__(4 * TC + 64, OCFD_LU_MINB) k_lusgs_wave4(Arena
 #pragma unroll
           for (int m = 0; m < NV; m++) {
             double v;
-            if (!UPPER) v = 0.5 * ((double)DF[m] * S + wLc * DUn[m]);
-            else v = -(0.5 * ((double)DF[m] * S - wLc * DUn[m]));
-            if (visc) v = v + Lvn * DUn[m];
+            if (sizeof(T) == 4) {   // the mixed form: off-diagonal products in FP32, the sum stays FP64
+              const float du = (float)DUn[m];
+              float x;
+              if (!UPPER) x = 0.5f * ((float)DF[m] * (float)S + (float)wLc * du);
+              else x = -(0.5f * ((float)DF[m] * (float)S - (float)wLc * du));
+              if (visc) x = x + (float)Lvn * du;
+              v = (double)x;
+            } else {
+              if (!UPPER) v = 0.5 * ((double)DF[m] * S + wLc * DUn[m]);
+              else v = -(0.5 * ((double)DF[m] * S - wLc * DUn[m]));
+              if (visc) v = v + Lvn * DUn[m];
+            }
             s_acc[d][m][c] = v;
           }
         } else if (on_at(t)) {

@@ -204,3 +204,22 @@ def test_bench_bytes_model():
     tot = {k: sum(v.values()) for k, v in bench.BYTES.items()}
     assert tot[("fp64", 5)] == 760 and tot[("fp64", 6)] == 1192 and tot[("fp64", 7)] == 1256
     assert tot[("mixed", 5)] == 500 and tot[("mixed", 6)] == 740 and tot[("mixed", 7)] == 796
+
+
+def test_bench_reference_arm_runs_on_cpu():
+    """bench.py's reference arm (the CPU restatement on the host cores) prints its JSON line on a
+    small workload, and every leg the GPU arm calls is defined."""
+    import json
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", "config1",
+                          "--steps", "2", "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "cell-updates/s"
+    assert {"workload", "cells", "parallelism", "l2"} <= set(line["config"])
+    sys.path.insert(0, ROOT)
+    import bench
+    for name in ("mixed_leg", "batch_leg", "config3_leg", "serving_leg", "sweep_serving_leg", "converged_leg",
+                 "bench_config", "cpu_sample", "run_reference", "diverges_at", "open_solver", "make_case"):
+        assert callable(getattr(bench, name)), name

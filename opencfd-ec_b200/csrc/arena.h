@@ -22,6 +22,14 @@ struct BlkD {
   long long obci, obcj, obck;           // offsets of the physical-boundary flag arrays
   long long ocol;                        // offset in the (j,k) column space used by LU-SGS
   int sub0, nsub;                        // subface table range
+  // cells whose primitives a residual reads: 1-glo[d] .. n-1+ghi[d] in direction d (glo/ghi = 4,
+  // all LAP ghost layers, on a face with an interface cell; else the reach of the boundary scheme,
+  // at least 1), RX x RY x RZ cells from offset oreg of that index space; and the 0..n layer
+  // ((nx+1)(ny+1)(nz+1) cells) from offset or1
+  int glo[3], ghi[3];
+  int RX, RY, RZ;
+  long long oreg, or1;
+  int tdim[3];  // cells per residual tile in i, j, k (the last tile of a direction may be shorter)
 };
 
 // One subface of the .inc table (sub_IO.f90:700-705), 0-based block numbers.
@@ -71,6 +79,11 @@ struct Arena {
   const int *hint_box, *hint_cell, *hint_face;
   const long long* pre_cell;  // nblk+1
   const long long* pre_face;  // nblk+1
+  // nblk+1: the primitive region and the 0..n layer (BlkD::oreg / or1) with their block hints; the
+  // region's total is read from pre_reg[nblk] on the device, since a reset_solve that changes a
+  // solve's boundary scheme changes it without touching a captured step
+  const long long *pre_reg, *pre_r1;
+  const int *hint_reg, *hint_r1;
   const long long* pre_col;   // nblk+1, (ny-1)(nz-1) columns per block
   const long long* pre_lnj;   // nblk+1, (nx-1)(nz-1) j-lines per block
   const long long* pre_lnk;   // nblk+1, (nx-1)(ny-1) k-lines per block
@@ -88,6 +101,9 @@ struct Arena {
   const SolveP* sp;
   int nsolve;
   long long tot_box, tot_cell, tot_face, tot_node, tot_col, tot_subcell, tot_halo, tot_lnj, tot_lnk;
+  long long tot_r1;
+  const int4* tiles;  // residual tiles (block, first cell i, j, k), block by block, i fastest
+  int ntile, tile_maxf, tile_maxc;  // largest face count of one direction / cell count of a tile
   // geometry
   const double *x, *y, *z;   // node
   const double* Md;          // 48 FP64 metric planes (face)

@@ -86,7 +86,13 @@ struct ocfd_handle {
   int nvar = 5, prec = 0, nblk = 0, nsolve = 1;
   std::vector<BlkD> blk;
   std::vector<SubD> sub;
-  std::vector<long long> pre_box, pre_cell, pre_face, pre_col, pre_subcell, pre_halo, pre_lnj, pre_lnk;
+  std::vector<long long> pre_box, pre_cell, pre_face, pre_col, pre_subcell, pre_halo, pre_lnj, pre_lnk, pre_reg, pre_r1;
+  long long tot_reg = 0, tot_r1 = 0;
+  std::vector<unsigned char> phys;  // per block and face (d*2+side): every face cell physical
+  int4* d_tiles = nullptr;
+  int ntile = 0, tile_maxf = 0, tile_maxc = 0;
+  long long *d_pre_reg = nullptr, *d_pre_r1 = nullptr;
+  int *d_hint_reg = nullptr, *d_hint_r1 = nullptr;
   std::vector<int4> cchunk, wchunk;
   std::vector<SolveP> sps;
   long long tot_box = 0, tot_cell = 0, tot_face = 0, tot_node = 0, tot_col = 0, tot_subcell = 0, tot_halo = 0;
@@ -307,6 +313,9 @@ static void fill_arena(ocfd_handle* h, Arena<T>& A, const T* M, const T* vol, co
   A.blk = h->d_blk; A.nblk = h->nblk;
   A.pre_box = h->d_pre_box; A.pre_cell = h->d_pre_cell; A.pre_face = h->d_pre_face; A.pre_col = h->d_pre_col;
   A.hint_box = h->d_hint_box; A.hint_cell = h->d_hint_cell; A.hint_face = h->d_hint_face;
+  A.pre_reg = h->d_pre_reg; A.pre_r1 = h->d_pre_r1; A.hint_reg = h->d_hint_reg; A.hint_r1 = h->d_hint_r1;
+  A.tot_r1 = h->tot_r1;
+  A.tiles = h->d_tiles; A.ntile = h->ntile; A.tile_maxf = h->tile_maxf; A.tile_maxc = h->tile_maxc;
   A.pre_lnj = h->d_pre_lnj; A.pre_lnk = h->d_pre_lnk; A.tot_lnj = h->pre_lnj[h->nblk]; A.tot_lnk = h->pre_lnk[h->nblk];
   A.sub = h->d_sub; A.nsub = (int)h->sub.size();
   A.pre_subcell = h->d_pre_subcell; A.pre_halo = h->d_pre_halo;
@@ -478,6 +487,69 @@ static int part_exchange(void* ctx, cudaStream_t st) {
                            P.recv_off.data());
   if (rc && !P.comm_err) P.comm_err = rc;
   return rc ? 0 : 1;
+}
+
+// the cells whose primitives a residual reads (BlkD::glo/ghi, the pre_reg prefix): all LAPH ghost
+// layers across a block face with an interface cell; across a wholly physical face only as deep
+// as that face's stencils reach.  The face at the boundary uses CD2 (cells 0 and 1), the next
+// LAPH-2 faces the boundary scheme, which reaches 1 cell below its face's left cell for the 2nd /
+// 3rd-order schemes (and UD1), 2 for WENO5 / UD5 and 3 for WENO7; the interior scheme starts
+// LAPH faces in and reaches layer 0 at most.  Depends on each solve's boundary scheme, so a
+// reset_solve recomputes it.
+static void region_tables(ocfd_handle* h) {
+  const int nblk = h->nblk;
+  h->pre_reg.assign(nblk + 1, 0);
+  for (int b = 0; b < nblk; b++) {
+    BlkD& B = h->blk[b];
+    const int bs = h->Ps[B.solve].bound_scheme;
+    const int reach = bs == OCFD_SCHEME_WENO7 ? 3 : ((bs == OCFD_SCHEME_WENO5 || bs == OCFD_SCHEME_UD5) ? 2 : 1);
+    for (int d = 0; d < 3; d++) {
+      B.glo[d] = h->phys[b * 6 + d * 2] ? reach : LAPH;
+      B.ghi[d] = h->phys[b * 6 + d * 2 + 1] ? reach : LAPH;
+    }
+    B.RX = B.nx - 1 + B.glo[0] + B.ghi[0];
+    B.RY = B.ny - 1 + B.glo[1] + B.ghi[1];
+    B.RZ = B.nz - 1 + B.glo[2] + B.ghi[2];
+    B.oreg = h->pre_reg[b];
+    h->pre_reg[b + 1] = h->pre_reg[b] + (long long)B.RX * B.RY * B.RZ;
+  }
+  h->tot_reg = h->pre_reg[nblk];
+}
+
+// residual tiles: about 512 cells, 16 along i, 4 along k (fewer on thinner blocks, whose tiles
+// grow in j instead), in block order with i fastest so that neighbouring tiles run together
+static std::vector<int4> tile_table(ocfd_handle* h) {
+  std::vector<int4> t;
+  h->tile_maxf = 1;
+  h->tile_maxc = 1;
+  int TI = 16, TK = 4, NC = 512;  // OCFD_RES_TILE="i,k,cells" overrides (tile-shape measurements)
+  if (const char* e = std::getenv("OCFD_RES_TILE")) {
+    int a = 0, c = 0, n = 0;
+    if (std::sscanf(e, "%d,%d,%d", &a, &c, &n) == 3 && a > 0 && c > 0 && n >= a * c && n <= 1024) { TI = a; TK = c; NC = n; }
+  }
+  for (int b = 0; b < h->nblk; b++) {
+    BlkD& B = h->blk[b];
+    const int ti = std::min(TI, B.nx - 1), tk = std::min(TK, B.nz - 1);
+    const int tj = std::min(B.ny - 1, std::max(1, NC / (ti * tk)));
+    B.tdim[0] = ti; B.tdim[1] = tj; B.tdim[2] = tk;
+    h->tile_maxc = std::max(h->tile_maxc, ti * tj * tk);
+    h->tile_maxf = std::max({h->tile_maxf, (ti + 1) * tj * tk, ti * (tj + 1) * tk, ti * tj * (tk + 1)});
+    for (int k = 1; k < B.nz; k += tk)
+      for (int j = 1; j < B.ny; j += tj)
+        for (int i = 1; i < B.nx; i += ti) t.push_back(make_int4(b, i, j, k));
+  }
+  return t;
+}
+
+static std::vector<int> hint_table(const std::vector<long long>& pre, int nblk) {
+  std::vector<int> hv((size_t)(pre[nblk] >> HINT_SHIFT) + 1);
+  int b = 0;
+  for (size_t q = 0; q < hv.size(); q++) {
+    const long long g = (long long)q << HINT_SHIFT;
+    while (b + 1 < nblk && pre[b + 1] <= g) b++;
+    hv[q] = b;
+  }
+  return hv;
 }
 
 static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, const int* nijk, const double* const* xyz, const int* nsub,
@@ -685,8 +757,36 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     unsigned char bit = S.face <= 3 ? 1 : 2;
     if (S.face == 1 || S.face == 4) for (int k = S.kb; k <= S.ke - 1; k++) for (int j = S.jb; j <= S.je - 1; j++) bci[B.obci + (j - 1) + (long long)(B.ny - 1) * (k - 1)] |= bit;
     if (S.face == 2 || S.face == 5) for (int k = S.kb; k <= S.ke - 1; k++) for (int i = S.ib; i <= S.ie - 1; i++) bcj[B.obcj + (i - 1) + (long long)(B.nx - 1) * (k - 1)] |= bit;
-    if (S.face == 3 || S.face == 6) for (int j = S.jb; j <= S.je - 1; j++) for (int i = S.ib; i <= S.ie - 1; i++) bck[B.obck + (i - 1) + (long long)(B.nx - 1) * (j - 1)] |= bit;
+    // k faces also mark bc > 0 (bits 4 / 8): their inviscid flux is the central one of k_inv_kbc
+    const unsigned char kbit = bit | (S.bc > 0 ? (unsigned char)(bit << 2) : 0);
+    if (S.face == 3 || S.face == 6) for (int j = S.jb; j <= S.je - 1; j++) for (int i = S.ib; i <= S.ie - 1; i++) bck[B.obck + (i - 1) + (long long)(B.nx - 1) * (j - 1)] |= kbit;
   }
+  // block faces whose every face cell carries a physical condition (the region tables below)
+  h->phys.assign((size_t)nblk * 6, 0);
+  for (int b = 0; b < nblk; b++) {
+    const BlkD& B = h->blk[b];
+    const int n[3] = {B.nx - 1, B.ny - 1, B.nz - 1};
+    for (int d = 0; d < 3; d++) {
+      const int na = d == 0 ? n[1] : n[0], nb = d == 2 ? n[1] : n[2];
+      const unsigned char* f = d == 0 ? &bci[B.obci] : (d == 1 ? &bcj[B.obcj] : &bck[B.obck]);
+      for (int side = 0; side < 2; side++) {
+        bool all = true;
+        for (long long l = 0; l < (long long)na * nb && all; l++) all = (f[l] & (side == 0 ? 1 : 2)) != 0;
+        h->phys[b * 6 + d * 2 + side] = all;
+      }
+    }
+  }
+  region_tables(h);
+  const std::vector<int4> tiles = tile_table(h);
+  h->ntile = (int)tiles.size();
+  h->tot_r1 = 0;
+  h->pre_r1.assign(nblk + 1, 0);
+  for (int b = 0; b < nblk; b++) {
+    BlkD& B = h->blk[b];
+    B.or1 = h->pre_r1[b];
+    h->pre_r1[b + 1] = h->pre_r1[b] + (long long)(B.nx + 1) * (B.ny + 1) * (B.nz + 1);
+  }
+  h->tot_r1 = h->pre_r1[nblk];
   // node coordinates + ghost layer
   std::vector<std::vector<double>> X(nblk);
   for (int b = 0; b < nblk; b++) {
@@ -744,17 +844,14 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   h->d_sub = M.alloc<SubD>(std::max(1, ns), e);
   h->d_sp = M.alloc<SolveP>(nsolve, e);
   // block hints of the box, cell and face index spaces (find_blk_h)
-  auto hints = [&](const std::vector<long long>& pre) {
-    std::vector<int> hv((size_t)(pre[nblk] >> HINT_SHIFT) + 1);
-    int b = 0;
-    for (size_t q = 0; q < hv.size(); q++) {
-      const long long g = (long long)q << HINT_SHIFT;
-      while (b + 1 < nblk && pre[b + 1] <= g) b++;
-      hv[q] = b;
-    }
-    return hv;
-  };
+  auto hints = [&](const std::vector<long long>& pre) { return hint_table(pre, nblk); };
   const std::vector<int> hint_box = hints(h->pre_box), hint_cell = hints(h->pre_cell), hint_face = hints(h->pre_face);
+  const std::vector<int> hint_reg = hints(h->pre_reg), hint_r1 = hints(h->pre_r1);
+  h->d_hint_reg = M.alloc<int>(hint_box.size(), e);  // the largest a reset_solve can make it
+  h->d_tiles = M.alloc<int4>(tiles.size(), e);
+  h->d_hint_r1 = M.alloc<int>(hint_r1.size(), e);
+  h->d_pre_reg = M.alloc<long long>(nblk + 1, e);
+  h->d_pre_r1 = M.alloc<long long>(nblk + 1, e);
   h->d_hint_box = M.alloc<int>(hint_box.size(), e);
   h->d_hint_cell = M.alloc<int>(hint_cell.size(), e);
   h->d_hint_face = M.alloc<int>(hint_face.size(), e);
@@ -830,6 +927,8 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   if ((e = up(h->d_blk, h->blk)) || (e = up(h->d_sub, h->sub)) || (e = up(h->d_sp, h->sps)) ||
       (e = up(h->d_hint_box, hint_box)) || (e = up(h->d_hint_cell, hint_cell)) || (e = up(h->d_hint_face, hint_face)) ||
       (e = up(h->d_pre_box, h->pre_box)) || (e = up(h->d_pre_cell, h->pre_cell)) || (e = up(h->d_pre_face, h->pre_face)) ||
+      (e = up(h->d_pre_reg, h->pre_reg)) || (e = up(h->d_pre_r1, h->pre_r1)) || (e = up(h->d_hint_reg, hint_reg)) ||
+      (e = up(h->d_hint_r1, hint_r1)) || (e = up(h->d_tiles, tiles)) ||
       (e = up(h->d_pre_col, h->pre_col)) || (e = up(h->d_pre_subcell, h->pre_subcell)) || (e = up(h->d_pre_halo, h->pre_halo)) ||
       (e = up(h->d_pre_lnj, h->pre_lnj)) || (e = up(h->d_pre_lnk, h->pre_lnk)) ||
       (e = up(h->d_cchunk, h->cchunk)) || (e = up(h->d_cspre, h->cspre)) || (e = up(h->d_bc_ent, h->bc_ent)) || (e = up(h->d_bc_pre, h->bc_pre)) || (e = up(h->d_wchunk, h->wchunk)) || (e = up(h->d_x, hx)) || (e = up(h->d_y, hy)) ||
@@ -974,6 +1073,10 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   for (int q = 1; q < nsolve; q++) {
     if (ps[q].iflag_scheme != h->info.int_scheme) h->info.int_scheme = -1;
     if (ps[q].iflag_flux != h->info.int_flux) h->info.int_flux = -1;
+  }
+  {
+    const char* fz = std::getenv("OCFD_RES_FUSED");  // the tile forms of the residual (opt-in: slower on config 2)
+    h->info.res_fused = fz ? std::max(0, std::min(2, std::atoi(fz))) : 0;
   }
   {
     int dev = 0;
@@ -1334,6 +1437,14 @@ extern "C" int ocfd_reset_solve(ocfd_handle* h, int q, const ocfd_params* p) {
   std::vector<ocfd_params> ps = h->Ps;
   ps[q] = *p;
   if (int rc = check_params(ps.data(), h->nsolve)) return fail(h, rc, "reset_solve: parameters incompatible with the handle's other solves");
+  // the step's kernels were picked for the handle's reconstruction and, for WENO5 / MUSCL3 with
+  // Roe in every solve, compiled with the Roe flux (RunInfo::recon_prim / int_scheme / int_flux)
+  if (h->info.recon_prim && p->iflag_reconstruction != 0)
+    return fail(h, OCFD_ERR_UNSUPPORTED, "reset_solve: the handle reconstructs primitive variables only");
+  const bool roe_fixed = h->info.recon_prim && h->info.int_flux == OCFD_FLUX_ROE &&
+                         (h->info.int_scheme == OCFD_SCHEME_WENO5 || h->info.int_scheme == OCFD_SCHEME_MUSCL3);
+  if (roe_fixed && p->iflag_flux != OCFD_FLUX_ROE)
+    return fail(h, OCFD_ERR_UNSUPPORTED, "reset_solve: the handle's step is built for the Roe flux");
   cudaError_t e = cudaStreamSynchronize(h->st);
   if (e != cudaSuccess) return cuda_fail(h, e, "reset_solve");
   h->Ps[q] = *p;
@@ -1346,6 +1457,11 @@ extern "C" int ocfd_reset_solve(ocfd_handle* h, int q, const ocfd_params* p) {
     if (ts == 4) ((float*)mu.data())[l] = (float)(1.0 / p->re);
     else ((double*)mu.data())[l] = 1.0 / p->re;
   }
+  region_tables(h);  // the boundary scheme sets how many ghost layers the primitives cover
+  const std::vector<int> hint_reg = hint_table(h->pre_reg, h->nblk);
+  if (!e) e = cudaMemcpy(h->d_blk, h->blk.data(), sizeof(BlkD) * h->nblk, cudaMemcpyHostToDevice);
+  if (!e) e = cudaMemcpy(h->d_pre_reg, h->pre_reg.data(), sizeof(long long) * (h->nblk + 1), cudaMemcpyHostToDevice);
+  if (!e) e = cudaMemcpy(h->d_hint_reg, hint_reg.data(), sizeof(int) * hint_reg.size(), cudaMemcpyHostToDevice);
   if (!e) e = cudaMemcpy(h->d_sp + q, &h->sps[q], sizeof(SolveP), cudaMemcpyHostToDevice);
   if (!e) e = cudaMemcpy((char*)h->d_mu + x0 * ts, mu.data(), mu.size(), cudaMemcpyHostToDevice);
   if (!e) e = cudaMemset((char*)h->d_mut + x0 * ts, 0, (x1 - x0) * ts);

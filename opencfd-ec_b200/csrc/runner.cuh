@@ -43,6 +43,12 @@ class RunnerT : public Runner {
     lu_wave4_prepare<T, NV, true, 32>();
     lu_wave4_prepare<T, NV, false, 64>();
     lu_wave4_prepare<T, NV, true, 64>();
+    if (I.res_fused) {
+      ns_prepare<true, S_WENO5, F_ROE>();
+      ns_prepare<true, S_MUSCL3, F_ROE>();
+      ns_prepare<true, -1, -1>();
+      ns_prepare<false, -1, -1>();
+    }
     if (I.lus) {
       S_ = *I.lus;
       if (L_.TJ * L_.TK == 64) { lu_wave5_prepare<T, NV, false, 64>(S_); lu_wave5_prepare<T, NV, true, 64>(S_); }
@@ -53,18 +59,18 @@ class RunnerT : public Runner {
   void residual(cudaStream_t st, bool lusgs) override {
     const Arena<T>& A = A_;
     const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
-    k_prim<T><<<grid_of(tb), 256, 0, st>>>(A);
+    k_prim<T><<<grid_of(tb), 256, 0, st>>>(A);  // sized for the box: the region is read on the device
     if (I_.viscous) {
       k_mu<T><<<grid_of(tc), 256, 0, st>>>(A);
       if (I_.turb == 2 && NV == 6) {
-        k_sa_pre<T><<<grid_of(tb), 256, 0, st>>>(A);
+        k_sa_pre<T><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
         k_sa_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
         k_sa_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
         k_sa_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
         k_sa_res<T><<<grid_of(tc), 256, 0, st>>>(A);
-        k_mu_finish<T, 1><<<grid_of(tb), 256, 0, st>>>(A);
+        k_mu_finish<T, 1><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
       } else if (I_.turb == 3 && NV == 7) {
-        k_sst_pre<T><<<grid_of(tb), 256, 0, st>>>(A);
+        k_sst_pre<T><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
         k_sst_src<T><<<grid_of(tc), 256, 0, st>>>(A);
         k_sst_mut_ghost<T, 0><<<grid_of(tb), 256, 0, st>>>(A);
         k_sst_mut_ghost<T, 1><<<grid_of(tb), 256, 0, st>>>(A);
@@ -74,28 +80,39 @@ class RunnerT : public Runner {
         k_sst_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
         k_sst_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
         k_sst_res<T><<<grid_of(tc), 256, 0, st>>>(A);
-        k_mu_finish<T, 1><<<grid_of(tb), 256, 0, st>>>(A);
+        k_mu_finish<T, 1><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
       } else {
         cudaMemsetAsync(A.mut, 0, sizeof(T) * tb, st);
       }
       k_amut<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
     }
-    if (I_.recon_prim) {
-      // specialised instantiations for the WENO5 / MUSCL3 + Roe pairs (residual phase -3 % on
-      // config 2 FP64, -8 % on config 1; MUSCL3 + AUSMPW was measured slower and is left general)
-      if (I_.int_scheme == S_WENO5 && I_.int_flux == F_ROE) inv_flux<true, S_WENO5, F_ROE>(st);
-      else if (I_.int_scheme == S_MUSCL3 && I_.int_flux == F_ROE) inv_flux<true, S_MUSCL3, F_ROE>(st);
-      else inv_flux<true, -1, -1>(st);
+    // specialised instantiations for the WENO5 / MUSCL3 + Roe pairs (residual phase -3 % on
+    // config 2 FP64, -8 % on config 1; MUSCL3 + AUSMPW was measured slower and is left general)
+    const bool weno5_roe = I_.recon_prim && I_.int_scheme == S_WENO5 && I_.int_flux == F_ROE;
+    const bool muscl3_roe = I_.recon_prim && I_.int_scheme == S_MUSCL3 && I_.int_flux == F_ROE;
+    if (I_.res_fused) {
+      if (I_.res_fused == 2 && I_.viscous) {
+        k_visc_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
+        k_visc_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
+        k_visc_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+      }
+      if (weno5_roe) ns_tile<true, S_WENO5, F_ROE>(st);
+      else if (muscl3_roe) ns_tile<true, S_MUSCL3, F_ROE>(st);
+      else if (I_.recon_prim) ns_tile<true, -1, -1>(st);
+      else ns_tile<false, -1, -1>(st);
     } else {
-      inv_flux<false, -1, -1>(st);
+      if (weno5_roe) inv_flux<true, S_WENO5, F_ROE>(st);
+      else if (muscl3_roe) inv_flux<true, S_MUSCL3, F_ROE>(st);
+      else if (I_.recon_prim) inv_flux<true, -1, -1>(st);
+      else inv_flux<false, -1, -1>(st);
+      k_inv_kbc<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
+      if (I_.viscous) {
+        k_visc_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
+        k_visc_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
+        k_visc_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+      }
+      k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
     }
-    k_inv_kbc<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
-    if (I_.viscous) {
-      k_visc_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
-      k_visc_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
-      k_visc_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
-    }
-    k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
     if (I_.time_method == -1) k_dual_res<T, NV><<<grid_of(tc), 256, 0, st>>>(A);
     if (I_.smoothing) {  // after the spectral radii, before dt (sub_Residual.f90:110-113); dt does not read Res
       k_smooth<T, 0><<<grid_of(A.tot_col, 128), 128, 0, st>>>(A);
@@ -106,6 +123,26 @@ class RunnerT : public Runner {
       lusgs_sweep(st, false);
       lusgs_sweep(st, true);
     }
+  }
+
+  template <bool PRIM, int ISCH, int IFLUX>
+  size_t ns_smem() const { return sizeof(T) * 5 * ((size_t)A_.tile_maxf + A_.tile_maxc); }
+  template <bool PRIM, int ISCH, int IFLUX>
+  void ns_prepare() {
+    const size_t sm = ns_smem<PRIM, ISCH, IFLUX>();
+    auto kern = I_.res_fused == 1 ? k_ns_tile<T, PRIM, ISCH, IFLUX, true> : k_ns_tile<T, PRIM, ISCH, IFLUX, false>;
+    if (sm > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, sm);
+    ns_grid_[ns_slot<PRIM, ISCH, IFLUX>()] = std::max(1, std::min(A_.ntile, 148 * std::max(1, occ)));
+  }
+  template <bool PRIM, int ISCH, int IFLUX>
+  static constexpr int ns_slot() { return !PRIM ? 3 : (ISCH == S_WENO5 ? 0 : (ISCH == S_MUSCL3 ? 1 : 2)); }
+  template <bool PRIM, int ISCH, int IFLUX>
+  void ns_tile(cudaStream_t st) {
+    const int g = ns_grid_[ns_slot<PRIM, ISCH, IFLUX>()];
+    if (I_.res_fused == 1) k_ns_tile<T, PRIM, ISCH, IFLUX, true><<<g, 256, ns_smem<PRIM, ISCH, IFLUX>(), st>>>(A_);
+    else k_ns_tile<T, PRIM, ISCH, IFLUX, false><<<g, 256, ns_smem<PRIM, ISCH, IFLUX>(), st>>>(A_);
   }
 
   template <bool PRIM, int ISCH, int IFLUX>
@@ -307,6 +344,7 @@ class RunnerT : public Runner {
   RunInfo I_;
   LuArgs L_{};
   LuStream S_{};
+  int ns_grid_[4] = {1, 1, 1, 1};  // CTAs of k_ns_tile per instantiation (resident CTAs, at most the tiles)
 };
 
 template <class T>

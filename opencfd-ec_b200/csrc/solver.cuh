@@ -73,15 +73,33 @@ __device__ __forceinline__ void dec_box(const BlkD& B, long long l, int& i, int&
   i = (int)(u - t * NX) - 3; j = (int)(t % NY) - 3; k = (int)(t / NY) - 3;
 }
 
+// a block's primitive region (cells 1-glo .. n-1+ghi) and its 0..n layer
+__device__ __forceinline__ void dec_reg(const BlkD& B, long long l, int& i, int& j, int& k) {
+  const unsigned u = (unsigned)l, RX = (unsigned)B.RX, RY = (unsigned)B.RY;
+  const unsigned t = u / RX;
+  i = (int)(u - t * RX) + 1 - B.glo[0]; j = (int)(t % RY) + 1 - B.glo[1]; k = (int)(t / RY) + 1 - B.glo[2];
+}
+__device__ __forceinline__ void dec_r1(const BlkD& B, long long l, int& i, int& j, int& k) {
+  const unsigned u = (unsigned)l, X = (unsigned)(B.nx + 1), Y = (unsigned)(B.ny + 1);
+  const unsigned t = u / X;
+  i = (int)(u - t * X); j = (int)(t % Y); k = (int)(t / Y);
+}
+
 // ============================================================================================
-// primitives (comput_duvtpc, sub_Residual.f90:1417-1456) over the whole ghost box
+// primitives (comput_duvtpc, sub_Residual.f90:1417-1456) on the cells a residual reads: the
+// reference fills the whole ghost box, of which the stencils across a physical face read only
+// the layers their boundary scheme reaches (BlkD::glo/ghi); the cells left out are never read
 // ============================================================================================
 template <class T>
 __global__ void k_prim(Arena<T> A) {
-  const long long tb = A.tot_box;
-  OCFD_GRID_STRIDE(g, tb) {
-    int b = find_blk_h(A.pre_box, A.hint_box, A.nblk, g);
-    const SolveP& s = A.sp[A.blk[b].solve];
+  const long long tb = A.tot_box, tr = __ldg(A.pre_reg + A.nblk);
+  OCFD_GRID_STRIDE(r, tr) {
+    const int b = find_blk_h(A.pre_reg, A.hint_reg, A.nblk, r);
+    const BlkD& B = A.blk[b];
+    int i, j, k;
+    dec_reg(B, r - __ldg(A.pre_reg + b), i, j, k);
+    const long long g = bix(B, i, j, k);
+    const SolveP& s = A.sp[B.solve];
     double d = A.U[g], u1 = A.U[tb + g], u2 = A.U[2 * tb + g], u3 = A.U[3 * tb + g], u4 = A.U[4 * tb + g];
     double uu = u1 / d, v = u2 / d, w = u3 / d;
     double Tt = (u4 - 0.5 * d * (uu * uu + v * v + w * w)) / (s.cv * d);
@@ -133,12 +151,12 @@ __device__ __forceinline__ double Cw1() { return Cb1 / (kap * kap) + (1.0 + Cb2)
 template <class T>
 __global__ void k_sa_pre(Arena<T> A) {
   const long long tb = A.tot_box;
-  OCFD_GRID_STRIDE(g, tb) {
-    int b = find_blk_h(A.pre_box, A.hint_box, A.nblk, g);
+  OCFD_GRID_STRIDE(r, A.tot_r1) {
+    const int b = find_blk_h(A.pre_r1, A.hint_r1, A.nblk, r);
     const BlkD& B = A.blk[b];
     int i, j, k;
-    dec_box(B, g - B.obox, i, j, k);
-    if (i < 0 || i > B.nx || j < 0 || j > B.ny || k < 0 || k > B.nz) continue;
+    dec_r1(B, r - B.or1, i, j, k);
+    const long long g = bix(B, i, j, k);
     const SolveP& s = A.sp[B.solve];
     T mu = T((double)A.mu[g] * s.re);
     T vt = T(clamp0(A.U[5 * tb + g]));
@@ -268,12 +286,12 @@ constexpr double a1 = 0.31, betas = 0.09;
 template <class T>
 __global__ void k_sst_pre(Arena<T> A) {
   const long long tb = A.tot_box;
-  OCFD_GRID_STRIDE(g, tb) {
-    int b = find_blk_h(A.pre_box, A.hint_box, A.nblk, g);
+  OCFD_GRID_STRIDE(r, A.tot_r1) {
+    const int b = find_blk_h(A.pre_r1, A.hint_r1, A.nblk, r);
     const BlkD& B = A.blk[b];
     int i, j, k;
-    dec_box(B, g - B.obox, i, j, k);
-    if (i < 0 || i > B.nx || j < 0 || j > B.ny || k < 0 || k > B.nz) continue;
+    dec_r1(B, r - B.or1, i, j, k);
+    const long long g = bix(B, i, j, k);
     const SolveP& s = A.sp[B.solve];
     const T mu = T((double)A.mu[g] * s.re);
     const double d = A.U[g], u5 = A.U[5 * tb + g], u6 = A.U[6 * tb + g];  // loads before the stores
@@ -449,12 +467,12 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sst_res(Arena<T> A) {
 // MODE 0: laminar (mu_t was zeroed); 1: turbulence model ran with mu scaled by Re.
 template <class T, int MODE>
 __global__ void k_mu_finish(Arena<T> A) {
-  OCFD_GRID_STRIDE(g, A.tot_box) {
-    int b = find_blk_h(A.pre_box, A.hint_box, A.nblk, g);
+  OCFD_GRID_STRIDE(r, A.tot_r1) {
+    const int b = find_blk_h(A.pre_r1, A.hint_r1, A.nblk, r);
     const BlkD& B = A.blk[b];
     int i, j, k;
-    dec_box(B, g - B.obox, i, j, k);
-    if (i < 0 || i > B.nx || j < 0 || j > B.ny || k < 0 || k > B.nz) continue;
+    dec_r1(B, r - B.or1, i, j, k);
+    const long long g = bix(B, i, j, k);
     const SolveP& s = A.sp[B.solve];
     T mu = A.mu[g], mut = A.mut[g];
     if (MODE == 1) { mu = T((double)mu / s.re); mut = T((double)mut / s.re); A.mu[g] = mu; }
@@ -520,9 +538,123 @@ struct InvFluxOcc { static constexpr int value = sizeof(T) == 8 ? 3 : INV_FLUX_M
 // spills: config 1 residual phase 0.099 -> 0.094 ms; WENO5 is faster at 3, 1.85 against 2.00 ms)
 template <class T, int ISCH>
 struct InvFluxOccS { static constexpr int value = (sizeof(T) == 8 && ISCH == S_MUSCL3) ? 2 : InvFluxOcc<T>::value; };
+// one face of direction DIR: its five inviscid flux components (the face's Fi plane entries)
+template <class T, int DIR, bool PRIM, int ISCH, int IFLUX>
+__device__ __forceinline__ void inv_face(const Arena<T>& A, const BlkD& B, const SolveP& s, int b, int i, int j, int k, long long g,
+                                         T* Fo) {
+  const long long tb = A.tot_box, tf = A.tot_face;
+  int idx, nd;
+  unsigned char bc;
+  if (DIR == 0) { idx = i; nd = B.nx; bc = A.bci[B.obci + (j - 1) + (long long)(B.ny - 1) * (k - 1)]; }
+  else if (DIR == 1) { idx = j; nd = B.ny; bc = A.bcj[B.obcj + (i - 1) + (long long)(B.nx - 1) * (k - 1)]; }
+  else { idx = k; nd = B.nz; bc = A.bck[B.obck + (i - 1) + (long long)(B.nx - 1) * (j - 1)]; }
+  int scheme = s.scheme;
+  if (bc & 1) { if (idx == 1) scheme = S_CD2; else if (idx < LAP) scheme = s.bound_scheme; }
+  if (bc & 2) { if (idx == nd) scheme = S_CD2; else if (idx > nd - LAP + 1) scheme = s.bound_scheme; }
+  if (A.flags[b] == 1) scheme = S_UD1;
+  const int di = DIR == 0, dj = DIR == 1, dk = DIR == 2;
+  // stencil cells idx-4 .. idx+3 along DIR
+  long long c0 = bix(B, i - 4 * di, j - 4 * dj, k - 4 * dk);
+  const long long st = DIR == 0 ? 1 : (DIR == 1 ? (long long)B.NX : (long long)B.NX * B.NY);
+  T UL[5], UR[5];
+  if ((PRIM || s.recon == 0) && ISCH >= 0 && scheme == ISCH) {
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      const int pl = m == 4 ? P_P : m;
+      T u[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) u[q] = A.P[pl * tb + c0 + q * st];
+      scheme_LR(u, ISCH < 0 ? 0 : ISCH, UL[m], UR[m]);
+    }
+  } else if (PRIM || s.recon == 0) {
+    T u[8];
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      const int pl = m == 4 ? P_P : m;
+#pragma unroll
+      for (int q = 0; q < 8; q++) u[q] = A.P[pl * tb + c0 + q * st];
+      scheme_LR(u, scheme, UL[m], UR[m]);
+    }
+  } else {
+    T gm = T(s.gamma);
+    T U0[5][8];
+    for (int m = 0; m < 5; m++)
+      for (int q = 0; q < 8; q++) U0[m][q] = T(A.U[m * tb + c0 + q * st]);
+    if (s.recon == 1) {
+      T QL[5], QR[5];
+      for (int m = 0; m < 5; m++) scheme_LR(U0[m], scheme, QL[m], QR[m]);
+      UL[0] = QL[0]; UL[1] = QL[1] / UL[0]; UL[2] = QL[2] / UL[0]; UL[3] = QL[3] / UL[0];
+      UL[4] = (QL[4] - (UL[1] * QL[1] + UL[2] * QL[2] + UL[3] * QL[3]) * T(0.5)) * (gm - T(1));
+      UR[0] = QR[0]; UR[1] = QR[1] / UR[0]; UR[2] = QR[2] / UR[0]; UR[3] = QR[3] / UR[0];
+      UR[4] = (QR[4] - (UR[1] * QR[1] + UR[2] * QR[2] + UR[3] * QR[3]) * T(0.5)) * (gm - T(1));
+    } else {  // characteristic (sub_Residual.f90:1291-1347)
+      T Uh[5];
+      for (int m = 0; m < 5; m++) Uh[m] = T(0.5) * (U0[m][3] + U0[m][4]);
+      T d1 = Uh[0], u1 = Uh[1] / d1, v1 = Uh[2] / d1, w1 = Uh[3] / d1;
+      T p1 = (Uh[4] - (Uh[1] * u1 + Uh[2] * v1 + Uh[3] * w1) * T(0.5)) * (gm - T(1));
+      T c1 = dsqrt(gm * p1 / d1);
+      T V2 = (u1 * u1 + v1 * v1 + w1 * w1) * T(0.5);
+      T tmp1 = (gm - T(1)) / c1, tmp3 = (gm - T(1)) / (c1 * c1), tmp5 = T(1) / (T(2) * c1), tmp0 = T(1) / tmp3;
+      T Sm[5][5] = {{V2 - tmp0, -u1, -v1, -w1, T(1)},
+                    {-v1, T(0), T(1), T(0), T(0)},
+                    {-w1, T(0), T(0), T(1), T(0)},
+                    {-u1 - V2 * tmp1, T(1) + tmp1 * u1, tmp1 * v1, tmp1 * w1, -tmp1},
+                    {-u1 + V2 * tmp1, T(1) - tmp1 * u1, -tmp1 * v1, -tmp1 * w1, tmp1}};
+      T S1[5][5] = {{-tmp3, T(0), T(0), -tmp5, tmp5},
+                    {-tmp3 * u1, T(0), T(0), T(0.5) - u1 * tmp5, T(0.5) + u1 * tmp5},
+                    {-tmp3 * v1, T(1), T(0), -v1 * tmp5, v1 * tmp5},
+                    {-tmp3 * w1, T(0), T(1), -w1 * tmp5, w1 * tmp5},
+                    {-tmp3 * V2, v1, w1, (c1 * u1 - V2 - tmp0) * tmp5, (c1 * u1 + V2 + tmp0) * tmp5}};
+      T V0[5][8];
+      for (int q = 0; q < 8; q++)
+        for (int m = 0; m < 5; m++) {
+          T acc = T(0);
+          for (int jj = 0; jj < 5; jj++) acc = acc + Sm[m][jj] * U0[jj][q];
+          V0[m][q] = acc;
+        }
+      T VL[5], VR[5], QL[5], QR[5];
+      for (int m = 0; m < 5; m++) scheme_LR(V0[m], scheme, VL[m], VR[m]);
+      for (int m = 0; m < 5; m++) {
+        QL[m] = T(0); QR[m] = T(0);
+        for (int jj = 0; jj < 5; jj++) { QL[m] = QL[m] + S1[m][jj] * VL[jj]; QR[m] = QR[m] + S1[m][jj] * VR[jj]; }
+      }
+      UL[0] = QL[0]; UL[1] = QL[1] / UL[0]; UL[2] = QL[2] / UL[0]; UL[3] = QL[3] / UL[0];
+      UL[4] = (QL[4] - (UL[1] * QL[1] + UL[2] * QL[2] + UL[3] * QL[3]) * T(0.5)) * (gm - T(1));
+      UR[0] = QR[0]; UR[1] = QR[1] / UR[0]; UR[2] = QR[2] / UR[0]; UR[3] = QR[3] / UR[0];
+      UR[4] = (QR[4] - (UR[1] * QR[1] + UR[2] * QR[2] + UR[3] * QR[3]) * T(0.5)) * (gm - T(1));
+    }
+  }
+  if (s.positivity == 1) {  // first-order fallback (sub_Residual.f90:283-299)
+    const T lz = T(1.e-20);
+    if (UL[0] <= lz || UL[4] <= lz) {
+      long long cl = c0 + 3 * st;
+      UL[0] = A.P[P_D * tb + cl]; UL[1] = A.P[P_U * tb + cl]; UL[2] = A.P[P_V * tb + cl]; UL[3] = A.P[P_W * tb + cl]; UL[4] = A.P[P_P * tb + cl];
+    }
+    if (UR[0] <= lz || UR[4] <= lz) {
+      long long cr = c0 + 4 * st;
+      UR[0] = A.P[P_D * tb + cr]; UR[1] = A.P[P_U * tb + cr]; UR[2] = A.P[P_V * tb + cr]; UR[3] = A.P[P_W * tb + cr]; UR[4] = A.P[P_P * tb + cr];
+    }
+  }
+  T s1x = A.M[(M_NI1 + 3 * DIR) * tf + g], s1y = A.M[(M_NI2 + 3 * DIR) * tf + g], s1z = A.M[(M_NI3 + 3 * DIR) * tf + g];
+  T s2x = A.M[(M_TI + 3 * DIR) * tf + g], s2y = A.M[(M_TI + 3 * DIR + 1) * tf + g], s2z = A.M[(M_TI + 3 * DIR + 2) * tf + g];
+  T s3x = s1y * s2z - s1z * s2y, s3y = s1z * s2x - s1x * s2z, s3z = s1x * s2y - s1y * s2x;
+  T QL[5], QR[5], F0[5];
+  QL[0] = UL[0]; QL[1] = UL[1] * s1x + UL[2] * s1y + UL[3] * s1z; QL[2] = UL[1] * s2x + UL[2] * s2y + UL[3] * s2z;
+  QL[3] = UL[1] * s3x + UL[2] * s3y + UL[3] * s3z; QL[4] = UL[4];
+  QR[0] = UR[0]; QR[1] = UR[1] * s1x + UR[2] * s1y + UR[3] * s1z; QR[2] = UR[1] * s2x + UR[2] * s2y + UR[3] * s2z;
+  QR[3] = UR[1] * s3x + UR[2] * s3y + UR[3] * s3z; QR[4] = UR[4];
+  flux_1d(QL, QR, F0, T(s.gamma), IFLUX >= 0 ? IFLUX : s.flux);
+  T S = A.M[(M_SI + DIR) * tf + g];
+  Fo[0] = -F0[0] * S;
+  Fo[1] = -(F0[1] * s1x + F0[2] * s2x + F0[3] * s3x) * S;
+  Fo[2] = -(F0[1] * s1y + F0[2] * s2y + F0[3] * s3y) * S;
+  Fo[3] = -(F0[1] * s1z + F0[2] * s2z + F0[3] * s3z) * S;
+  Fo[4] = -F0[4] * S;
+}
+
 template <class T, int DIR, bool PRIM = false, int ISCH = -1, int IFLUX = -1>
 __global__ void __launch_bounds__(256, InvFluxOccS<T, ISCH>::value) k_inv_flux(Arena<T> A) {
-  const long long tb = A.tot_box, tf = A.tot_face;
+  const long long tf = A.tot_face;
   OCFD_GRID_STRIDE(g, tf) {
     int b = find_blk_h(A.pre_face, A.hint_face, A.nblk, g);
     const BlkD& B = A.blk[b];
@@ -531,155 +663,152 @@ __global__ void __launch_bounds__(256, InvFluxOccS<T, ISCH>::value) k_inv_flux(A
     if (DIR == 0 && (j == B.ny || k == B.nz)) continue;
     if (DIR == 1 && (i == B.nx || k == B.nz)) continue;
     if (DIR == 2 && (i == B.nx || j == B.ny)) continue;
-    const SolveP& s = A.sp[B.solve];
-    int idx, nd;
-    unsigned char bc;
-    if (DIR == 0) { idx = i; nd = B.nx; bc = A.bci[B.obci + (j - 1) + (long long)(B.ny - 1) * (k - 1)]; }
-    else if (DIR == 1) { idx = j; nd = B.ny; bc = A.bcj[B.obcj + (i - 1) + (long long)(B.nx - 1) * (k - 1)]; }
-    else { idx = k; nd = B.nz; bc = A.bck[B.obck + (i - 1) + (long long)(B.nx - 1) * (j - 1)]; }
-    int scheme = s.scheme;
-    if (bc & 1) { if (idx == 1) scheme = S_CD2; else if (idx < LAP) scheme = s.bound_scheme; }
-    if (bc & 2) { if (idx == nd) scheme = S_CD2; else if (idx > nd - LAP + 1) scheme = s.bound_scheme; }
-    if (A.flags[b] == 1) scheme = S_UD1;
-    const int di = DIR == 0, dj = DIR == 1, dk = DIR == 2;
-    // stencil cells idx-4 .. idx+3 along DIR
-    long long c0 = bix(B, i - 4 * di, j - 4 * dj, k - 4 * dk);
-    const long long st = DIR == 0 ? 1 : (DIR == 1 ? (long long)B.NX : (long long)B.NX * B.NY);
-    T UL[5], UR[5];
-    if ((PRIM || s.recon == 0) && ISCH >= 0 && scheme == ISCH) {
-#pragma unroll
-      for (int m = 0; m < 5; m++) {
-        const int pl = m == 4 ? P_P : m;
-        T u[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) u[q] = A.P[pl * tb + c0 + q * st];
-        scheme_LR(u, ISCH < 0 ? 0 : ISCH, UL[m], UR[m]);
-      }
-    } else if (PRIM || s.recon == 0) {
-      T u[8];
-#pragma unroll
-      for (int m = 0; m < 5; m++) {
-        const int pl = m == 4 ? P_P : m;
-#pragma unroll
-        for (int q = 0; q < 8; q++) u[q] = A.P[pl * tb + c0 + q * st];
-        scheme_LR(u, scheme, UL[m], UR[m]);
-      }
-    } else {
-      T gm = T(s.gamma);
-      T U0[5][8];
-      for (int m = 0; m < 5; m++)
-        for (int q = 0; q < 8; q++) U0[m][q] = T(A.U[m * tb + c0 + q * st]);
-      if (s.recon == 1) {
-        T QL[5], QR[5];
-        for (int m = 0; m < 5; m++) scheme_LR(U0[m], scheme, QL[m], QR[m]);
-        UL[0] = QL[0]; UL[1] = QL[1] / UL[0]; UL[2] = QL[2] / UL[0]; UL[3] = QL[3] / UL[0];
-        UL[4] = (QL[4] - (UL[1] * QL[1] + UL[2] * QL[2] + UL[3] * QL[3]) * T(0.5)) * (gm - T(1));
-        UR[0] = QR[0]; UR[1] = QR[1] / UR[0]; UR[2] = QR[2] / UR[0]; UR[3] = QR[3] / UR[0];
-        UR[4] = (QR[4] - (UR[1] * QR[1] + UR[2] * QR[2] + UR[3] * QR[3]) * T(0.5)) * (gm - T(1));
-      } else {  // characteristic (sub_Residual.f90:1291-1347)
-        T Uh[5];
-        for (int m = 0; m < 5; m++) Uh[m] = T(0.5) * (U0[m][3] + U0[m][4]);
-        T d1 = Uh[0], u1 = Uh[1] / d1, v1 = Uh[2] / d1, w1 = Uh[3] / d1;
-        T p1 = (Uh[4] - (Uh[1] * u1 + Uh[2] * v1 + Uh[3] * w1) * T(0.5)) * (gm - T(1));
-        T c1 = dsqrt(gm * p1 / d1);
-        T V2 = (u1 * u1 + v1 * v1 + w1 * w1) * T(0.5);
-        T tmp1 = (gm - T(1)) / c1, tmp3 = (gm - T(1)) / (c1 * c1), tmp5 = T(1) / (T(2) * c1), tmp0 = T(1) / tmp3;
-        T Sm[5][5] = {{V2 - tmp0, -u1, -v1, -w1, T(1)},
-                      {-v1, T(0), T(1), T(0), T(0)},
-                      {-w1, T(0), T(0), T(1), T(0)},
-                      {-u1 - V2 * tmp1, T(1) + tmp1 * u1, tmp1 * v1, tmp1 * w1, -tmp1},
-                      {-u1 + V2 * tmp1, T(1) - tmp1 * u1, -tmp1 * v1, -tmp1 * w1, tmp1}};
-        T S1[5][5] = {{-tmp3, T(0), T(0), -tmp5, tmp5},
-                      {-tmp3 * u1, T(0), T(0), T(0.5) - u1 * tmp5, T(0.5) + u1 * tmp5},
-                      {-tmp3 * v1, T(1), T(0), -v1 * tmp5, v1 * tmp5},
-                      {-tmp3 * w1, T(0), T(1), -w1 * tmp5, w1 * tmp5},
-                      {-tmp3 * V2, v1, w1, (c1 * u1 - V2 - tmp0) * tmp5, (c1 * u1 + V2 + tmp0) * tmp5}};
-        T V0[5][8];
-        for (int q = 0; q < 8; q++)
-          for (int m = 0; m < 5; m++) {
-            T acc = T(0);
-            for (int jj = 0; jj < 5; jj++) acc = acc + Sm[m][jj] * U0[jj][q];
-            V0[m][q] = acc;
-          }
-        T VL[5], VR[5], QL[5], QR[5];
-        for (int m = 0; m < 5; m++) scheme_LR(V0[m], scheme, VL[m], VR[m]);
-        for (int m = 0; m < 5; m++) {
-          QL[m] = T(0); QR[m] = T(0);
-          for (int jj = 0; jj < 5; jj++) { QL[m] = QL[m] + S1[m][jj] * VL[jj]; QR[m] = QR[m] + S1[m][jj] * VR[jj]; }
-        }
-        UL[0] = QL[0]; UL[1] = QL[1] / UL[0]; UL[2] = QL[2] / UL[0]; UL[3] = QL[3] / UL[0];
-        UL[4] = (QL[4] - (UL[1] * QL[1] + UL[2] * QL[2] + UL[3] * QL[3]) * T(0.5)) * (gm - T(1));
-        UR[0] = QR[0]; UR[1] = QR[1] / UR[0]; UR[2] = QR[2] / UR[0]; UR[3] = QR[3] / UR[0];
-        UR[4] = (QR[4] - (UR[1] * QR[1] + UR[2] * QR[2] + UR[3] * QR[3]) * T(0.5)) * (gm - T(1));
-      }
-    }
-    if (s.positivity == 1) {  // first-order fallback (sub_Residual.f90:283-299)
-      const T lz = T(1.e-20);
-      if (UL[0] <= lz || UL[4] <= lz) {
-        long long cl = c0 + 3 * st;
-        UL[0] = A.P[P_D * tb + cl]; UL[1] = A.P[P_U * tb + cl]; UL[2] = A.P[P_V * tb + cl]; UL[3] = A.P[P_W * tb + cl]; UL[4] = A.P[P_P * tb + cl];
-      }
-      if (UR[0] <= lz || UR[4] <= lz) {
-        long long cr = c0 + 4 * st;
-        UR[0] = A.P[P_D * tb + cr]; UR[1] = A.P[P_U * tb + cr]; UR[2] = A.P[P_V * tb + cr]; UR[3] = A.P[P_W * tb + cr]; UR[4] = A.P[P_P * tb + cr];
-      }
-    }
-    T s1x = A.M[(M_NI1 + 3 * DIR) * tf + g], s1y = A.M[(M_NI2 + 3 * DIR) * tf + g], s1z = A.M[(M_NI3 + 3 * DIR) * tf + g];
-    T s2x = A.M[(M_TI + 3 * DIR) * tf + g], s2y = A.M[(M_TI + 3 * DIR + 1) * tf + g], s2z = A.M[(M_TI + 3 * DIR + 2) * tf + g];
-    T s3x = s1y * s2z - s1z * s2y, s3y = s1z * s2x - s1x * s2z, s3z = s1x * s2y - s1y * s2x;
-    T QL[5], QR[5], F0[5];
-    QL[0] = UL[0]; QL[1] = UL[1] * s1x + UL[2] * s1y + UL[3] * s1z; QL[2] = UL[1] * s2x + UL[2] * s2y + UL[3] * s2z;
-    QL[3] = UL[1] * s3x + UL[2] * s3y + UL[3] * s3z; QL[4] = UL[4];
-    QR[0] = UR[0]; QR[1] = UR[1] * s1x + UR[2] * s1y + UR[3] * s1z; QR[2] = UR[1] * s2x + UR[2] * s2y + UR[3] * s2z;
-    QR[3] = UR[1] * s3x + UR[2] * s3y + UR[3] * s3z; QR[4] = UR[4];
-    flux_1d(QL, QR, F0, T(s.gamma), IFLUX >= 0 ? IFLUX : s.flux);
-    T S = A.M[(M_SI + DIR) * tf + g];
+    T F[5];
+    inv_face<T, DIR, PRIM, ISCH, IFLUX>(A, B, A.sp[B.solve], b, i, j, k, g, F);
     T* Fo = A.Fi + (long long)DIR * 5 * tf + g;
-    Fo[0] = -F0[0] * S;
-    Fo[tf] = -(F0[1] * s1x + F0[2] * s2x + F0[3] * s3x) * S;
-    Fo[2 * tf] = -(F0[1] * s1y + F0[2] * s2y + F0[3] * s3y) * S;
-    Fo[3 * tf] = -(F0[1] * s1z + F0[2] * s2z + F0[3] * s3z) * S;
-    Fo[4 * tf] = -F0[4] * S;
+#pragma unroll
+    for (int m = 0; m < 5; m++) Fo[m * tf] = F[m];
   }
 }
 
-// physical k-faces: central flux of the averaged primitives (sub_Residual.f90:666-689)
+// physical k-faces: central flux of the averaged primitives (sub_Residual.f90:666-689), for the
+// face (i, j, k) between cells k-1 and k
+template <class T>
+__device__ __forceinline__ void kbc_face(const Arena<T>& A, const BlkD& B, const SolveP& sp, int i, int j, int k, long long f, T* Fo) {
+  const long long tb = A.tot_box, tf = A.tot_face;
+  long long c0 = bix(B, i, j, k), c1 = bix(B, i, j, k - 1);
+  T gm = T(sp.gamma);
+  T d0 = (A.P[P_D * tb + c0] + A.P[P_D * tb + c1]) * T(0.5), uu0 = (A.P[P_U * tb + c0] + A.P[P_U * tb + c1]) * T(0.5);
+  T v0 = (A.P[P_V * tb + c0] + A.P[P_V * tb + c1]) * T(0.5), w0 = (A.P[P_W * tb + c0] + A.P[P_W * tb + c1]) * T(0.5);
+  T p0 = (A.P[P_P * tb + c0] + A.P[P_P * tb + c1]) * T(0.5);
+  T E0 = p0 / (gm - T(1)) + d0 * (uu0 * uu0 + v0 * v0 + w0 * w0) * T(0.5);
+  T n1 = A.M[M_NK1 * tf + f], n2 = A.M[M_NK2 * tf + f], n3 = A.M[M_NK3 * tf + f], Sk = A.M[M_SK * tf + f];
+  T un = uu0 * n1 + v0 * n2 + w0 * n3;
+  Fo[0] = -d0 * un * Sk;
+  Fo[1] = -(d0 * un * uu0 + p0 * n1) * Sk;
+  Fo[2] = -(d0 * un * v0 + p0 * n2) * Sk;
+  Fo[3] = -(d0 * un * w0 + p0 * n3) * Sk;
+  Fo[4] = -(E0 + p0) * un * Sk;
+}
+
 template <class T>
 __global__ void k_inv_kbc(Arena<T> A) {
-  const long long tb = A.tot_box, tf = A.tot_face;
+  const long long tf = A.tot_face;
   OCFD_GRID_STRIDE(g, A.tot_subcell) {
     int s = find_blk(A.pre_subcell, A.nsub, g);
     const SubD S = A.sub[s];
     if (!(S.bc > 0 && (S.face == 3 || S.face == 6))) continue;
     const BlkD& B = A.blk[S.blk];
-    const SolveP& sp = A.sp[B.solve];
     long long l = g - A.pre_subcell[s];
     const unsigned ni = (unsigned)(S.ie - S.ib), u = (unsigned)l;
     int i = S.ib + (int)(u % ni), j = S.jb + (int)(u / ni), k = S.kb;
-    long long c0 = bix(B, i, j, k), c1 = bix(B, i, j, k - 1);
-    T gm = T(sp.gamma);
-    T d0 = (A.P[P_D * tb + c0] + A.P[P_D * tb + c1]) * T(0.5), uu0 = (A.P[P_U * tb + c0] + A.P[P_U * tb + c1]) * T(0.5);
-    T v0 = (A.P[P_V * tb + c0] + A.P[P_V * tb + c1]) * T(0.5), w0 = (A.P[P_W * tb + c0] + A.P[P_W * tb + c1]) * T(0.5);
-    T p0 = (A.P[P_P * tb + c0] + A.P[P_P * tb + c1]) * T(0.5);
-    T E0 = p0 / (gm - T(1)) + d0 * (uu0 * uu0 + v0 * v0 + w0 * w0) * T(0.5);
     long long f = fix_(B, i, j, k);
-    T n1 = A.M[M_NK1 * tf + f], n2 = A.M[M_NK2 * tf + f], n3 = A.M[M_NK3 * tf + f], Sk = A.M[M_SK * tf + f];
-    T un = uu0 * n1 + v0 * n2 + w0 * n3;
+    T F[5];
+    kbc_face(A, B, A.sp[B.solve], i, j, k, f, F);
     T* Fo = A.Fi + 2LL * 5 * tf + f;
-    Fo[0] = -d0 * un * Sk;
-    Fo[tf] = -(d0 * un * uu0 + p0 * n1) * Sk;
-    Fo[2 * tf] = -(d0 * un * v0 + p0 * n2) * Sk;
-    Fo[3 * tf] = -(d0 * un * w0 + p0 * n3) * Sk;
-    Fo[4 * tf] = -(E0 + p0) * un * Sk;
+#pragma unroll
+    for (int m = 0; m < 5; m++) Fo[m * tf] = F[m];
   }
 }
 
 // ============================================================================================
 // viscous fluxes (flux_viscous_i/j/k, sub_Residual.f90:712-1247)
 // ============================================================================================
+// one face of direction DIR: its four viscous flux components (m = 1..4 of Res; the face's Fv
+// plane entries).  Returns 0 with Fo[0..3] set; under OverLimit (no viscous flux, Surf = 0,
+// sub_Residual.f90:734-750) 1 on a block-boundary face, whose Fo[0..2] are then 0, and 2 elsewhere
+// (Fo untouched).  The flag is tested after the stencil loads (a branch on it first would hold
+// every load of the face behind the flag's load).
+template <class T, int DIR>
+__device__ __forceinline__ int visc_face(const Arena<T>& A, const BlkD& B, const SolveP& s, int overlimit, int i, int j, int k,
+                                         long long g, T* Fo) {
+  const long long tb = A.tot_box, tf = A.tot_face;
+  const T *Pu = A.P + P_U * tb, *Pv = A.P + P_V * tb, *Pw = A.P + P_W * tb, *PT = A.P + P_T * tb;
+  auto avg = [&](const T* a, int i1, int j1, int k1, int i2, int j2, int k2) -> T { return T(0.5) * (a[bix(B, i1, j1, k1)] + a[bix(B, i2, j2, k2)]); };
+  T ui, vi, wi, Ti, uj, vj, wj, Tj, uk, vk, wk, Tk;
+  const int di = DIR == 0, dj = DIR == 1, dk = DIR == 2;
+  const int im = i - di, jm = j - dj, km = k - dk;
+  long long c0 = bix(B, i, j, k), c1 = bix(B, im, jm, km);
+  if (DIR == 0) {
+    ui = Pu[c0] - Pu[c1]; vi = Pv[c0] - Pv[c1]; wi = Pw[c0] - Pw[c1]; Ti = PT[c0] - PT[c1];
+    bool zj = (i == 1 || i == B.nx) && (j == 1 || j == B.ny - 1), zk = (i == 1 || i == B.nx) && (k == 1 || k == B.nz - 1);
+    T uj1 = T(0), vj1 = T(0), wj1 = T(0), Tj1 = T(0), uj2 = T(0), vj2 = T(0), wj2 = T(0), Tj2 = T(0);
+    T uk1 = T(0), vk1 = T(0), wk1 = T(0), Tk1 = T(0), uk2 = T(0), vk2 = T(0), wk2 = T(0), Tk2 = T(0);
+    if (!zj) {
+      uj1 = avg(Pu, i, j - 1, k, i - 1, j - 1, k); vj1 = avg(Pv, i, j - 1, k, i - 1, j - 1, k); wj1 = avg(Pw, i, j - 1, k, i - 1, j - 1, k); Tj1 = avg(PT, i, j - 1, k, i - 1, j - 1, k);
+      uj2 = avg(Pu, i, j + 1, k, i - 1, j + 1, k); vj2 = avg(Pv, i, j + 1, k, i - 1, j + 1, k); wj2 = avg(Pw, i, j + 1, k, i - 1, j + 1, k); Tj2 = avg(PT, i, j + 1, k, i - 1, j + 1, k);
+    }
+    if (!zk) {
+      uk1 = avg(Pu, i, j, k - 1, i - 1, j, k - 1); vk1 = avg(Pv, i, j, k - 1, i - 1, j, k - 1); wk1 = avg(Pw, i, j, k - 1, i - 1, j, k - 1); Tk1 = avg(PT, i, j, k - 1, i - 1, j, k - 1);
+      uk2 = avg(Pu, i, j, k + 1, i - 1, j, k + 1); vk2 = avg(Pv, i, j, k + 1, i - 1, j, k + 1); wk2 = avg(Pw, i, j, k + 1, i - 1, j, k + 1); Tk2 = avg(PT, i, j, k + 1, i - 1, j, k + 1);
+    }
+    uj = T(0.5) * (uj2 - uj1); vj = T(0.5) * (vj2 - vj1); wj = T(0.5) * (wj2 - wj1); Tj = T(0.5) * (Tj2 - Tj1);
+    uk = T(0.5) * (uk2 - uk1); vk = T(0.5) * (vk2 - vk1); wk = T(0.5) * (wk2 - wk1); Tk = T(0.5) * (Tk2 - Tk1);
+  } else if (DIR == 1) {
+    uj = Pu[c0] - Pu[c1]; vj = Pv[c0] - Pv[c1]; wj = Pw[c0] - Pw[c1]; Tj = PT[c0] - PT[c1];
+    bool zi = (j == 1 || j == B.ny) && (i == 1 || i == B.nx - 1), zk = (j == 1 || j == B.ny) && (k == 1 || k == B.nz - 1);
+    T ui1 = T(0), vi1 = T(0), wi1 = T(0), Ti1 = T(0), ui2 = T(0), vi2 = T(0), wi2 = T(0), Ti2 = T(0);
+    T uk1 = T(0), vk1 = T(0), wk1 = T(0), Tk1 = T(0), uk2 = T(0), vk2 = T(0), wk2 = T(0), Tk2 = T(0);
+    if (!zi) {
+      ui1 = avg(Pu, i - 1, j, k, i - 1, j - 1, k); vi1 = avg(Pv, i - 1, j, k, i - 1, j - 1, k); wi1 = avg(Pw, i - 1, j, k, i - 1, j - 1, k); Ti1 = avg(PT, i - 1, j, k, i - 1, j - 1, k);
+      ui2 = avg(Pu, i + 1, j, k, i + 1, j - 1, k); vi2 = avg(Pv, i + 1, j, k, i + 1, j - 1, k); wi2 = avg(Pw, i + 1, j, k, i + 1, j - 1, k); Ti2 = avg(PT, i + 1, j, k, i + 1, j - 1, k);
+    }
+    if (!zk) {
+      uk1 = avg(Pu, i, j, k - 1, i, j - 1, k - 1); vk1 = avg(Pv, i, j, k - 1, i, j - 1, k - 1); wk1 = avg(Pw, i, j, k - 1, i, j - 1, k - 1); Tk1 = avg(PT, i, j, k - 1, i, j - 1, k - 1);
+      uk2 = avg(Pu, i, j, k + 1, i, j - 1, k + 1); vk2 = avg(Pv, i, j, k + 1, i, j - 1, k + 1); wk2 = avg(Pw, i, j, k + 1, i, j - 1, k + 1); Tk2 = avg(PT, i, j, k + 1, i, j - 1, k + 1);
+    }
+    ui = T(0.5) * (ui2 - ui1); vi = T(0.5) * (vi2 - vi1); wi = T(0.5) * (wi2 - wi1); Ti = T(0.5) * (Ti2 - Ti1);
+    uk = T(0.5) * (uk2 - uk1); vk = T(0.5) * (vk2 - vk1); wk = T(0.5) * (wk2 - wk1); Tk = T(0.5) * (Tk2 - Tk1);
+  } else {
+    uk = Pu[c0] - Pu[c1]; vk = Pv[c0] - Pv[c1]; wk = Pw[c0] - Pw[c1]; Tk = PT[c0] - PT[c1];
+    bool zi = (k == 1 || k == B.nz) && (i == 1 || i == B.nx - 1), zj = (k == 1 || k == B.nz) && (j == 1 || j == B.ny - 1);
+    T ui1 = T(0), vi1 = T(0), wi1 = T(0), Ti1 = T(0), ui2 = T(0), vi2 = T(0), wi2 = T(0), Ti2 = T(0);
+    T uj1 = T(0), vj1 = T(0), wj1 = T(0), Tj1 = T(0), uj2 = T(0), vj2 = T(0), wj2 = T(0), Tj2 = T(0);
+    if (!zi) {
+      ui1 = avg(Pu, i - 1, j, k, i - 1, j, k - 1); vi1 = avg(Pv, i - 1, j, k, i - 1, j, k - 1); wi1 = avg(Pw, i - 1, j, k, i - 1, j, k - 1); Ti1 = avg(PT, i - 1, j, k, i - 1, j, k - 1);
+      ui2 = avg(Pu, i + 1, j, k, i + 1, j, k - 1); vi2 = avg(Pv, i + 1, j, k, i + 1, j, k - 1); wi2 = avg(Pw, i + 1, j, k, i + 1, j, k - 1); Ti2 = avg(PT, i + 1, j, k, i + 1, j, k - 1);
+    }
+    if (!zj) {
+      uj1 = avg(Pu, i, j - 1, k, i, j - 1, k - 1); vj1 = avg(Pv, i, j - 1, k, i, j - 1, k - 1); wj1 = avg(Pw, i, j - 1, k, i, j - 1, k - 1); Tj1 = avg(PT, i, j - 1, k, i, j - 1, k - 1);
+      uj2 = avg(Pu, i, j + 1, k, i, j + 1, k - 1); vj2 = avg(Pv, i, j + 1, k, i, j + 1, k - 1); wj2 = avg(Pw, i, j + 1, k, i, j + 1, k - 1); Tj2 = avg(PT, i, j + 1, k, i, j + 1, k - 1);
+    }
+    ui = T(0.5) * (ui2 - ui1); vi = T(0.5) * (vi2 - vi1); wi = T(0.5) * (wi2 - wi1); Ti = T(0.5) * (Ti2 - Ti1);
+    uj = T(0.5) * (uj2 - uj1); vj = T(0.5) * (vj2 - vj1); wj = T(0.5) * (wj2 - wj1); Tj = T(0.5) * (Tj2 - Tj1);
+  }
+  if (overlimit == 1) {
+    int idx = DIR == 0 ? i : (DIR == 1 ? j : k), nd = DIR == 0 ? B.nx : (DIR == 1 ? B.ny : B.nz);
+    if (idx == 1 || idx == nd) { Fo[0] = T(0); Fo[1] = T(0); Fo[2] = T(0); return 1; }
+    return 2;
+  }
+  const int J = DIR == 0 ? M_J1 : (DIR == 1 ? M_J2 : M_J3);
+  T ix = A.M[(J + 0) * tf + g], iy = A.M[(J + 1) * tf + g], iz = A.M[(J + 2) * tf + g];
+  T jx = A.M[(J + 3) * tf + g], jy = A.M[(J + 4) * tf + g], jz = A.M[(J + 5) * tf + g];
+  T kx = A.M[(J + 6) * tf + g], ky = A.M[(J + 7) * tf + g], kz = A.M[(J + 8) * tf + g];
+  T ux = ui * ix + uj * jx + uk * kx, vx = vi * ix + vj * jx + vk * kx, wx = wi * ix + wj * jx + wk * kx, Tx = Ti * ix + Tj * jx + Tk * kx;
+  T uy = ui * iy + uj * jy + uk * ky, vy = vi * iy + vj * jy + vk * ky, wy = wi * iy + wj * jy + wk * ky, Ty = Ti * iy + Tj * jy + Tk * ky;
+  T uz = ui * iz + uj * jz + uk * kz, vz = vi * iz + vj * jz + vk * kz, wz = wi * iz + wj * jz + wk * kz, Tz = Ti * iz + Tj * jz + Tk * kz;
+  T mu0 = T(0.5) * (A.mu[c0] + A.mut[c0] + A.mu[c1] + A.mut[c1]);
+  T PrL = T(s.prl), PrT = T(s.prt);
+  T k0 = T(0.5) * T(s.cp) * (A.mu[c0] / PrL + A.mut[c0] / PrT + A.mu[c1] / PrL + A.mut[c1] / PrT);
+  const T t1 = T(4.0 / 3.0), t2 = T(2.0 / 3.0);
+  T s11 = mu0 * (t1 * ux - t2 * (vy + wz)), s12 = mu0 * (uy + vx), s13 = mu0 * (uz + wx);
+  T s22 = mu0 * (t1 * vy - t2 * (ux + wz)), s23 = mu0 * (vz + wy), s33 = mu0 * (t1 * wz - t2 * (ux + vy));
+  T u1 = (Pu[c0] + Pu[c1]) * T(0.5), v1 = (Pv[c0] + Pv[c1]) * T(0.5), w1 = (Pw[c0] + Pw[c1]) * T(0.5);
+  T E1 = u1 * s11 + v1 * s12 + w1 * s13 + k0 * Tx;
+  T E2 = u1 * s12 + v1 * s22 + w1 * s23 + k0 * Ty;
+  T E3 = u1 * s13 + v1 * s23 + w1 * s33 + k0 * Tz;
+  T s1x = A.M[(M_NI1 + 3 * DIR) * tf + g], s1y = A.M[(M_NI2 + 3 * DIR) * tf + g], s1z = A.M[(M_NI3 + 3 * DIR) * tf + g];
+  T S = A.M[(M_SI + DIR) * tf + g];
+  Fo[0] = (s11 * s1x + s12 * s1y + s13 * s1z) * S;
+  Fo[1] = (s12 * s1x + s22 * s1y + s23 * s1z) * S;
+  Fo[2] = (s13 * s1x + s23 * s1y + s33 * s1z) * S;
+  Fo[3] = (E1 * s1x + E2 * s1y + E3 * s1z) * S;
+  return 0;
+}
+
 template <class T, int DIR>
 __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_visc_flux(Arena<T> A) {
-  const long long tb = A.tot_box, tf = A.tot_face;
+  const long long tf = A.tot_face;
   OCFD_GRID_STRIDE(g, tf) {
     int b = find_blk_h(A.pre_face, A.hint_face, A.nblk, g);
     const BlkD& B = A.blk[b];
@@ -688,91 +817,11 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_visc_flux(Arena<T> A) {
     if (DIR == 0 && (j == B.ny || k == B.nz)) continue;
     if (DIR == 1 && (i == B.nx || k == B.nz)) continue;
     if (DIR == 2 && (i == B.nx || j == B.ny)) continue;
+    T F[4];
+    const int r = visc_face<T, DIR>(A, B, A.sp[B.solve], A.flags[b], i, j, k, g, F);
     T* Fo = A.Fv + (long long)DIR * 4 * tf + g;
-    // the block's OverLimit flag is tested after the stencil loads below (a branch on it here
-    // would hold every load of the face behind the flag's load)
-    const int overlimit = A.flags[b];
-    const SolveP& s = A.sp[B.solve];
-    const T *Pu = A.P + P_U * tb, *Pv = A.P + P_V * tb, *Pw = A.P + P_W * tb, *PT = A.P + P_T * tb;
-    auto avg = [&](const T* a, int i1, int j1, int k1, int i2, int j2, int k2) -> T { return T(0.5) * (a[bix(B, i1, j1, k1)] + a[bix(B, i2, j2, k2)]); };
-    T ui, vi, wi, Ti, uj, vj, wj, Tj, uk, vk, wk, Tk;
-    const int di = DIR == 0, dj = DIR == 1, dk = DIR == 2;
-    const int im = i - di, jm = j - dj, km = k - dk;
-    long long c0 = bix(B, i, j, k), c1 = bix(B, im, jm, km);
-    if (DIR == 0) {
-      ui = Pu[c0] - Pu[c1]; vi = Pv[c0] - Pv[c1]; wi = Pw[c0] - Pw[c1]; Ti = PT[c0] - PT[c1];
-      bool zj = (i == 1 || i == B.nx) && (j == 1 || j == B.ny - 1), zk = (i == 1 || i == B.nx) && (k == 1 || k == B.nz - 1);
-      T uj1 = T(0), vj1 = T(0), wj1 = T(0), Tj1 = T(0), uj2 = T(0), vj2 = T(0), wj2 = T(0), Tj2 = T(0);
-      T uk1 = T(0), vk1 = T(0), wk1 = T(0), Tk1 = T(0), uk2 = T(0), vk2 = T(0), wk2 = T(0), Tk2 = T(0);
-      if (!zj) {
-        uj1 = avg(Pu, i, j - 1, k, i - 1, j - 1, k); vj1 = avg(Pv, i, j - 1, k, i - 1, j - 1, k); wj1 = avg(Pw, i, j - 1, k, i - 1, j - 1, k); Tj1 = avg(PT, i, j - 1, k, i - 1, j - 1, k);
-        uj2 = avg(Pu, i, j + 1, k, i - 1, j + 1, k); vj2 = avg(Pv, i, j + 1, k, i - 1, j + 1, k); wj2 = avg(Pw, i, j + 1, k, i - 1, j + 1, k); Tj2 = avg(PT, i, j + 1, k, i - 1, j + 1, k);
-      }
-      if (!zk) {
-        uk1 = avg(Pu, i, j, k - 1, i - 1, j, k - 1); vk1 = avg(Pv, i, j, k - 1, i - 1, j, k - 1); wk1 = avg(Pw, i, j, k - 1, i - 1, j, k - 1); Tk1 = avg(PT, i, j, k - 1, i - 1, j, k - 1);
-        uk2 = avg(Pu, i, j, k + 1, i - 1, j, k + 1); vk2 = avg(Pv, i, j, k + 1, i - 1, j, k + 1); wk2 = avg(Pw, i, j, k + 1, i - 1, j, k + 1); Tk2 = avg(PT, i, j, k + 1, i - 1, j, k + 1);
-      }
-      uj = T(0.5) * (uj2 - uj1); vj = T(0.5) * (vj2 - vj1); wj = T(0.5) * (wj2 - wj1); Tj = T(0.5) * (Tj2 - Tj1);
-      uk = T(0.5) * (uk2 - uk1); vk = T(0.5) * (vk2 - vk1); wk = T(0.5) * (wk2 - wk1); Tk = T(0.5) * (Tk2 - Tk1);
-    } else if (DIR == 1) {
-      uj = Pu[c0] - Pu[c1]; vj = Pv[c0] - Pv[c1]; wj = Pw[c0] - Pw[c1]; Tj = PT[c0] - PT[c1];
-      bool zi = (j == 1 || j == B.ny) && (i == 1 || i == B.nx - 1), zk = (j == 1 || j == B.ny) && (k == 1 || k == B.nz - 1);
-      T ui1 = T(0), vi1 = T(0), wi1 = T(0), Ti1 = T(0), ui2 = T(0), vi2 = T(0), wi2 = T(0), Ti2 = T(0);
-      T uk1 = T(0), vk1 = T(0), wk1 = T(0), Tk1 = T(0), uk2 = T(0), vk2 = T(0), wk2 = T(0), Tk2 = T(0);
-      if (!zi) {
-        ui1 = avg(Pu, i - 1, j, k, i - 1, j - 1, k); vi1 = avg(Pv, i - 1, j, k, i - 1, j - 1, k); wi1 = avg(Pw, i - 1, j, k, i - 1, j - 1, k); Ti1 = avg(PT, i - 1, j, k, i - 1, j - 1, k);
-        ui2 = avg(Pu, i + 1, j, k, i + 1, j - 1, k); vi2 = avg(Pv, i + 1, j, k, i + 1, j - 1, k); wi2 = avg(Pw, i + 1, j, k, i + 1, j - 1, k); Ti2 = avg(PT, i + 1, j, k, i + 1, j - 1, k);
-      }
-      if (!zk) {
-        uk1 = avg(Pu, i, j, k - 1, i, j - 1, k - 1); vk1 = avg(Pv, i, j, k - 1, i, j - 1, k - 1); wk1 = avg(Pw, i, j, k - 1, i, j - 1, k - 1); Tk1 = avg(PT, i, j, k - 1, i, j - 1, k - 1);
-        uk2 = avg(Pu, i, j, k + 1, i, j - 1, k + 1); vk2 = avg(Pv, i, j, k + 1, i, j - 1, k + 1); wk2 = avg(Pw, i, j, k + 1, i, j - 1, k + 1); Tk2 = avg(PT, i, j, k + 1, i, j - 1, k + 1);
-      }
-      ui = T(0.5) * (ui2 - ui1); vi = T(0.5) * (vi2 - vi1); wi = T(0.5) * (wi2 - wi1); Ti = T(0.5) * (Ti2 - Ti1);
-      uk = T(0.5) * (uk2 - uk1); vk = T(0.5) * (vk2 - vk1); wk = T(0.5) * (wk2 - wk1); Tk = T(0.5) * (Tk2 - Tk1);
-    } else {
-      uk = Pu[c0] - Pu[c1]; vk = Pv[c0] - Pv[c1]; wk = Pw[c0] - Pw[c1]; Tk = PT[c0] - PT[c1];
-      bool zi = (k == 1 || k == B.nz) && (i == 1 || i == B.nx - 1), zj = (k == 1 || k == B.nz) && (j == 1 || j == B.ny - 1);
-      T ui1 = T(0), vi1 = T(0), wi1 = T(0), Ti1 = T(0), ui2 = T(0), vi2 = T(0), wi2 = T(0), Ti2 = T(0);
-      T uj1 = T(0), vj1 = T(0), wj1 = T(0), Tj1 = T(0), uj2 = T(0), vj2 = T(0), wj2 = T(0), Tj2 = T(0);
-      if (!zi) {
-        ui1 = avg(Pu, i - 1, j, k, i - 1, j, k - 1); vi1 = avg(Pv, i - 1, j, k, i - 1, j, k - 1); wi1 = avg(Pw, i - 1, j, k, i - 1, j, k - 1); Ti1 = avg(PT, i - 1, j, k, i - 1, j, k - 1);
-        ui2 = avg(Pu, i + 1, j, k, i + 1, j, k - 1); vi2 = avg(Pv, i + 1, j, k, i + 1, j, k - 1); wi2 = avg(Pw, i + 1, j, k, i + 1, j, k - 1); Ti2 = avg(PT, i + 1, j, k, i + 1, j, k - 1);
-      }
-      if (!zj) {
-        uj1 = avg(Pu, i, j - 1, k, i, j - 1, k - 1); vj1 = avg(Pv, i, j - 1, k, i, j - 1, k - 1); wj1 = avg(Pw, i, j - 1, k, i, j - 1, k - 1); Tj1 = avg(PT, i, j - 1, k, i, j - 1, k - 1);
-        uj2 = avg(Pu, i, j + 1, k, i, j + 1, k - 1); vj2 = avg(Pv, i, j + 1, k, i, j + 1, k - 1); wj2 = avg(Pw, i, j + 1, k, i, j + 1, k - 1); Tj2 = avg(PT, i, j + 1, k, i, j + 1, k - 1);
-      }
-      ui = T(0.5) * (ui2 - ui1); vi = T(0.5) * (vi2 - vi1); wi = T(0.5) * (wi2 - wi1); Ti = T(0.5) * (Ti2 - Ti1);
-      uj = T(0.5) * (uj2 - uj1); vj = T(0.5) * (vj2 - vj1); wj = T(0.5) * (wj2 - wj1); Tj = T(0.5) * (Tj2 - Tj1);
-    }
-    if (overlimit == 1) {  // OverLimit: no viscous flux, Surf = 0 (734-750)
-      int idx = DIR == 0 ? i : (DIR == 1 ? j : k), nd = DIR == 0 ? B.nx : (DIR == 1 ? B.ny : B.nz);
-      if (idx == 1 || idx == nd) { Fo[0] = T(0); Fo[tf] = T(0); Fo[2 * tf] = T(0); }
-      continue;
-    }
-    const int J = DIR == 0 ? M_J1 : (DIR == 1 ? M_J2 : M_J3);
-    T ix = A.M[(J + 0) * tf + g], iy = A.M[(J + 1) * tf + g], iz = A.M[(J + 2) * tf + g];
-    T jx = A.M[(J + 3) * tf + g], jy = A.M[(J + 4) * tf + g], jz = A.M[(J + 5) * tf + g];
-    T kx = A.M[(J + 6) * tf + g], ky = A.M[(J + 7) * tf + g], kz = A.M[(J + 8) * tf + g];
-    T ux = ui * ix + uj * jx + uk * kx, vx = vi * ix + vj * jx + vk * kx, wx = wi * ix + wj * jx + wk * kx, Tx = Ti * ix + Tj * jx + Tk * kx;
-    T uy = ui * iy + uj * jy + uk * ky, vy = vi * iy + vj * jy + vk * ky, wy = wi * iy + wj * jy + wk * ky, Ty = Ti * iy + Tj * jy + Tk * ky;
-    T uz = ui * iz + uj * jz + uk * kz, vz = vi * iz + vj * jz + vk * kz, wz = wi * iz + wj * jz + wk * kz, Tz = Ti * iz + Tj * jz + Tk * kz;
-    T mu0 = T(0.5) * (A.mu[c0] + A.mut[c0] + A.mu[c1] + A.mut[c1]);
-    T PrL = T(s.prl), PrT = T(s.prt);
-    T k0 = T(0.5) * T(s.cp) * (A.mu[c0] / PrL + A.mut[c0] / PrT + A.mu[c1] / PrL + A.mut[c1] / PrT);
-    const T t1 = T(4.0 / 3.0), t2 = T(2.0 / 3.0);
-    T s11 = mu0 * (t1 * ux - t2 * (vy + wz)), s12 = mu0 * (uy + vx), s13 = mu0 * (uz + wx);
-    T s22 = mu0 * (t1 * vy - t2 * (ux + wz)), s23 = mu0 * (vz + wy), s33 = mu0 * (t1 * wz - t2 * (ux + vy));
-    T u1 = (Pu[c0] + Pu[c1]) * T(0.5), v1 = (Pv[c0] + Pv[c1]) * T(0.5), w1 = (Pw[c0] + Pw[c1]) * T(0.5);
-    T E1 = u1 * s11 + v1 * s12 + w1 * s13 + k0 * Tx;
-    T E2 = u1 * s12 + v1 * s22 + w1 * s23 + k0 * Ty;
-    T E3 = u1 * s13 + v1 * s23 + w1 * s33 + k0 * Tz;
-    T s1x = A.M[(M_NI1 + 3 * DIR) * tf + g], s1y = A.M[(M_NI2 + 3 * DIR) * tf + g], s1z = A.M[(M_NI3 + 3 * DIR) * tf + g];
-    T S = A.M[(M_SI + DIR) * tf + g];
-    Fo[0] = (s11 * s1x + s12 * s1y + s13 * s1z) * S;
-    Fo[tf] = (s12 * s1x + s22 * s1y + s23 * s1z) * S;
-    Fo[2 * tf] = (s13 * s1x + s23 * s1y + s33 * s1z) * S;
-    Fo[3 * tf] = (E1 * s1x + E2 * s1y + E3 * s1z) * S;
+    if (r == 0) { Fo[0] = F[0]; Fo[tf] = F[1]; Fo[2 * tf] = F[2]; Fo[3 * tf] = F[3]; }
+    else if (r == 1) { Fo[0] = F[0]; Fo[tf] = F[1]; Fo[2 * tf] = F[2]; }
   }
 }
 
@@ -780,9 +829,55 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_visc_flux(Arena<T> A) {
 // Res(1:5) assembly in the reference order (inviscid i "=", j "+=", k "+=", viscous i, j, k),
 // spectral radii (comput_Lijk, sub_time_acceleraction.f90:7-56) and local dt (comput_dt, 61-112)
 // ============================================================================================
+// the cell part of the assembly: spectral radii (comput_Lijk, sub_time_acceleraction.f90:7-56) and
+// local dt (comput_dt, 61-112) from the primitives, then the stores of Res(1:5) = Rm, Lc, Lv, dt;
+// f / fi1 / fj1 / fk1 are the cell's faces in the face index space, g its cell index
+template <class T>
+__device__ __forceinline__ void cell_finish(const Arena<T>& A, const BlkD& B, const SolveP& s, int b, int i, int j, int k, long long g,
+                                            long long f, long long fi1, long long fj1, long long fk1, const T* Rm) {
+  const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
+  long long c = bix(B, i, j, k);
+  T D0 = T(0);
+  if (s.viscous == 1) {
+    T gm = T(s.gamma), f43 = T((double)(4.0f / 3.0f));  // `4./3.` default-real literal
+    D0 = fmax_(gm, f43) / A.P[P_D * tb + c] * (A.mu[c] / T(s.prl) + A.mut[c] / T(s.prt));
+  }
+  T vol = A.vol[g];
+  T vol1 = T(1) / vol;
+  T uu = A.P[P_U * tb + c], v = A.P[P_V * tb + c], w = A.P[P_W * tb + c], cc = A.P[P_C * tb + c];
+  T L[6];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    long long fo = d == 0 ? fi1 : (d == 1 ? fj1 : fk1);
+    const T* n1 = A.M + (M_NI1 + 3 * d) * tf;
+    const T* n2 = A.M + (M_NI2 + 3 * d) * tf;
+    const T* n3 = A.M + (M_NI3 + 3 * d) * tf;
+    const T* Sd = A.M + (M_SI + d) * tf;
+    T un = T(0.5) * (uu * (n1[f] + n1[fo]) + v * (n2[f] + n2[fo]) + w * (n3[f] + n3[fo]));
+    T S0 = (Sd[f] + Sd[fo]) * T(0.5);
+    L[d] = (dabs(un) + cc) * S0;
+    L[3 + d] = D0 * S0 * S0 * vol1;
+  }
+  T dtv;
+  if (s.local_dt == 1) {
+    T dt_fac = A.flags[b] == 0 ? T(1) : T(0.1);
+    dtv = dt_fac * T(s.cfl) * vol / (L[0] + L[1] + L[2] + T(1) * (L[3] + L[4] + L[5]));
+    if (s.dtime_mesh == 1) dtv = dtv * A.dtm[g];
+    if (dtv > T(s.dtmax)) dtv = T(s.dtmax);
+    if (dtv < T(s.dtmin)) dtv = T(s.dtmin);
+  } else {
+    dtv = T(s.dt_global);
+  }
+#pragma unroll
+  for (int m = 0; m < 5; m++) A.Res[m * tc + g] = Rm[m];
+#pragma unroll
+  for (int d = 0; d < 3; d++) { A.Lc[d * tc + g] = L[d]; A.Lv[d * tc + g] = L[3 + d]; }
+  A.dt[g] = dtv;
+}
+
 template <class T>
 __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
-  const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
+  const long long tf = A.tot_face, tc = A.tot_cell;
   OCFD_GRID_STRIDE(g, tc) {
     int b = find_blk_h(A.pre_cell, A.hint_cell, A.nblk, g);
     const BlkD& B = A.blk[b];
@@ -812,43 +907,154 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
       }
       Rm[m] = R;
     }
-    long long c = bix(B, i, j, k);
-    T D0 = T(0);
-    if (s.viscous == 1) {
-      T gm = T(s.gamma), f43 = T((double)(4.0f / 3.0f));  // `4./3.` default-real literal
-      D0 = fmax_(gm, f43) / A.P[P_D * tb + c] * (A.mu[c] / T(s.prl) + A.mut[c] / T(s.prt));
-    }
-    T vol = A.vol[g];
-    T vol1 = T(1) / vol;
-    T uu = A.P[P_U * tb + c], v = A.P[P_V * tb + c], w = A.P[P_W * tb + c], cc = A.P[P_C * tb + c];
-    T L[6];
+    cell_finish(A, B, s, b, i, j, k, g, f, fi1, fj1, fk1, Rm);
+  }
+}
+
+// ============================================================================================
+// The Navier-Stokes residual of a tile of cells in one pass (one CTA per tile at a time): the
+// inviscid face fluxes of direction i, then j, then k, are computed into shared memory and each
+// cell adds its two faces' difference to its Res held in shared memory, then the viscous ones the
+// same way, then the spectral radii, dt and the stores - the order of k_assemble, so the bits are
+// those of k_inv_flux + k_inv_kbc + k_visc_flux + k_assemble, without the face-flux planes.  A
+// face on a tile's border is computed by both tiles that share it.  The viscous fluxes of the
+// block-boundary faces are still stored to Fv, where the forces read them.
+// ============================================================================================
+template <class T, int DIR, bool PRIM, int ISCH, int IFLUX>
+__device__ __forceinline__ void tile_inv_dir(const Arena<T>& A, const BlkD& B, const SolveP& s, int b, int i0, int j0, int k0,
+                                             int ni, int nj, int nk, T* Fs, T* Rs) {
+  const int fa = ni + (DIR == 0), fb = nj + (DIR == 1), fc = nk + (DIR == 2);
+  const int nf = fa * fb * fc, MF = A.tile_maxf, MC = A.tile_maxc;
+  for (int q = threadIdx.x; q < nf; q += blockDim.x) {
+    const int a = q % fa, r = q / fa, bb = r % fb, c = r / fb;
+    const int i = i0 + a, j = j0 + bb, k = k0 + c;
+    const long long g = fix_(B, i, j, k);
+    T F[5];
+    bool kbc = false;
+    if (DIR == 2 && (k == 1 || k == B.nz)) kbc = (A.bck[B.obck + (i - 1) + (long long)(B.nx - 1) * (j - 1)] & (k == 1 ? 4 : 8)) != 0;
+    if (kbc) kbc_face(A, B, s, i, j, k, g, F);
+    else inv_face<T, DIR, PRIM, ISCH, IFLUX>(A, B, s, b, i, j, k, g, F);
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-      long long fo = d == 0 ? fi1 : (d == 1 ? fj1 : fk1);
-      const T* n1 = A.M + (M_NI1 + 3 * d) * tf;
-      const T* n2 = A.M + (M_NI2 + 3 * d) * tf;
-      const T* n3 = A.M + (M_NI3 + 3 * d) * tf;
-      const T* Sd = A.M + (M_SI + d) * tf;
-      T un = T(0.5) * (uu * (n1[f] + n1[fo]) + v * (n2[f] + n2[fo]) + w * (n3[f] + n3[fo]));
-      T S0 = (Sd[f] + Sd[fo]) * T(0.5);
-      L[d] = (dabs(un) + cc) * S0;
-      L[3 + d] = D0 * S0 * S0 * vol1;
-    }
-    T dtv;
-    if (s.local_dt == 1) {
-      T dt_fac = A.flags[b] == 0 ? T(1) : T(0.1);
-      dtv = dt_fac * T(s.cfl) * vol / (L[0] + L[1] + L[2] + T(1) * (L[3] + L[4] + L[5]));
-      if (s.dtime_mesh == 1) dtv = dtv * A.dtm[g];
-      if (dtv > T(s.dtmax)) dtv = T(s.dtmax);
-      if (dtv < T(s.dtmin)) dtv = T(s.dtmin);
-    } else {
-      dtv = T(s.dt_global);
-    }
+    for (int m = 0; m < 5; m++) Fs[m * MF + q] = F[m];
+  }
+  __syncthreads();
+  const int nc = ni * nj * nk, step = DIR == 0 ? 1 : (DIR == 1 ? fa : fa * fb);
+  for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+    const int a = q % ni, r = q / ni, bb = r % nj, c = r / nj;
+    const int lo = a + fa * (bb + fb * c);
 #pragma unroll
-    for (int m = 0; m < 5; m++) A.Res[m * tc + g] = Rm[m];
+    for (int m = 0; m < 5; m++) {
+      const T* F = Fs + m * MF;
+      Rs[m * MC + q] = DIR == 0 ? F[lo + step] - F[lo] : Rs[m * MC + q] + F[lo + step] - F[lo];
+    }
+  }
+  __syncthreads();
+}
+
+template <class T, int DIR>
+__device__ __forceinline__ void tile_visc_dir(const Arena<T>& A, const BlkD& B, const SolveP& s, int i0, int j0, int k0, int ni,
+                                              int nj, int nk, T* Fs, T* Rs) {
+  const long long tf = A.tot_face;
+  const int fa = ni + (DIR == 0), fb = nj + (DIR == 1), fc = nk + (DIR == 2);
+  const int nf = fa * fb * fc, MF = A.tile_maxf, MC = A.tile_maxc;
+  const int nd = DIR == 0 ? B.nx : (DIR == 1 ? B.ny : B.nz);
+  for (int q = threadIdx.x; q < nf; q += blockDim.x) {
+    const int a = q % fa, r = q / fa, bb = r % fb, c = r / fb;
+    const int i = i0 + a, j = j0 + bb, k = k0 + c;
+    const long long g = fix_(B, i, j, k);
+    T F[4];
+    visc_face<T, DIR>(A, B, s, 0, i, j, k, g, F);
 #pragma unroll
-    for (int d = 0; d < 3; d++) { A.Lc[d * tc + g] = L[d]; A.Lv[d * tc + g] = L[3 + d]; }
-    A.dt[g] = dtv;
+    for (int m = 0; m < 4; m++) Fs[m * MF + q] = F[m];
+    const int idx = DIR == 0 ? i : (DIR == 1 ? j : k);
+    if (idx == 1 || idx == nd) {
+      T* Fo = A.Fv + (long long)DIR * 4 * tf + g;
+      Fo[0] = F[0]; Fo[tf] = F[1]; Fo[2 * tf] = F[2]; Fo[3 * tf] = F[3];
+    }
+  }
+  __syncthreads();
+  const int nc = ni * nj * nk, step = DIR == 0 ? 1 : (DIR == 1 ? fa : fa * fb);
+  for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+    const int a = q % ni, r = q / ni, bb = r % nj, c = r / nj;
+    const int lo = a + fa * (bb + fb * c);
+#pragma unroll
+    for (int m = 1; m < 5; m++) {
+      const T* F = Fs + (m - 1) * MF;
+      Rs[m * MC + q] = Rs[m * MC + q] + F[lo + step] - F[lo];
+    }
+  }
+  __syncthreads();
+}
+
+// OverLimit: no viscous flux; the block-boundary faces of Fv hold 0 in components 1..3
+template <class T, int DIR>
+__device__ __forceinline__ void tile_visc_zero(const Arena<T>& A, const BlkD& B, int i0, int j0, int k0, int ni, int nj, int nk) {
+  const long long tf = A.tot_face;
+  const int fa = ni + (DIR == 0), fb = nj + (DIR == 1), fc = nk + (DIR == 2);
+  const int nd = DIR == 0 ? B.nx : (DIR == 1 ? B.ny : B.nz);
+  for (int q = threadIdx.x; q < fa * fb * fc; q += blockDim.x) {
+    const int a = q % fa, r = q / fa, bb = r % fb, c = r / fb;
+    const int i = i0 + a, j = j0 + bb, k = k0 + c;
+    const int idx = DIR == 0 ? i : (DIR == 1 ? j : k);
+    if (idx == 1 || idx == nd) {
+      T* Fo = A.Fv + (long long)DIR * 4 * tf + fix_(B, i, j, k);
+      Fo[0] = T(0); Fo[tf] = T(0); Fo[2 * tf] = T(0);
+    }
+  }
+}
+
+// VISC: the viscous fluxes are computed in the tile too (else k_visc_flux wrote them to Fv, and the
+// cells add them from there, in the same order)
+template <class T, bool PRIM, int ISCH, int IFLUX, bool VISC>
+__global__ void __launch_bounds__(256, InvFluxOccS<T, ISCH>::value) k_ns_tile(Arena<T> A) {
+  extern __shared__ __align__(16) unsigned char ns_smem[];
+  T* Fs = reinterpret_cast<T*>(ns_smem);
+  T* Rs = Fs + 5 * A.tile_maxf;
+  const int MC = A.tile_maxc;
+  for (int t = blockIdx.x; t < A.ntile; t += gridDim.x) {
+    const int4 tl = A.tiles[t];
+    const int b = tl.x, i0 = tl.y, j0 = tl.z, k0 = tl.w;
+    const BlkD& B = A.blk[b];
+    const SolveP& s = A.sp[B.solve];
+    const int ni = min(B.tdim[0], B.nx - i0), nj = min(B.tdim[1], B.ny - j0), nk = min(B.tdim[2], B.nz - k0);
+    tile_inv_dir<T, 0, PRIM, ISCH, IFLUX>(A, B, s, b, i0, j0, k0, ni, nj, nk, Fs, Rs);
+    tile_inv_dir<T, 1, PRIM, ISCH, IFLUX>(A, B, s, b, i0, j0, k0, ni, nj, nk, Fs, Rs);
+    tile_inv_dir<T, 2, PRIM, ISCH, IFLUX>(A, B, s, b, i0, j0, k0, ni, nj, nk, Fs, Rs);
+    if (VISC && s.viscous == 1) {
+      if (A.flags[b] != 1) {
+        tile_visc_dir<T, 0>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs);
+        tile_visc_dir<T, 1>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs);
+        tile_visc_dir<T, 2>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs);
+      } else {
+        tile_visc_zero<T, 0>(A, B, i0, j0, k0, ni, nj, nk);
+        tile_visc_zero<T, 1>(A, B, i0, j0, k0, ni, nj, nk);
+        tile_visc_zero<T, 2>(A, B, i0, j0, k0, ni, nj, nk);
+      }
+    }
+    const int nc = ni * nj * nk;
+    for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+      const int i = i0 + q % ni, r = q / ni, j = j0 + r % nj, k = k0 + r / nj;
+      const long long f = fix_(B, i, j, k), fi1 = fix_(B, i + 1, j, k), fj1 = fix_(B, i, j + 1, k), fk1 = fix_(B, i, j, k + 1);
+      T Rm[5];
+#pragma unroll
+      for (int m = 0; m < 5; m++) Rm[m] = Rs[m * MC + q];
+      if (!VISC && s.viscous == 1 && A.flags[b] != 1) {
+        const long long tf = A.tot_face;
+#pragma unroll
+        for (int m = 1; m < 5; m++) {
+          const T* V0 = A.Fv + (0 * 4 + m - 1) * tf;
+          const T* V1 = A.Fv + (1 * 4 + m - 1) * tf;
+          const T* V2 = A.Fv + (2 * 4 + m - 1) * tf;
+          T R = Rm[m];
+          R = R + V0[fi1] - V0[f];
+          R = R + V1[fj1] - V1[f];
+          R = R + V2[fk1] - V2[f];
+          Rm[m] = R;
+        }
+      }
+      cell_finish(A, B, s, b, i, j, k, cix(B, i, j, k), f, fi1, fj1, fk1, Rm);
+    }
+    __syncthreads();
   }
 }
 

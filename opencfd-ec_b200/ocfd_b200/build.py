@@ -1,7 +1,9 @@
 """Builds libocfd_b200.so in-tree with nvcc for sm_100a.
 
 The FP64 translation units (setup.cu, solver_fp64.cu) are compiled with --fmad=false so every
-a*b+c is rounded twice, as the FP64 reference evaluates it; the mixed-precision unit keeps FMA.
+a*b+c is rounded twice, as the FP64 reference evaluates it; the mixed-precision unit keeps FMA and
+the IEEE-rounded FP32 division and square root (the approximate ones made the mixed step 8 % faster
+and its residual norms leave the stated 1e-3 tolerance against FP64 after 10 steps).
 """
 import os
 import subprocess
@@ -25,8 +27,9 @@ UNITS = [
 
 
 def sources():
+    """Everything the library depends on, this file (its compiler flags) included."""
     return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))] + [
-        os.path.join(os.path.dirname(ROOT_DIR), "include", "ocfd_ec_gpu.h")]
+        os.path.join(os.path.dirname(ROOT_DIR), "include", "ocfd_ec_gpu.h"), os.path.abspath(__file__)]
 
 
 def up_to_date():

@@ -37,6 +37,11 @@ def small_cases():
         "foil_sa_muscl2u_sw": lambda: cases.airfoil(ni=65, nj=17, scheme=3, flux=1, turb=2),
         "bump_ud5_ausmpw": lambda: cases.config1(scale=0.25, iflag_scheme=8, iflag_flux=6),
         "foil_sa_ud3_bound_ud1": lambda: cases.airfoil(ni=65, nj=17, scheme=2, flux=4, turb=2, bound_scheme=0),
+        # the wide boundary schemes, whose stencils at a physical face reach 2 (WENO5, UD5) and 3
+        # (WENO7) ghost layers: the primitives are computed on exactly those layers there
+        "foil_sa_weno7_bound_weno7": lambda: cases.airfoil(ni=65, nj=17, scheme=9, flux=4, turb=2, bound_scheme=9),
+        "bump_weno5_bound_weno5": lambda: cases.config1(scale=0.25, cuts_i=(12,), iflag_scheme=7, bound_scheme=7),
+        "foil_lam_ud5_bound_ud5": lambda: cases.airfoil(ni=65, nj=17, scheme=8, flux=6, turb=0, bound_scheme=8),
         "bump_dual_smooth": lambda: cases.config1(scale=0.25, cuts_i=(12,), time_method=-1, dt_global=0.2, step_inner_limit=3,
                                                   res_inner_limit=1e-14, if_residual_smoothing=1),
     }

@@ -6,11 +6,13 @@ cells, WENO5 + Roe, LU-SGS, M 0.8, AoA 3 deg, Re 1e7 per chord (analytic O-H mes
 seeded - no external mesh or dataset).  A step is one NS_Time_advance (residual + LU-SGS +
 update + limiter + BC + halo); the metric is cell-updates/s = cells x steps / device time.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed] [--impl ours|reference] [--shard]
 
 With N > 1 (torchrun) every rank solves its own copy of the case (independent solves at
 different angles of attack, no collective on the data path: "weak" scaling); the timed region is
-bracketed by barriers and the slowest rank's device time is used.  --impl reference times the CPU
+bracketed by barriers and the slowest rank's device time is used.  --shard instead splits one
+config 3 wing-body solve (24 blocks) over the ranks by whole blocks, with the packed interface
+halos crossing by NCCL send/recv every step ("strong" scaling).  --impl reference times the CPU
 restatement of the reference algorithm (oracle/) on the host cores instead (rank 0 only).
 One JSON line is printed by rank 0.
 """
@@ -470,6 +472,106 @@ def run_reference(args, budget_s=150.0):
     return 0
 
 
+def shard_main(args):
+    """--shard: one config 3 wing-body solve (24 blocks) split over the ranks by whole blocks (the
+    reference's automatic partition), each rank's blocks on its GPU, the packed interface halos
+    crossing by NCCL send/recv on the handle's stream every step and the norms and forces
+    all-reduced (ocfd_create_part).  The total work is fixed: strong scaling.  One rank runs the
+    same code path with no peers."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from ocfd_b200 import build, capi, cases
+    from ocfd_b200.shard import ShardedSolver, ThreadComm, TorchComm, partition
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if not os.path.exists(capi.LIB_PATH):
+        build.build()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+        comm, d = TorchComm(), dist
+    else:
+        comm, d = ThreadComm(1).comm(0), None
+    prec = args.precision
+    p, case = cases.config3(precision=1 if prec == "mixed" else 0)
+    owner = partition(case.dims, world)
+    s = ShardedSolver(p, case, owner, rank, comm)
+    stream = torch.cuda.ExternalStream(s.stream())
+    s.advance(args.warmup)
+    s.residual()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if d is not None:
+            d.barrier()
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        s.advance(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), d, "cuda")
+    value = case.ncells * args.steps / (ms * 1e-3)
+    ph = s.profile(3)
+    phases = {k: max_over_ranks(v / 3.0, d, "cuda") for k, v in ph.items()}
+    rmax, rrms = s.residual()
+    _, cl, cd, _ = s.forces()
+    # end to end: this rank's blocks' state from pinned host memory, every step advance + norms +
+    # forces read back, the state back to the host at the end
+    host = [torch.empty(s.state_shape(b), dtype=torch.float64, pin_memory=True).numpy() for b in range(s.nblk)]
+    for b in range(s.nblk):
+        s.get_state(b, out=host[b])
+    e2e_steps = min(args.steps, 50)
+    barrier()
+    t0 = time.perf_counter()
+    for b in range(s.nblk):
+        s.set_state(b, host[b])
+    for _ in range(e2e_steps):
+        s.advance(1)
+        s.residual()
+        s.forces()
+    for b in range(s.nblk):
+        s.get_state(b, out=host[b])
+    t_e2e = max_over_ranks(time.perf_counter() - t0, d, "cuda")
+    state_bytes = sum(h.nbytes for h in host)
+    nb = s.nblk
+    launches = s.launches_per_step() * args.steps
+    s.close()
+    if d is not None:
+        d.barrier()
+        d.destroy_process_group()
+    if rank == 0:
+        peak, peak_kind = peaks()
+        bmodel = BYTES[(prec, int(p.nvar))]
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32/f64", "data": "synthetic (analytic mesh, seeded)",
+            "config": {"workload": describe(p, case) + " block-sharded", "cells": case.ncells, "blocks": len(case.dims),
+                       "precision": prec, "blocks_on_rank0": nb,
+                       "parallelism": "blocks sharded over %d ranks (packed halos by NCCL send/recv each step; "
+                                      "norms and forces all-reduced)" % world,
+                       "l2": "working set %.1f GB > 126 MB L2 (no flush needed)" % (case.ncells * 1200 / 1e9)},
+            "roofline": {"bound": "hbm", "kernel": "residual phase (slowest rank)", "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "traffic": None,
+                         "achieved": bmodel["residual"] * case.ncells / world / (phases["residual"] * 1e-3) / 1e9,
+                         "frac": bmodel["residual"] * case.ncells / world / (phases["residual"] * 1e-3) / 1e9 / peak,
+                         "phase_ms_per_step": phases},
+            "cpu_baseline": None,
+            "e2e": {"value": case.ncells * e2e_steps / t_e2e, "unit": "cell-updates/s", "steps": e2e_steps,
+                    "h2d_bytes_per_step": state_bytes / e2e_steps, "d2h_bytes_per_step": state_bytes / e2e_steps + (14 + 9) * 8},
+            "gpu_launches": launches, "clocks": clk.summary(), "residual_rms": rrms[: int(p.nvar)].tolist(), "cl": cl, "cd": cd,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -483,11 +585,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-extra", action="store_true", help="skip the mixed-precision, batch and serving legs")
     ap.add_argument("--no-converged", action="store_true", help="skip the runs to convergence (mixed vs FP64 error per config)")
+    ap.add_argument("--shard", action="store_true",
+                    help="one config 3 wing-body solve split over the ranks by blocks (NCCL halo exchange, strong scaling) "
+                         "instead of one replica of the workload per rank")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.shard:
+        return shard_main(args)
 
     import numpy as np
     import torch

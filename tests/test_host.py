@@ -221,5 +221,5 @@ def test_bench_reference_arm_runs_on_cpu():
     sys.path.insert(0, ROOT)
     import bench
     for name in ("mixed_leg", "batch_leg", "config3_leg", "serving_leg", "sweep_serving_leg", "converged_leg",
-                 "bench_config", "cpu_sample", "run_reference", "diverges_at", "open_solver", "make_case"):
+                 "bench_config", "cpu_sample", "run_reference", "diverges_at", "open_solver", "make_case", "shard_main"):
         assert callable(getattr(bench, name)), name

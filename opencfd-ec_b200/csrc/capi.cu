@@ -1076,7 +1076,10 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   }
   {
     const char* fz = std::getenv("OCFD_RES_FUSED");  // the tile forms of the residual (opt-in: slower on config 2)
-    h->info.res_fused = fz ? std::max(0, std::min(2, std::atoi(fz))) : 0;
+    h->info.res_fused = fz ? std::max(0, std::min(3, std::atoi(fz))) : 0;
+    // the SA residual as one tile kernel (config 2 FP64 residual 1.85 -> 1.82 ms); OCFD_SA_SPLIT
+    // restores the face-flux kernels + k_sa_res
+    h->info.sa_fused = std::getenv("OCFD_SA_SPLIT") ? 0 : 1;
   }
   {
     int dev = 0;

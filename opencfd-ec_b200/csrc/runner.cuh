@@ -43,7 +43,21 @@ class RunnerT : public Runner {
     lu_wave4_prepare<T, NV, true, 32>();
     lu_wave4_prepare<T, NV, false, 64>();
     lu_wave4_prepare<T, NV, true, 64>();
-    if (I.res_fused) {
+    if (I.sa_fused && NV == 6) {
+      const size_t sm = sa_smem();
+      if (sm > 48 * 1024) cudaFuncSetAttribute(k_sa_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      int occ = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sa_tile<T>, 256, sm);
+      sa_grid_ = std::max(1, std::min(A_.ntile, 148 * std::max(1, occ)));
+    }
+    if (I.res_fused == 3) {
+      const size_t sm = sizeof(T) * 5 * ((size_t)A_.tile_maxf + A_.tile_maxc);
+      auto kern = k_ns_tile<T, true, -1, -1, true, false>;
+      if (sm > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      int occ = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, sm);
+      ns_grid_[4] = std::max(1, std::min(A_.ntile, 148 * std::max(1, occ)));
+    } else if (I.res_fused) {
       ns_prepare<true, S_WENO5, F_ROE>();
       ns_prepare<true, S_MUSCL3, F_ROE>();
       ns_prepare<true, -1, -1>();
@@ -64,10 +78,14 @@ class RunnerT : public Runner {
       k_mu<T><<<grid_of(tc), 256, 0, st>>>(A);
       if (I_.turb == 2 && NV == 6) {
         k_sa_pre<T><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
-        k_sa_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
-        k_sa_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
-        k_sa_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
-        k_sa_res<T><<<grid_of(tc), 256, 0, st>>>(A);
+        if (I_.sa_fused) {
+          k_sa_tile<T><<<sa_grid_, 256, sa_smem(), st>>>(A);
+        } else {
+          k_sa_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
+          k_sa_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
+          k_sa_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+          k_sa_res<T><<<grid_of(tc), 256, 0, st>>>(A);
+        }
         k_mu_finish<T, 1><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
       } else if (I_.turb == 3 && NV == 7) {
         k_sst_pre<T><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
@@ -90,7 +108,14 @@ class RunnerT : public Runner {
     // config 2 FP64, -8 % on config 1; MUSCL3 + AUSMPW was measured slower and is left general)
     const bool weno5_roe = I_.recon_prim && I_.int_scheme == S_WENO5 && I_.int_flux == F_ROE;
     const bool muscl3_roe = I_.recon_prim && I_.int_scheme == S_MUSCL3 && I_.int_flux == F_ROE;
-    if (I_.res_fused) {
+    if (I_.res_fused == 3) {
+      if (weno5_roe) inv_flux<true, S_WENO5, F_ROE>(st);
+      else if (muscl3_roe) inv_flux<true, S_MUSCL3, F_ROE>(st);
+      else if (I_.recon_prim) inv_flux<true, -1, -1>(st);
+      else inv_flux<false, -1, -1>(st);
+      k_inv_kbc<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
+      k_ns_tile<T, true, -1, -1, true, false><<<ns_grid_[4], 256, sizeof(T) * 5 * ((size_t)A.tile_maxf + A.tile_maxc), st>>>(A);
+    } else if (I_.res_fused) {
       if (I_.res_fused == 2 && I_.viscous) {
         k_visc_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
         k_visc_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
@@ -125,6 +150,7 @@ class RunnerT : public Runner {
     }
   }
 
+  size_t sa_smem() const { return sizeof(T) * (2 * (size_t)A_.tile_maxf + 2 * (size_t)A_.tile_maxc); }
   template <bool PRIM, int ISCH, int IFLUX>
   size_t ns_smem() const { return sizeof(T) * 5 * ((size_t)A_.tile_maxf + A_.tile_maxc); }
   template <bool PRIM, int ISCH, int IFLUX>
@@ -288,11 +314,18 @@ class RunnerT : public Runner {
     if (ev) cudaEventRecord(ev[3], st);
   }
   int launches_per_step() const override {
-    int res = 1 + 4 /*inviscid*/ + 1 /*assemble*/ + (I_.smoothing ? 3 : 0);
+    // primitives, then the Navier-Stokes part: inviscid fluxes (3) + k-face central fluxes,
+    // viscous fluxes (3), assembly, or the tile forms in their place
+    const int vis = I_.viscous ? 3 : 0;
+    int res = 1 + (I_.smoothing ? 3 : 0);
+    if (I_.res_fused == 1) res += 1;
+    else if (I_.res_fused == 2) res += vis + 1;
+    else if (I_.res_fused == 3) res += 4 + 1;
+    else res += 4 + vis + 1;
     if (I_.viscous) {
-      res += 1 + 3 + 1;  // mu, viscous fluxes, amut
-      if (I_.turb == 2) res += 6;
-      else if (I_.turb == 3) res += 11;
+      res += 1 + 1;  // mu, amut
+      if (I_.turb == 2 && NV == 6) res += I_.sa_fused ? 3 : 6;  // sa_pre, (tile | 3 fluxes + res), mu_finish
+      else if (I_.turb == 3 && NV == 7) res += 11;
     }
     int lu = I_.lu_planes ? 2 * (I_.max_plane - 2) : (I_.lu_version == 5 ? 3 : 2);
     int upd = 1 + 1 + (NV == 6 ? 3 : 0);
@@ -344,7 +377,8 @@ class RunnerT : public Runner {
   RunInfo I_;
   LuArgs L_{};
   LuStream S_{};
-  int ns_grid_[4] = {1, 1, 1, 1};  // CTAs of k_ns_tile per instantiation (resident CTAs, at most the tiles)
+  int ns_grid_[5] = {1, 1, 1, 1, 1};  // CTAs of k_ns_tile per instantiation (resident CTAs, at most the tiles)
+  int sa_grid_ = 1;                 // CTAs of k_sa_tile
 };
 
 template <class T>

@@ -172,9 +172,51 @@ __global__ void k_sa_pre(Arena<T> A) {
 }
 
 // SA face fluxes Fluxv / Fluxv2 (SA.f90:74-96, 110-131, 145-167) for direction DIR
+// one face of direction DIR: the SA convection + diffusion flux F and the gradient flux G (the
+// face's two Ft plane entries)
+template <class T, int DIR>
+__device__ __forceinline__ void sa_face(const Arena<T>& A, const BlkD& B, const SolveP& s, int i, int j, int k, long long g, T& Fo,
+                                        T& Go) {
+  const long long tb = A.tot_box, tf = A.tot_face;
+  auto vt = [&](int a, int c, int e) -> T { return T(clamp0(A.U[5 * tb + bix(B, a, c, e)])); };
+  const int di = DIR == 0, dj = DIR == 1, dk = DIR == 2;
+  const int im = i - di, jm = j - dj, km = k - dk;  // the other cell of the face
+  T s1x = A.M[(M_NI1 + 3 * DIR) * tf + g], s1y = A.M[(M_NI2 + 3 * DIR) * tf + g], s1z = A.M[(M_NI3 + 3 * DIR) * tf + g];
+  T S = A.M[(M_SI + DIR) * tf + g];
+  T vti, vtj, vtk;
+  if (DIR == 0) {
+    vti = vt(i, j, k) - vt(i - 1, j, k);
+    vtj = T(0.25) * (vt(i, j + 1, k) - vt(i, j - 1, k) + vt(i - 1, j + 1, k) - vt(i - 1, j - 1, k));
+    vtk = T(0.25) * (vt(i, j, k + 1) - vt(i, j, k - 1) + vt(i - 1, j, k + 1) - vt(i - 1, j, k - 1));
+  } else if (DIR == 1) {
+    vti = T(0.25) * (vt(i + 1, j, k) - vt(i - 1, j, k) + vt(i + 1, j - 1, k) - vt(i - 1, j - 1, k));
+    vtj = vt(i, j, k) - vt(i, j - 1, k);
+    vtk = T(0.25) * (vt(i, j, k + 1) - vt(i, j, k - 1) + vt(i, j - 1, k + 1) - vt(i, j - 1, k - 1));
+  } else {
+    vti = T(0.25) * (vt(i + 1, j, k) - vt(i - 1, j, k) + vt(i + 1, j, k - 1) - vt(i - 1, j, k - 1));
+    vtj = T(0.25) * (vt(i, j + 1, k) - vt(i, j - 1, k) + vt(i, j + 1, k - 1) - vt(i, j - 1, k - 1));
+    vtk = vt(i, j, k) - vt(i, j, k - 1);
+  }
+  const int J = DIR == 0 ? M_J1 : (DIR == 1 ? M_J2 : M_J3);
+  T ix = A.M[(J + 0) * tf + g], iy = A.M[(J + 1) * tf + g], iz = A.M[(J + 2) * tf + g];
+  T jx = A.M[(J + 3) * tf + g], jy = A.M[(J + 4) * tf + g], jz = A.M[(J + 5) * tf + g];
+  T kx = A.M[(J + 6) * tf + g], ky = A.M[(J + 7) * tf + g], kz = A.M[(J + 8) * tf + g];
+  T vtx = vti * ix + vtj * jx + vtk * kx, vty = vti * iy + vtj * jy + vtk * ky, vtz = vti * iz + vtj * jz + vtk * kz;
+  long long c0 = bix(B, i, j, k), c1 = bix(B, im, jm, km);
+  T d0 = A.P[P_D * tb + c0], d1 = A.P[P_D * tb + c1];
+  const T cc = T(0.5 * (1.0 + sa::Cb2) / sa::sigma);
+  T v0 = cc * (vt(i, j, k) + A.mu[c0] / d0 + vt(im, jm, km) + A.mu[c1] / d1);
+  T vn1 = A.P[P_U * tb + c1] * s1x + A.P[P_V * tb + c1] * s1y + A.P[P_W * tb + c1] * s1z;
+  T vn2 = A.P[P_U * tb + c0] * s1x + A.P[P_V * tb + c0] * s1y + A.P[P_W * tb + c0] * s1z;
+  T vfi = T(0.5) * ((vn1 + dabs(vn1)) * vt(im, jm, km) + (vn2 - dabs(vn2)) * vt(i, j, k));
+  T gn = vtx * s1x + vty * s1y + vtz * s1z;
+  Fo = (-vfi + v0 / T(s.re) * gn) * S;
+  Go = gn * S;
+}
+
 template <class T, int DIR>
 __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_flux(Arena<T> A) {
-  const long long tb = A.tot_box, tf = A.tot_face;
+  const long long tf = A.tot_face;
   OCFD_GRID_STRIDE(g, tf) {
     int b = find_blk_h(A.pre_face, A.hint_face, A.nblk, g);
     const BlkD& B = A.blk[b];
@@ -183,51 +225,56 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_flux(Arena<T> A) {
     if (DIR == 0 && (j == B.ny || k == B.nz)) continue;
     if (DIR == 1 && (i == B.nx || k == B.nz)) continue;
     if (DIR == 2 && (i == B.nx || j == B.ny)) continue;
-    const SolveP& s = A.sp[B.solve];
-    const T* U6 = nullptr;
-    (void)U6;
-    auto vt = [&](int a, int c, int e) -> T { return T(clamp0(A.U[5 * tb + bix(B, a, c, e)])); };
-    const int di = DIR == 0, dj = DIR == 1, dk = DIR == 2;
-    const int im = i - di, jm = j - dj, km = k - dk;  // the other cell of the face
-    T s1x = A.M[(M_NI1 + 3 * DIR) * tf + g], s1y = A.M[(M_NI2 + 3 * DIR) * tf + g], s1z = A.M[(M_NI3 + 3 * DIR) * tf + g];
-    T S = A.M[(M_SI + DIR) * tf + g];
-    T vti, vtj, vtk;
-    if (DIR == 0) {
-      vti = vt(i, j, k) - vt(i - 1, j, k);
-      vtj = T(0.25) * (vt(i, j + 1, k) - vt(i, j - 1, k) + vt(i - 1, j + 1, k) - vt(i - 1, j - 1, k));
-      vtk = T(0.25) * (vt(i, j, k + 1) - vt(i, j, k - 1) + vt(i - 1, j, k + 1) - vt(i - 1, j, k - 1));
-    } else if (DIR == 1) {
-      vti = T(0.25) * (vt(i + 1, j, k) - vt(i - 1, j, k) + vt(i + 1, j - 1, k) - vt(i - 1, j - 1, k));
-      vtj = vt(i, j, k) - vt(i, j - 1, k);
-      vtk = T(0.25) * (vt(i, j, k + 1) - vt(i, j, k - 1) + vt(i, j - 1, k + 1) - vt(i, j - 1, k - 1));
-    } else {
-      vti = T(0.25) * (vt(i + 1, j, k) - vt(i - 1, j, k) + vt(i + 1, j, k - 1) - vt(i - 1, j, k - 1));
-      vtj = T(0.25) * (vt(i, j + 1, k) - vt(i, j - 1, k) + vt(i, j + 1, k - 1) - vt(i, j - 1, k - 1));
-      vtk = vt(i, j, k) - vt(i, j, k - 1);
-    }
-    const int J = DIR == 0 ? M_J1 : (DIR == 1 ? M_J2 : M_J3);
-    T ix = A.M[(J + 0) * tf + g], iy = A.M[(J + 1) * tf + g], iz = A.M[(J + 2) * tf + g];
-    T jx = A.M[(J + 3) * tf + g], jy = A.M[(J + 4) * tf + g], jz = A.M[(J + 5) * tf + g];
-    T kx = A.M[(J + 6) * tf + g], ky = A.M[(J + 7) * tf + g], kz = A.M[(J + 8) * tf + g];
-    T vtx = vti * ix + vtj * jx + vtk * kx, vty = vti * iy + vtj * jy + vtk * ky, vtz = vti * iz + vtj * jz + vtk * kz;
-    long long c0 = bix(B, i, j, k), c1 = bix(B, im, jm, km);
-    T d0 = A.P[P_D * tb + c0], d1 = A.P[P_D * tb + c1];
-    const T cc = T(0.5 * (1.0 + sa::Cb2) / sa::sigma);
-    T v0 = cc * (vt(i, j, k) + A.mu[c0] / d0 + vt(im, jm, km) + A.mu[c1] / d1);
-    T vn1 = A.P[P_U * tb + c1] * s1x + A.P[P_V * tb + c1] * s1y + A.P[P_W * tb + c1] * s1z;
-    T vn2 = A.P[P_U * tb + c0] * s1x + A.P[P_V * tb + c0] * s1y + A.P[P_W * tb + c0] * s1z;
-    T vfi = T(0.5) * ((vn1 + dabs(vn1)) * vt(im, jm, km) + (vn2 - dabs(vn2)) * vt(i, j, k));
-    T gn = vtx * s1x + vty * s1y + vtz * s1z;
-    A.Ft[(DIR * 2 + 0) * tf + g] = (-vfi + v0 / T(s.re) * gn) * S;
-    A.Ft[(DIR * 2 + 1) * tf + g] = gn * S;
+    T F, G;
+    sa_face<T, DIR>(A, B, A.sp[B.solve], i, j, k, g, F, G);
+    A.Ft[(DIR * 2 + 0) * tf + g] = F;
+    A.Ft[(DIR * 2 + 1) * tf + g] = G;
   }
 }
 
 // Res(6): flux sums in the i, j, k order of SA.f90:99-178 plus the source (180-254)
+// Res(6) of one cell: the SA source (CFL3D form, SA.f90:188-249) added to the flux sum R, stored
+template <class T>
+__device__ __forceinline__ void sa_finish(const Arena<T>& A, const BlkD& B, const SolveP& s, int i, int j, int k, long long g, long long c,
+                                          long long f, T vt0, T mu0, T d0, T R) {
+  const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
+  const T Re = T(s.re);
+  const T* Pu = A.P + P_U * tb;
+  const T* Pv = A.P + P_V * tb;
+  const T* Pw = A.P + P_W * tb;
+  long long cip = bix(B, i + 1, j, k), cim = bix(B, i - 1, j, k), cjp = bix(B, i, j + 1, k), cjm = bix(B, i, j - 1, k);
+  long long ckp = bix(B, i, j, k + 1), ckm = bix(B, i, j, k - 1);
+  T ui = Pu[cip] - Pu[cim], vi = Pv[cip] - Pv[cim], wi = Pw[cip] - Pw[cim];
+  T uj = Pu[cjp] - Pu[cjm], vj = Pv[cjp] - Pv[cjm], wj = Pw[cjp] - Pw[cjm];
+  T uk = Pu[ckp] - Pu[ckm], vk = Pv[ckp] - Pv[ckm], wk = Pw[ckp] - Pw[ckm];
+  T ix = A.M[(M_J0 + 0) * tf + f], iy = A.M[(M_J0 + 1) * tf + f], iz = A.M[(M_J0 + 2) * tf + f];
+  T jx = A.M[(M_J0 + 3) * tf + f], jy = A.M[(M_J0 + 4) * tf + f], jz = A.M[(M_J0 + 5) * tf + f];
+  T kx = A.M[(M_J0 + 6) * tf + f], ky = A.M[(M_J0 + 7) * tf + f], kz = A.M[(M_J0 + 8) * tf + f];
+  T ux = ui * ix + uj * jx + uk * kx, vx = vi * ix + vj * jx + vk * kx, wx = wi * ix + wj * jx + wk * kx;
+  T uy = ui * iy + uj * jy + uk * ky, vy = vi * iy + vj * jy + vk * ky, wy = wi * iy + wj * jy + wk * ky;
+  T uz = ui * iz + uj * jz + uk * kz, vz = vi * iz + vj * jz + vk * kz, wz = wi * iz + wj * jz + wk * kz;
+  (void)ux; (void)vy; (void)wz;
+  T Sv = dsqrt(sq(wy - vz) + sq(uz - wx) + sq(vx - uy));
+  T dw = A.dw[g];
+  T X = d0 * vt0 / mu0;
+  T fv1 = cube(X) / (cube(X) + T(sa::Cv1_3));
+  T fv2 = T(1) - X / (T(1) + X * fv1);
+  T ft2 = T(sa::Ct3) * dexp(-(T(sa::Ct4) * X * X));
+  const T kap = T(sa::kap);
+  T S1 = fmax_(Sv + fv2 * vt0 / (Re * sq(kap * dw)), T(0));
+  T r = fmin_(vt0 / (Re * S1 * kap * kap * dw * dw), T(10));
+  T gg = r + T(sa::Cw2) * (pow6(r) - r);
+  T fw = gg * dpow((T(1) + T(sa::Cw3_6)) / (pow6(gg) + T(sa::Cw3_6)), T(1.0 / 6.0));
+  T Q3 = T(sa::Cb1) * ((T(1) - ft2) * fv2 + ft2) / (kap * kap) - T(sa::Cw1()) * fw;
+  T Q = T(sa::Cb1) * (T(1) - ft2) * S1 * vt0 + Q3 * sq(vt0 / dw) / Re;
+  R = R + Q * A.vol[g];
+  A.Res[5 * tc + g] = R;
+}
+
 template <class T>
 __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_res(Arena<T> A) {
-  const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
-  OCFD_GRID_STRIDE(g, tc) {
+  const long long tb = A.tot_box, tf = A.tot_face;
+  OCFD_GRID_STRIDE(g, A.tot_cell) {
     int b = find_blk_h(A.pre_cell, A.hint_cell, A.nblk, g);
     const BlkD& B = A.blk[b];
     const SolveP& s = A.sp[B.solve];
@@ -243,37 +290,71 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_res(Arena<T> A) {
     T R = F0[fi1] - F0[f] - v0 / Re * (G0[fi1] - G0[f]);
     R = R + F1[fj1] - F1[f] - v0 / Re * (G1[fj1] - G1[f]);
     R = R + F2[fk1] - F2[f] - v0 / Re * (G2[fk1] - G2[f]);
-    // source term (CFL3D form, SA.f90:188-249)
-    const T* Pu = A.P + P_U * tb;
-    const T* Pv = A.P + P_V * tb;
-    const T* Pw = A.P + P_W * tb;
-    long long cip = bix(B, i + 1, j, k), cim = bix(B, i - 1, j, k), cjp = bix(B, i, j + 1, k), cjm = bix(B, i, j - 1, k);
-    long long ckp = bix(B, i, j, k + 1), ckm = bix(B, i, j, k - 1);
-    T ui = Pu[cip] - Pu[cim], vi = Pv[cip] - Pv[cim], wi = Pw[cip] - Pw[cim];
-    T uj = Pu[cjp] - Pu[cjm], vj = Pv[cjp] - Pv[cjm], wj = Pw[cjp] - Pw[cjm];
-    T uk = Pu[ckp] - Pu[ckm], vk = Pv[ckp] - Pv[ckm], wk = Pw[ckp] - Pw[ckm];
-    T ix = A.M[(M_J0 + 0) * tf + f], iy = A.M[(M_J0 + 1) * tf + f], iz = A.M[(M_J0 + 2) * tf + f];
-    T jx = A.M[(M_J0 + 3) * tf + f], jy = A.M[(M_J0 + 4) * tf + f], jz = A.M[(M_J0 + 5) * tf + f];
-    T kx = A.M[(M_J0 + 6) * tf + f], ky = A.M[(M_J0 + 7) * tf + f], kz = A.M[(M_J0 + 8) * tf + f];
-    T ux = ui * ix + uj * jx + uk * kx, vx = vi * ix + vj * jx + vk * kx, wx = wi * ix + wj * jx + wk * kx;
-    T uy = ui * iy + uj * jy + uk * ky, vy = vi * iy + vj * jy + vk * ky, wy = wi * iy + wj * jy + wk * ky;
-    T uz = ui * iz + uj * jz + uk * kz, vz = vi * iz + vj * jz + vk * kz, wz = wi * iz + wj * jz + wk * kz;
-    (void)ux; (void)vy; (void)wz;
-    T Sv = dsqrt(sq(wy - vz) + sq(uz - wx) + sq(vx - uy));
-    T dw = A.dw[g];
-    T X = d0 * vt0 / mu0;
-    T fv1 = cube(X) / (cube(X) + T(sa::Cv1_3));
-    T fv2 = T(1) - X / (T(1) + X * fv1);
-    T ft2 = T(sa::Ct3) * dexp(-(T(sa::Ct4) * X * X));
-    const T kap = T(sa::kap);
-    T S1 = fmax_(Sv + fv2 * vt0 / (Re * sq(kap * dw)), T(0));
-    T r = fmin_(vt0 / (Re * S1 * kap * kap * dw * dw), T(10));
-    T gg = r + T(sa::Cw2) * (pow6(r) - r);
-    T fw = gg * dpow((T(1) + T(sa::Cw3_6)) / (pow6(gg) + T(sa::Cw3_6)), T(1.0 / 6.0));
-    T Q3 = T(sa::Cb1) * ((T(1) - ft2) * fv2 + ft2) / (kap * kap) - T(sa::Cw1()) * fw;
-    T Q = T(sa::Cb1) * (T(1) - ft2) * S1 * vt0 + Q3 * sq(vt0 / dw) / Re;
-    R = R + Q * A.vol[g];
-    A.Res[5 * tc + g] = R;
+    sa_finish(A, B, s, i, j, k, g, c, f, vt0, mu0, d0, R);
+  }
+}
+
+// Res(6) of a tile of cells in one pass: the SA face fluxes F, G of direction i, then j, then k, in
+// shared memory, each cell adding its two faces' terms in the order of k_sa_res, then the source;
+// bit-equal to k_sa_flux + k_sa_res without the Ft planes (faces on a tile border are computed by
+// both tiles that share them)
+template <class T, int DIR>
+__device__ __forceinline__ void tile_sa_dir(const Arena<T>& A, const BlkD& B, const SolveP& s, int i0, int j0, int k0, int ni, int nj,
+                                            int nk, T* Fs, T* Rs, const T* Vs) {
+  const int fa = ni + (DIR == 0), fb = nj + (DIR == 1), fc = nk + (DIR == 2);
+  const int nf = fa * fb * fc, MF = A.tile_maxf;
+  for (int q = threadIdx.x; q < nf; q += blockDim.x) {
+    const int a = q % fa, r = q / fa, bb = r % fb, c = r / fb;
+    T F, G;
+    sa_face<T, DIR>(A, B, s, i0 + a, j0 + bb, k0 + c, fix_(B, i0 + a, j0 + bb, k0 + c), F, G);
+    Fs[q] = F;
+    Fs[MF + q] = G;
+  }
+  __syncthreads();
+  const int nc = ni * nj * nk, step = DIR == 0 ? 1 : (DIR == 1 ? fa : fa * fb);
+  const T Re = T(s.re);
+  for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+    const int a = q % ni, r = q / ni, bb = r % nj, c = r / nj;
+    const int lo = a + fa * (bb + fb * c), hi = lo + step;
+    const T* F = Fs;
+    const T* G = Fs + MF;
+    const T v0 = Vs[q];
+    if (DIR == 0) Rs[q] = F[hi] - F[lo] - v0 / Re * (G[hi] - G[lo]);
+    else Rs[q] = Rs[q] + F[hi] - F[lo] - v0 / Re * (G[hi] - G[lo]);
+  }
+  __syncthreads();
+}
+
+template <class T>
+__global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_tile(Arena<T> A) {
+  extern __shared__ __align__(16) unsigned char sa_smem[];
+  T* Fs = reinterpret_cast<T*>(sa_smem);
+  T* Rs = Fs + 2 * A.tile_maxf;
+  T* Vs = Rs + A.tile_maxc;
+  const long long tb = A.tot_box;
+  for (int t = blockIdx.x; t < A.ntile; t += gridDim.x) {
+    const int4 tl = A.tiles[t];
+    const int b = tl.x, i0 = tl.y, j0 = tl.z, k0 = tl.w;
+    const BlkD& B = A.blk[b];
+    const SolveP& s = A.sp[B.solve];
+    const int ni = min(B.tdim[0], B.nx - i0), nj = min(B.tdim[1], B.ny - j0), nk = min(B.tdim[2], B.nz - k0);
+    const int nc = ni * nj * nk;
+    for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+      const int i = i0 + q % ni, r = q / ni, j = j0 + r % nj, k = k0 + r / nj;
+      const long long c = bix(B, i, j, k);
+      T vt0 = T(clamp0(A.U[5 * tb + c])), mu0 = A.mu[c], d0 = A.P[P_D * tb + c];
+      Vs[q] = (vt0 + mu0 / d0) * T(sa::Cb2) / T(sa::sigma);
+    }
+    tile_sa_dir<T, 0>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs, Vs);
+    tile_sa_dir<T, 1>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs, Vs);
+    tile_sa_dir<T, 2>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs, Vs);
+    for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+      const int i = i0 + q % ni, r = q / ni, j = j0 + r % nj, k = k0 + r / nj;
+      const long long c = bix(B, i, j, k);
+      T vt0 = T(clamp0(A.U[5 * tb + c])), mu0 = A.mu[c], d0 = A.P[P_D * tb + c];
+      sa_finish(A, B, s, i, j, k, cix(B, i, j, k), c, fix_(B, i, j, k), vt0, mu0, d0, Rs[q]);
+    }
+    __syncthreads();
   }
 }
 
@@ -1004,9 +1085,12 @@ __device__ __forceinline__ void tile_visc_zero(const Arena<T>& A, const BlkD& B,
 }
 
 // VISC: the viscous fluxes are computed in the tile too (else k_visc_flux wrote them to Fv, and the
-// cells add them from there, in the same order)
-template <class T, bool PRIM, int ISCH, int IFLUX, bool VISC>
-__global__ void __launch_bounds__(256, InvFluxOccS<T, ISCH>::value) k_ns_tile(Arena<T> A) {
+// cells add them from there, in the same order).  INV: the inviscid fluxes are computed in the tile
+// (else k_inv_flux / k_inv_kbc wrote them to Fi, and the cells start from their differences there)
+template <class T, int ISCH, bool INV>
+struct NsTileOcc { static constexpr int value = INV ? InvFluxOccS<T, ISCH>::value : OCFD_MEM_MINB; };
+template <class T, bool PRIM, int ISCH, int IFLUX, bool VISC, bool INV = true>
+__global__ void __launch_bounds__(256, NsTileOcc<T, ISCH, INV>::value) k_ns_tile(Arena<T> A) {
   extern __shared__ __align__(16) unsigned char ns_smem[];
   T* Fs = reinterpret_cast<T*>(ns_smem);
   T* Rs = Fs + 5 * A.tile_maxf;
@@ -1017,9 +1101,31 @@ __global__ void __launch_bounds__(256, InvFluxOccS<T, ISCH>::value) k_ns_tile(Ar
     const BlkD& B = A.blk[b];
     const SolveP& s = A.sp[B.solve];
     const int ni = min(B.tdim[0], B.nx - i0), nj = min(B.tdim[1], B.ny - j0), nk = min(B.tdim[2], B.nz - k0);
-    tile_inv_dir<T, 0, PRIM, ISCH, IFLUX>(A, B, s, b, i0, j0, k0, ni, nj, nk, Fs, Rs);
-    tile_inv_dir<T, 1, PRIM, ISCH, IFLUX>(A, B, s, b, i0, j0, k0, ni, nj, nk, Fs, Rs);
-    tile_inv_dir<T, 2, PRIM, ISCH, IFLUX>(A, B, s, b, i0, j0, k0, ni, nj, nk, Fs, Rs);
+    if (INV) {
+      tile_inv_dir<T, 0, PRIM, ISCH, IFLUX>(A, B, s, b, i0, j0, k0, ni, nj, nk, Fs, Rs);
+      tile_inv_dir<T, 1, PRIM, ISCH, IFLUX>(A, B, s, b, i0, j0, k0, ni, nj, nk, Fs, Rs);
+      tile_inv_dir<T, 2, PRIM, ISCH, IFLUX>(A, B, s, b, i0, j0, k0, ni, nj, nk, Fs, Rs);
+    } else {
+      const long long tf = A.tot_face;
+      for (int q = threadIdx.x; q < ni * nj * nk; q += blockDim.x) {
+        const int i = i0 + q % ni, r = q / ni, j = j0 + r % nj, k = k0 + r / nj;
+        const long long f = fix_(B, i, j, k), fi1 = fix_(B, i + 1, j, k), fj1 = fix_(B, i, j + 1, k), fk1 = fix_(B, i, j, k + 1);
+        T Rm[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+          const T* F0 = A.Fi + (0 * 5 + m) * tf;
+          const T* F1 = A.Fi + (1 * 5 + m) * tf;
+          const T* F2 = A.Fi + (2 * 5 + m) * tf;
+          T R = F0[fi1] - F0[f];
+          R = R + F1[fj1] - F1[f];
+          R = R + F2[fk1] - F2[f];
+          Rm[m] = R;
+        }
+#pragma unroll
+        for (int m = 0; m < 5; m++) Rs[m * MC + q] = Rm[m];
+      }
+      __syncthreads();
+    }
     if (VISC && s.viscous == 1) {
       if (A.flags[b] != 1) {
         tile_visc_dir<T, 0>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs);

@@ -1,11 +1,13 @@
-"""The tile forms of the Navier-Stokes residual give the bits of the face-flux form.
+"""The tile forms of the residual give the bits of the face-flux form.
 
-By default the residual computes each direction's face fluxes in its own kernel, stores them to
-face planes and assembles Res from them (k_inv_flux, k_inv_kbc, k_visc_flux, k_assemble).  The
-opt-in tile forms (OCFD_RES_FUSED=1: all fluxes of a tile of cells in shared memory; 2: the
-inviscid ones, the viscous ones still from k_visc_flux) must give the same FP64 results, bit for
-bit, on cases with the OverLimit path, physical k faces (the central flux of k_inv_kbc), several
-blocks, tiles cut by block edges (OCFD_RES_TILE) and both reconstructions.
+The Navier-Stokes part of the residual computes each direction's face fluxes in its own kernel,
+stores them to face planes and assembles Res from them (k_inv_flux, k_inv_kbc, k_visc_flux,
+k_assemble); the opt-in tile forms (OCFD_RES_FUSED=1: all fluxes of a tile of cells in shared
+memory; 2: the inviscid ones, the viscous ones still from k_visc_flux; 3: the viscous ones, the
+inviscid ones from k_inv_flux) must give the same FP64 results, bit for bit.  The SA part runs as
+one tile kernel by default (k_sa_tile); OCFD_SA_SPLIT restores k_sa_flux + k_sa_res, which must
+give the same bits too.  Cases cover the OverLimit path, physical k faces (the central flux of
+k_inv_kbc), several blocks, tiles cut by block edges (OCFD_RES_TILE) and both reconstructions.
 """
 import os
 
@@ -14,7 +16,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SWITCHES = ("OCFD_RES_FUSED", "OCFD_RES_TILE")
+SWITCHES = ("OCFD_RES_FUSED", "OCFD_RES_TILE", "OCFD_SA_SPLIT")
 
 
 def run(gpu, p, case, env, nsteps):
@@ -53,18 +55,24 @@ def case_list():
 
 
 CASES = case_list()
-FORMS = (("1", None), ("2", None), ("2", "8,4,200"), ("1", "32,2,1024"))
+FORMS = {
+    "fused1": {"OCFD_RES_FUSED": "1"},
+    "fused2": {"OCFD_RES_FUSED": "2"},
+    "fused2_8x6x4": {"OCFD_RES_FUSED": "2", "OCFD_RES_TILE": "8,4,200"},
+    "fused1_32x16x2": {"OCFD_RES_FUSED": "1", "OCFD_RES_TILE": "32,2,1024"},
+    "fused3": {"OCFD_RES_FUSED": "3"},
+    "fused3_8x6x4": {"OCFD_RES_FUSED": "3", "OCFD_RES_TILE": "8,4,200"},
+    "sa_split": {"OCFD_SA_SPLIT": "1"},
+    "sa_tile_8x6x4_fused1": {"OCFD_RES_FUSED": "1", "OCFD_RES_TILE": "8,4,200"},
+}
 
 
 @pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("form", FORMS, ids=lambda f: "fused%s_%s" % (f[0], f[1] or "default"))
+@pytest.mark.parametrize("form", list(FORMS))
 def test_tile_form_bits(gpu, name, form):
     p, case = CASES[name]
     ref = run(gpu, p, case, {}, 4)
-    env = {"OCFD_RES_FUSED": form[0]}
-    if form[1]:
-        env["OCFD_RES_TILE"] = form[1]
-    got = run(gpu, p, case, env, 4)
+    got = run(gpu, p, case, FORMS[form], 4)
     assert bits_equal(ref[0], got[0]), "state"
     assert bits_equal(ref[1], got[1]), "Res"
     assert np.array_equal(ref[2][0], got[2][0]) and ref[2][1:] == got[2][1:], "forces"
@@ -76,7 +84,7 @@ def test_tile_form_overlimit(gpu):
     import branch_cases
     p, case, warm, preps, steps = branch_cases.limiter_cases()["foil_sa_lusgs"]()
     outs = []
-    for env in ({}, {"OCFD_RES_FUSED": "1"}, {"OCFD_RES_FUSED": "2"}):
+    for env in ({}, {"OCFD_RES_FUSED": "1"}, {"OCFD_RES_FUSED": "2"}, {"OCFD_RES_FUSED": "3"}, {"OCFD_SA_SPLIT": "1"}):
         old = {k: os.environ.get(k) for k in SWITCHES}
         for k in SWITCHES:
             os.environ.pop(k, None)

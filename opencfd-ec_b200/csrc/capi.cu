@@ -1080,6 +1080,9 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     // the SA residual as one tile kernel (config 2 FP64 residual 1.85 -> 1.82 ms); OCFD_SA_SPLIT
     // restores the face-flux kernels + k_sa_res
     h->info.sa_fused = std::getenv("OCFD_SA_SPLIT") ? 0 : 1;
+    // the inviscid fluxes beside the viscosity / turbulence chain on a second stream (config 2 FP64
+    // residual 1.82 -> 1.73 ms); OCFD_RES_ONE_STREAM keeps the residual on the handle's stream
+    h->info.res_streams = std::getenv("OCFD_RES_ONE_STREAM") ? 0 : 1;
   }
   {
     int dev = 0;

@@ -33,7 +33,17 @@ __global__ void k_gather_state(Arena<T> A, int b, double* aos, long long box_b) 
 template <class T, int NV>
 class RunnerT : public Runner {
  public:
+  ~RunnerT() override {
+    if (ev_fork_) cudaEventDestroy(ev_fork_);
+    if (ev_join_) cudaEventDestroy(ev_join_);
+    if (st2_) cudaStreamDestroy(st2_);
+  }
   RunnerT(const Arena<T>& A, const RunInfo& I) : A_(A), I_(I) {
+    if (I.res_streams && I.viscous && !I.res_fused) {
+      cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking);
+      cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming);
+      cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming);
+    }
     if (I.lu) L_ = *I.lu;
     lu_wave3_prepare<T, NV, false, 32>();
     lu_wave3_prepare<T, NV, true, 32>();
@@ -74,6 +84,25 @@ class RunnerT : public Runner {
     const Arena<T>& A = A_;
     const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
     k_prim<T><<<grid_of(tb), 256, 0, st>>>(A);  // sized for the box: the region is read on the device
+    // the inviscid fluxes read only the primitives and the metrics: with a second stream they run
+    // beside the viscosity / turbulence chain (FP64 arithmetic beside memory latency), joined
+    // before the viscous fluxes' assembly
+    const bool weno5_roe = I_.recon_prim && I_.int_scheme == S_WENO5 && I_.int_flux == F_ROE;
+    const bool muscl3_roe = I_.recon_prim && I_.int_scheme == S_MUSCL3 && I_.int_flux == F_ROE;
+    const bool fork = st2_ != nullptr;
+    auto inviscid = [&](cudaStream_t s) {
+      if (weno5_roe) inv_flux<true, S_WENO5, F_ROE>(s);
+      else if (muscl3_roe) inv_flux<true, S_MUSCL3, F_ROE>(s);
+      else if (I_.recon_prim) inv_flux<true, -1, -1>(s);
+      else inv_flux<false, -1, -1>(s);
+      k_inv_kbc<T><<<grid_of(A.tot_subcell), 256, 0, s>>>(A);
+    };
+    if (fork) {
+      cudaEventRecord(ev_fork_, st);
+      cudaStreamWaitEvent(st2_, ev_fork_, 0);
+      inviscid(st2_);
+      cudaEventRecord(ev_join_, st2_);
+    }
     if (I_.viscous) {
       k_mu<T><<<grid_of(tc), 256, 0, st>>>(A);
       if (I_.turb == 2 && NV == 6) {
@@ -106,8 +135,6 @@ class RunnerT : public Runner {
     }
     // specialised instantiations for the WENO5 / MUSCL3 + Roe pairs (residual phase -3 % on
     // config 2 FP64, -8 % on config 1; MUSCL3 + AUSMPW was measured slower and is left general)
-    const bool weno5_roe = I_.recon_prim && I_.int_scheme == S_WENO5 && I_.int_flux == F_ROE;
-    const bool muscl3_roe = I_.recon_prim && I_.int_scheme == S_MUSCL3 && I_.int_flux == F_ROE;
     if (I_.res_fused == 3) {
       if (weno5_roe) inv_flux<true, S_WENO5, F_ROE>(st);
       else if (muscl3_roe) inv_flux<true, S_MUSCL3, F_ROE>(st);
@@ -126,16 +153,13 @@ class RunnerT : public Runner {
       else if (I_.recon_prim) ns_tile<true, -1, -1>(st);
       else ns_tile<false, -1, -1>(st);
     } else {
-      if (weno5_roe) inv_flux<true, S_WENO5, F_ROE>(st);
-      else if (muscl3_roe) inv_flux<true, S_MUSCL3, F_ROE>(st);
-      else if (I_.recon_prim) inv_flux<true, -1, -1>(st);
-      else inv_flux<false, -1, -1>(st);
-      k_inv_kbc<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
+      if (!fork) inviscid(st);
       if (I_.viscous) {
         k_visc_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
         k_visc_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
         k_visc_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
       }
+      if (fork) cudaStreamWaitEvent(st, ev_join_, 0);
       k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
     }
     if (I_.time_method == -1) k_dual_res<T, NV><<<grid_of(tc), 256, 0, st>>>(A);
@@ -379,6 +403,8 @@ class RunnerT : public Runner {
   LuStream S_{};
   int ns_grid_[5] = {1, 1, 1, 1, 1};  // CTAs of k_ns_tile per instantiation (resident CTAs, at most the tiles)
   int sa_grid_ = 1;                 // CTAs of k_sa_tile
+  cudaStream_t st2_ = nullptr;      // the inviscid fluxes' stream when the residual forks (RunInfo::res_streams)
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
 };
 
 template <class T>

@@ -1080,9 +1080,12 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     // the SA residual as one tile kernel (config 2 FP64 residual 1.85 -> 1.82 ms); OCFD_SA_SPLIT
     // restores the face-flux kernels + k_sa_res
     h->info.sa_fused = std::getenv("OCFD_SA_SPLIT") ? 0 : 1;
-    // the inviscid fluxes beside the viscosity / turbulence chain on a second stream (config 2 FP64
-    // residual 1.82 -> 1.73 ms); OCFD_RES_ONE_STREAM keeps the residual on the handle's stream
-    h->info.res_streams = std::getenv("OCFD_RES_ONE_STREAM") ? 0 : 1;
+    // the viscosity / turbulence chain on a second, high-priority stream beside the inviscid fluxes
+    // (config 2 FP64 step 3.32 -> 3.25 ms, mixed 2.50 -> 2.44, 64-airfoil batch 3.55 -> 3.45).
+    // OCFD_RES_STREAMS=0: the whole residual on the handle's stream; 1: the inviscid fluxes on the
+    // second stream, at the default priority
+    const char* rs = std::getenv("OCFD_RES_STREAMS");
+    h->info.res_streams = rs ? std::max(0, std::min(2, std::atoi(rs))) : 2;
   }
   {
     int dev = 0;

@@ -40,7 +40,13 @@ class RunnerT : public Runner {
   }
   RunnerT(const Arena<T>& A, const RunInfo& I) : A_(A), I_(I) {
     if (I.res_streams && I.viscous && !I.res_fused) {
-      cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking);
+      if (I.res_streams == 2) {  // the chain on a high-priority stream, the inviscid fluxes on the handle's
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        cudaStreamCreateWithPriority(&st2_, cudaStreamNonBlocking, hi);
+      } else {
+        cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking);
+      }
       cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming);
       cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming);
     }
@@ -84,9 +90,11 @@ class RunnerT : public Runner {
     const Arena<T>& A = A_;
     const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
     k_prim<T><<<grid_of(tb), 256, 0, st>>>(A);  // sized for the box: the region is read on the device
-    // the inviscid fluxes read only the primitives and the metrics: with a second stream they run
-    // beside the viscosity / turbulence chain (FP64 arithmetic beside memory latency), joined
-    // before the viscous fluxes' assembly
+    // the inviscid fluxes read only the primitives and the metrics: on two streams they run beside
+    // the viscosity / turbulence chain and the viscous fluxes (FP64 arithmetic beside memory
+    // latency), joined before the assembly; the chain, the longer path, gets the higher priority
+    // specialised instantiations for the WENO5 / MUSCL3 + Roe pairs (residual phase -3 % on
+    // config 2 FP64, -8 % on config 1; MUSCL3 + AUSMPW was measured slower and is left general)
     const bool weno5_roe = I_.recon_prim && I_.int_scheme == S_WENO5 && I_.int_flux == F_ROE;
     const bool muscl3_roe = I_.recon_prim && I_.int_scheme == S_MUSCL3 && I_.int_flux == F_ROE;
     const bool fork = st2_ != nullptr;
@@ -97,44 +105,48 @@ class RunnerT : public Runner {
       else inv_flux<false, -1, -1>(s);
       k_inv_kbc<T><<<grid_of(A.tot_subcell), 256, 0, s>>>(A);
     };
+    // cs: the viscosity / turbulence chain and the viscous fluxes; is: the inviscid fluxes
+    cudaStream_t cs = st, is = st;
     if (fork) {
       cudaEventRecord(ev_fork_, st);
       cudaStreamWaitEvent(st2_, ev_fork_, 0);
-      inviscid(st2_);
-      cudaEventRecord(ev_join_, st2_);
+      if (I_.res_streams == 2) cs = st2_;
+      else is = st2_;
+    }
+    if (is != st) {
+      inviscid(is);
+      cudaEventRecord(ev_join_, is);
     }
     if (I_.viscous) {
-      k_mu<T><<<grid_of(tc), 256, 0, st>>>(A);
+      k_mu<T><<<grid_of(tc), 256, 0, cs>>>(A);
       if (I_.turb == 2 && NV == 6) {
-        k_sa_pre<T><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
+        k_sa_pre<T><<<grid_of(A.tot_r1), 256, 0, cs>>>(A);
         if (I_.sa_fused) {
-          k_sa_tile<T><<<sa_grid_, 256, sa_smem(), st>>>(A);
+          k_sa_tile<T><<<sa_grid_, 256, sa_smem(), cs>>>(A);
         } else {
-          k_sa_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
-          k_sa_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
-          k_sa_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
-          k_sa_res<T><<<grid_of(tc), 256, 0, st>>>(A);
+          k_sa_flux<T, 0><<<grid_of(tf), 256, 0, cs>>>(A);
+          k_sa_flux<T, 1><<<grid_of(tf), 256, 0, cs>>>(A);
+          k_sa_flux<T, 2><<<grid_of(tf), 256, 0, cs>>>(A);
+          k_sa_res<T><<<grid_of(tc), 256, 0, cs>>>(A);
         }
-        k_mu_finish<T, 1><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
+        k_mu_finish<T, 1><<<grid_of(A.tot_r1), 256, 0, cs>>>(A);
       } else if (I_.turb == 3 && NV == 7) {
-        k_sst_pre<T><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
-        k_sst_src<T><<<grid_of(tc), 256, 0, st>>>(A);
-        k_sst_mut_ghost<T, 0><<<grid_of(tb), 256, 0, st>>>(A);
-        k_sst_mut_ghost<T, 1><<<grid_of(tb), 256, 0, st>>>(A);
-        k_sst_mut_ghost<T, 2><<<grid_of(tb), 256, 0, st>>>(A);
-        k_amut<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
-        k_sst_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
-        k_sst_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
-        k_sst_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
-        k_sst_res<T><<<grid_of(tc), 256, 0, st>>>(A);
-        k_mu_finish<T, 1><<<grid_of(A.tot_r1), 256, 0, st>>>(A);
+        k_sst_pre<T><<<grid_of(A.tot_r1), 256, 0, cs>>>(A);
+        k_sst_src<T><<<grid_of(tc), 256, 0, cs>>>(A);
+        k_sst_mut_ghost<T, 0><<<grid_of(tb), 256, 0, cs>>>(A);
+        k_sst_mut_ghost<T, 1><<<grid_of(tb), 256, 0, cs>>>(A);
+        k_sst_mut_ghost<T, 2><<<grid_of(tb), 256, 0, cs>>>(A);
+        k_amut<T><<<grid_of(A.tot_subcell), 256, 0, cs>>>(A);
+        k_sst_flux<T, 0><<<grid_of(tf), 256, 0, cs>>>(A);
+        k_sst_flux<T, 1><<<grid_of(tf), 256, 0, cs>>>(A);
+        k_sst_flux<T, 2><<<grid_of(tf), 256, 0, cs>>>(A);
+        k_sst_res<T><<<grid_of(tc), 256, 0, cs>>>(A);
+        k_mu_finish<T, 1><<<grid_of(A.tot_r1), 256, 0, cs>>>(A);
       } else {
-        cudaMemsetAsync(A.mut, 0, sizeof(T) * tb, st);
+        cudaMemsetAsync(A.mut, 0, sizeof(T) * tb, cs);
       }
-      k_amut<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
+      k_amut<T><<<grid_of(A.tot_subcell), 256, 0, cs>>>(A);
     }
-    // specialised instantiations for the WENO5 / MUSCL3 + Roe pairs (residual phase -3 % on
-    // config 2 FP64, -8 % on config 1; MUSCL3 + AUSMPW was measured slower and is left general)
     if (I_.res_fused == 3) {
       if (weno5_roe) inv_flux<true, S_WENO5, F_ROE>(st);
       else if (muscl3_roe) inv_flux<true, S_MUSCL3, F_ROE>(st);
@@ -153,12 +165,13 @@ class RunnerT : public Runner {
       else if (I_.recon_prim) ns_tile<true, -1, -1>(st);
       else ns_tile<false, -1, -1>(st);
     } else {
-      if (!fork) inviscid(st);
+      if (is == st) inviscid(st);
       if (I_.viscous) {
-        k_visc_flux<T, 0><<<grid_of(tf), 256, 0, st>>>(A);
-        k_visc_flux<T, 1><<<grid_of(tf), 256, 0, st>>>(A);
-        k_visc_flux<T, 2><<<grid_of(tf), 256, 0, st>>>(A);
+        k_visc_flux<T, 0><<<grid_of(tf), 256, 0, cs>>>(A);
+        k_visc_flux<T, 1><<<grid_of(tf), 256, 0, cs>>>(A);
+        k_visc_flux<T, 2><<<grid_of(tf), 256, 0, cs>>>(A);
       }
+      if (cs != st) cudaEventRecord(ev_join_, cs);
       if (fork) cudaStreamWaitEvent(st, ev_join_, 0);
       k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
     }

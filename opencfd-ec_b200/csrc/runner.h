@@ -27,7 +27,8 @@ struct RunInfo {
   int int_scheme;         // the interior scheme (Iflag_Scheme) if every solve uses the same one, else -1
   int int_flux;           // the flux (Iflag_Flux) if every solve uses the same one, else -1
   int sa_fused;           // 1: the SA fluxes and Res(6) in one tile kernel (k_sa_tile)
-  int res_streams;        // 1: the inviscid fluxes on a second stream beside the viscosity / turbulence chain
+  int res_streams;        // 0: one stream; 1: the inviscid fluxes on a second stream beside the viscosity /
+                          // turbulence chain; 2: the chain on a second, high-priority stream instead
   int res_fused;          // 0: the NS residual as face-flux kernels + k_assemble; 1: k_ns_tile (all fluxes in the
                           // tile); 2: k_visc_flux, then k_ns_tile with the inviscid fluxes in the tile; 3:
                           // k_inv_flux, then k_ns_tile with the viscous fluxes in the tile

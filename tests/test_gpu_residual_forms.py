@@ -1,13 +1,16 @@
-"""The tile forms of the residual give the bits of the face-flux form.
+"""The forms of the residual give the bits of the face-flux form.
 
 The Navier-Stokes part of the residual computes each direction's face fluxes in its own kernel,
 stores them to face planes and assembles Res from them (k_inv_flux, k_inv_kbc, k_visc_flux,
 k_assemble); the opt-in tile forms (OCFD_RES_FUSED=1: all fluxes of a tile of cells in shared
 memory; 2: the inviscid ones, the viscous ones still from k_visc_flux; 3: the viscous ones, the
 inviscid ones from k_inv_flux) must give the same FP64 results, bit for bit.  The SA part runs as
-one tile kernel by default (k_sa_tile); OCFD_SA_SPLIT restores k_sa_flux + k_sa_res, which must
-give the same bits too.  Cases cover the OverLimit path, physical k faces (the central flux of
-k_inv_kbc), several blocks, tiles cut by block edges (OCFD_RES_TILE) and both reconstructions.
+one tile kernel by default (k_sa_tile); OCFD_SA_SPLIT restores k_sa_flux + k_sa_res.  By default
+the viscosity / turbulence chain runs on a second stream beside the inviscid fluxes; the
+residual issued on one stream (OCFD_RES_STREAMS=0), or with the inviscid fluxes forked instead
+(1), must give the same bits too.  Cases cover the OverLimit path, physical k faces (the central
+flux of k_inv_kbc), several blocks, tiles cut by block edges (OCFD_RES_TILE) and both
+reconstructions.
 """
 import os
 
@@ -16,7 +19,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SWITCHES = ("OCFD_RES_FUSED", "OCFD_RES_TILE", "OCFD_SA_SPLIT")
+SWITCHES = ("OCFD_RES_FUSED", "OCFD_RES_TILE", "OCFD_SA_SPLIT", "OCFD_RES_STREAMS")
 
 
 def run(gpu, p, case, env, nsteps):
@@ -63,6 +66,8 @@ FORMS = {
     "fused3": {"OCFD_RES_FUSED": "3"},
     "fused3_8x6x4": {"OCFD_RES_FUSED": "3", "OCFD_RES_TILE": "8,4,200"},
     "sa_split": {"OCFD_SA_SPLIT": "1"},
+    "one_stream": {"OCFD_RES_STREAMS": "0"},
+    "inviscid_forked": {"OCFD_RES_STREAMS": "1"},
     "sa_tile_8x6x4_fused1": {"OCFD_RES_FUSED": "1", "OCFD_RES_TILE": "8,4,200"},
 }
 

@@ -242,9 +242,18 @@ def batch_leg(args, nsteps=100):
     phases = {k: v / 3 for k, v in b.profile(3).items()}   # ms per step, CUDA events on the handle's stream
     lu = (b.lu_kernel_version(), b.lu_tile_width())
     b.close()
+    # roofline per phase: the phase's algorithmic bytes per cell (mixed, NV = 6) x cells / its time
+    peak, peak_kind = peaks()
+    bm = BYTES[("mixed", 6)]
+    roof = {}
+    for k in ("residual", "lusgs_lower", "lusgs_upper"):
+        if phases.get(k, 0.0) > 0.0:
+            gbs = bm[k] * cells / (phases[k] * 1e-3) / 1e9
+            roof[k] = {"bytes_per_cell": bm[k], "achieved_GBps": gbs, "frac": gbs / peak}
     return {"workload": "config4: 64 NACA 4-digit O-mesh airfoils (k=3), SA, AUSMPW+MUSCL3, mixed, seed 1234",
             "cells": cells, "value": cells * n / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms / n,
             "steps": n, "launches_per_step": launches, "phase_ms_per_step": phases,
+            "phase_roofline": roof, "peak_GBps": peak, "peak_kind": peak_kind,
             "lu_kernel": {"version": lu[0], "tile_columns": lu[1]}}
 
 
@@ -706,6 +715,8 @@ def main():
             extra["mixed"]["speedup_vs_fp64"] = (ms / args.steps) / extra["mixed"]["ms_per_step"]
         if world == 1:
             leg("batch", batch_leg, args)
+            if "value" in extra["batch"]:  # the mixed batch against the FP64 single-solve rate (target 3x)
+                extra["batch"]["vs_fp64_config2"] = extra["batch"]["value"] / value
             leg("config3", config3_leg, args)
             leg("serving", serving_leg)
             leg("sweep_serving", sweep_serving_leg)

@@ -36,6 +36,7 @@ class RunnerT : public Runner {
   ~RunnerT() override {
     if (ev_fork_) cudaEventDestroy(ev_fork_);
     if (ev_join_) cudaEventDestroy(ev_join_);
+    if (ev_mu_) cudaEventDestroy(ev_mu_);
     if (st2_) cudaStreamDestroy(st2_);
   }
   RunnerT(const Arena<T>& A, const RunInfo& I) : A_(A), I_(I) {
@@ -49,6 +50,7 @@ class RunnerT : public Runner {
       }
       cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming);
       cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming);
+      cudaEventCreateWithFlags(&ev_mu_, cudaEventDisableTiming);
     }
     if (I.lu) L_ = *I.lu;
     lu_wave3_prepare<T, NV, false, 32>();
@@ -113,10 +115,7 @@ class RunnerT : public Runner {
       if (I_.res_streams == 2) cs = st2_;
       else is = st2_;
     }
-    if (is != st) {
-      inviscid(is);
-      cudaEventRecord(ev_join_, is);
-    }
+    if (fork) inviscid(is);
     if (I_.viscous) {
       k_mu<T><<<grid_of(tc), 256, 0, cs>>>(A);
       if (I_.turb == 2 && NV == 6) {
@@ -147,6 +146,13 @@ class RunnerT : public Runner {
       }
       k_amut<T><<<grid_of(A.tot_subcell), 256, 0, cs>>>(A);
     }
+    // forked: the spectral radii and dt (they need mu and mu_t) follow the inviscid fluxes on their
+    // stream, beside the viscous fluxes, and the assembly stores Res only
+    if (fork) {
+      cudaEventRecord(ev_mu_, cs);
+      cudaStreamWaitEvent(is, ev_mu_, 0);
+      k_cell_dt<T><<<grid_of(tc), 256, 0, is>>>(A);
+    }
     if (I_.res_fused == 3) {
       if (weno5_roe) inv_flux<true, S_WENO5, F_ROE>(st);
       else if (muscl3_roe) inv_flux<true, S_MUSCL3, F_ROE>(st);
@@ -165,15 +171,20 @@ class RunnerT : public Runner {
       else if (I_.recon_prim) ns_tile<true, -1, -1>(st);
       else ns_tile<false, -1, -1>(st);
     } else {
-      if (is == st) inviscid(st);
+      if (!fork) inviscid(st);
       if (I_.viscous) {
         k_visc_flux<T, 0><<<grid_of(tf), 256, 0, cs>>>(A);
         k_visc_flux<T, 1><<<grid_of(tf), 256, 0, cs>>>(A);
         k_visc_flux<T, 2><<<grid_of(tf), 256, 0, cs>>>(A);
       }
-      if (cs != st) cudaEventRecord(ev_join_, cs);
-      if (fork) cudaStreamWaitEvent(st, ev_join_, 0);
-      k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
+      if (fork) {  // join the second stream back into the handle's
+        cudaStream_t other = cs == st ? is : cs;
+        cudaEventRecord(ev_join_, other);
+        cudaStreamWaitEvent(st, ev_join_, 0);
+        k_assemble<T, true><<<grid_of(tc), 256, 0, st>>>(A);
+      } else {
+        k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
+      }
     }
     if (I_.time_method == -1) k_dual_res<T, NV><<<grid_of(tc), 256, 0, st>>>(A);
     if (I_.smoothing) {  // after the spectral radii, before dt (sub_Residual.f90:110-113); dt does not read Res
@@ -358,7 +369,7 @@ class RunnerT : public Runner {
     if (I_.res_fused == 1) res += 1;
     else if (I_.res_fused == 2) res += vis + 1;
     else if (I_.res_fused == 3) res += 4 + 1;
-    else res += 4 + vis + 1;
+    else res += 4 + vis + 1 + (st2_ ? 1 : 0);  // forked: k_cell_dt beside the viscous fluxes
     if (I_.viscous) {
       res += 1 + 1;  // mu, amut
       if (I_.turb == 2 && NV == 6) res += I_.sa_fused ? 3 : 6;  // sa_pre, (tile | 3 fluxes + res), mu_finish
@@ -416,8 +427,8 @@ class RunnerT : public Runner {
   LuStream S_{};
   int ns_grid_[5] = {1, 1, 1, 1, 1};  // CTAs of k_ns_tile per instantiation (resident CTAs, at most the tiles)
   int sa_grid_ = 1;                 // CTAs of k_sa_tile
-  cudaStream_t st2_ = nullptr;      // the inviscid fluxes' stream when the residual forks (RunInfo::res_streams)
-  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+  cudaStream_t st2_ = nullptr;      // the second stream of a forked residual (RunInfo::res_streams)
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr, ev_mu_ = nullptr;
 };
 
 template <class T>

@@ -912,51 +912,58 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_visc_flux(Arena<T> A) {
 // ============================================================================================
 // the cell part of the assembly: spectral radii (comput_Lijk, sub_time_acceleraction.f90:7-56) and
 // local dt (comput_dt, 61-112) from the primitives, then the stores of Res(1:5) = Rm, Lc, Lv, dt;
-// f / fi1 / fj1 / fk1 are the cell's faces in the face index space, g its cell index
-template <class T>
+// f / fi1 / fj1 / fk1 are the cell's faces in the face index space, g its cell index.  RES / LDT:
+// store Res / compute and store Lc, Lv, dt (the two parts read disjoint inputs)
+template <class T, bool RES = true, bool LDT = true>
 __device__ __forceinline__ void cell_finish(const Arena<T>& A, const BlkD& B, const SolveP& s, int b, int i, int j, int k, long long g,
                                             long long f, long long fi1, long long fj1, long long fk1, const T* Rm) {
   const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
-  long long c = bix(B, i, j, k);
-  T D0 = T(0);
-  if (s.viscous == 1) {
-    T gm = T(s.gamma), f43 = T((double)(4.0f / 3.0f));  // `4./3.` default-real literal
-    D0 = fmax_(gm, f43) / A.P[P_D * tb + c] * (A.mu[c] / T(s.prl) + A.mut[c] / T(s.prt));
-  }
-  T vol = A.vol[g];
-  T vol1 = T(1) / vol;
-  T uu = A.P[P_U * tb + c], v = A.P[P_V * tb + c], w = A.P[P_W * tb + c], cc = A.P[P_C * tb + c];
-  T L[6];
+  T L[6], dtv;
+  if (LDT) {
+    long long c = bix(B, i, j, k);
+    T D0 = T(0);
+    if (s.viscous == 1) {
+      T gm = T(s.gamma), f43 = T((double)(4.0f / 3.0f));  // `4./3.` default-real literal
+      D0 = fmax_(gm, f43) / A.P[P_D * tb + c] * (A.mu[c] / T(s.prl) + A.mut[c] / T(s.prt));
+    }
+    T vol = A.vol[g];
+    T vol1 = T(1) / vol;
+    T uu = A.P[P_U * tb + c], v = A.P[P_V * tb + c], w = A.P[P_W * tb + c], cc = A.P[P_C * tb + c];
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
-    long long fo = d == 0 ? fi1 : (d == 1 ? fj1 : fk1);
-    const T* n1 = A.M + (M_NI1 + 3 * d) * tf;
-    const T* n2 = A.M + (M_NI2 + 3 * d) * tf;
-    const T* n3 = A.M + (M_NI3 + 3 * d) * tf;
-    const T* Sd = A.M + (M_SI + d) * tf;
-    T un = T(0.5) * (uu * (n1[f] + n1[fo]) + v * (n2[f] + n2[fo]) + w * (n3[f] + n3[fo]));
-    T S0 = (Sd[f] + Sd[fo]) * T(0.5);
-    L[d] = (dabs(un) + cc) * S0;
-    L[3 + d] = D0 * S0 * S0 * vol1;
+    for (int d = 0; d < 3; d++) {
+      long long fo = d == 0 ? fi1 : (d == 1 ? fj1 : fk1);
+      const T* n1 = A.M + (M_NI1 + 3 * d) * tf;
+      const T* n2 = A.M + (M_NI2 + 3 * d) * tf;
+      const T* n3 = A.M + (M_NI3 + 3 * d) * tf;
+      const T* Sd = A.M + (M_SI + d) * tf;
+      T un = T(0.5) * (uu * (n1[f] + n1[fo]) + v * (n2[f] + n2[fo]) + w * (n3[f] + n3[fo]));
+      T S0 = (Sd[f] + Sd[fo]) * T(0.5);
+      L[d] = (dabs(un) + cc) * S0;
+      L[3 + d] = D0 * S0 * S0 * vol1;
+    }
+    if (s.local_dt == 1) {
+      T dt_fac = A.flags[b] == 0 ? T(1) : T(0.1);
+      dtv = dt_fac * T(s.cfl) * vol / (L[0] + L[1] + L[2] + T(1) * (L[3] + L[4] + L[5]));
+      if (s.dtime_mesh == 1) dtv = dtv * A.dtm[g];
+      if (dtv > T(s.dtmax)) dtv = T(s.dtmax);
+      if (dtv < T(s.dtmin)) dtv = T(s.dtmin);
+    } else {
+      dtv = T(s.dt_global);
+    }
   }
-  T dtv;
-  if (s.local_dt == 1) {
-    T dt_fac = A.flags[b] == 0 ? T(1) : T(0.1);
-    dtv = dt_fac * T(s.cfl) * vol / (L[0] + L[1] + L[2] + T(1) * (L[3] + L[4] + L[5]));
-    if (s.dtime_mesh == 1) dtv = dtv * A.dtm[g];
-    if (dtv > T(s.dtmax)) dtv = T(s.dtmax);
-    if (dtv < T(s.dtmin)) dtv = T(s.dtmin);
-  } else {
-    dtv = T(s.dt_global);
+  if (RES) {
+#pragma unroll
+    for (int m = 0; m < 5; m++) A.Res[m * tc + g] = Rm[m];
   }
+  if (LDT) {
 #pragma unroll
-  for (int m = 0; m < 5; m++) A.Res[m * tc + g] = Rm[m];
-#pragma unroll
-  for (int d = 0; d < 3; d++) { A.Lc[d * tc + g] = L[d]; A.Lv[d * tc + g] = L[3 + d]; }
-  A.dt[g] = dtv;
+    for (int d = 0; d < 3; d++) { A.Lc[d * tc + g] = L[d]; A.Lv[d * tc + g] = L[3 + d]; }
+    A.dt[g] = dtv;
+  }
 }
 
-template <class T>
+// RES_ONLY: Lc, Lv and dt were computed by k_cell_dt (the two-stream residual)
+template <class T, bool RES_ONLY = false>
 __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
   const long long tf = A.tot_face, tc = A.tot_cell;
   OCFD_GRID_STRIDE(g, tc) {
@@ -988,7 +995,20 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_assemble(Arena<T> A) {
       }
       Rm[m] = R;
     }
-    cell_finish(A, B, s, b, i, j, k, g, f, fi1, fj1, fk1, Rm);
+    cell_finish<T, true, !RES_ONLY>(A, B, s, b, i, j, k, g, f, fi1, fj1, fk1, Rm);
+  }
+}
+
+// the spectral radii and dt of every cell (the assembly's cell part without Res)
+template <class T>
+__global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_cell_dt(Arena<T> A) {
+  OCFD_GRID_STRIDE(g, A.tot_cell) {
+    int b = find_blk_h(A.pre_cell, A.hint_cell, A.nblk, g);
+    const BlkD& B = A.blk[b];
+    int i, j, k;
+    dec_cell(B, g - B.ocell, i, j, k);
+    cell_finish<T, false, true>(A, B, A.sp[B.solve], b, i, j, k, g, fix_(B, i, j, k), fix_(B, i + 1, j, k), fix_(B, i, j + 1, k),
+                                fix_(B, i, j, k + 1), nullptr);
   }
 }
 

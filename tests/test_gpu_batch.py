@@ -114,3 +114,34 @@ def test_reset_solve_starts_over_like_a_new_handle(gpu, precision):
         assert np.array_equal(bt.get_state(k), ref.get_state(k))
     for s in (bt, alone, ref):
         s.close()
+
+
+def test_reset_solve_with_a_wider_boundary_scheme(gpu):
+    """A reset that changes a slot's boundary scheme to one whose stencil reaches deeper across a
+    physical face (MUSCL2C, one ghost layer, to WENO7, three) recomputes the primitive region: the
+    slot then equals a new handle with the case alone, bit for bit, and the other slot is untouched.
+    A reset to a reconstruction the step was not built for is refused."""
+    from ocfd_b200 import cases
+    from ocfd_b200.capi import OcfdError
+    a = cases.airfoil(ni=65, nj=17, ma=0.6, aoa=1.0)
+    b = cases.airfoil(ni=81, nj=21, ma=0.7, aoa=2.5, m=0.03)
+    c = cases.airfoil(ni=81, nj=21, ma=0.6, aoa=3.0, m=0.03, scheme=9, bound_scheme=9)   # b's mesh
+    assert int(b[0].bound_scheme) == 4 and int(c[0].bound_scheme) == 9
+    bt = gpu.Batch([a, b])
+    bt.advance(10)
+    bt.reset_solve(1, c[0])
+    bt.advance(10)
+    alone = gpu.Solver(*c)
+    alone.advance(10)
+    nb0 = len(a[1].dims)
+    for k in range(alone.nblk):
+        assert np.array_equal(bt.get_state(nb0 + k), alone.get_state(k))
+    ref = gpu.Batch([a, b])
+    ref.advance(20)
+    for k in range(nb0):
+        assert np.array_equal(bt.get_state(k), ref.get_state(k))
+    d = cases.airfoil(ni=81, nj=21, ma=0.6, aoa=3.0, m=0.03, iflag_reconstruction=1)
+    with pytest.raises(OcfdError):
+        bt.reset_solve(1, d[0])
+    for s in (bt, alone, ref):
+        s.close()

@@ -657,11 +657,16 @@ def main():
     single = [k for k in ("lusgs_lower", "lusgs_upper") if ph[k] > 0.0]
     dom = max(single, key=lambda k: ph[k]) if single else "residual"
     luv, lutc = s.lu_kernel_version(), s.lu_tile_width()
+    one_launch = s.lu_one_launch()
     kernel_name = {"lusgs_lower": "k_lusgs_wave%d<lower, %d columns>" % (luv, lutc),
                    "lusgs_upper": "k_lusgs_wave%d<upper, %d columns>" % (luv, lutc),
                    "residual": "residual phase (all flux/source kernels)"}[dom]
+    dom_bytes = bmodel[dom]
+    if one_launch and dom == "lusgs_lower":  # both sweeps in one launch: their joint bytes and time
+        kernel_name = "k_lusgs_wave4_ul<both sweeps, %d columns>" % lutc
+        dom_bytes = bmodel["lusgs_lower"] + bmodel["lusgs_upper"]
     t_dom = ph[dom] / 3.0 * 1e-3
-    achieved = bmodel[dom] * ncell / t_dom / 1e9
+    achieved = dom_bytes * ncell / t_dom / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tfile):
@@ -669,12 +674,14 @@ def main():
             with open(tfile) as f:
                 tj = json.load(f)
             key = "%s/%s" % (prec, dom)
-            if key in tj:
+            if one_launch and dom == "lusgs_lower":
+                traffic = sum(tj["%s/%s" % (prec, k)]["bytes_per_cell"] for k in ("lusgs_lower", "lusgs_upper")) * ncell
+            elif key in tj:
                 traffic = tj[key]["bytes_per_cell"] * ncell
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic, "bytes_per_cell": bmodel[dom],
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic, "bytes_per_cell": dom_bytes,
                 "launch_ms": t_dom * 1e3, "phase_ms_per_step": {k: v / 3.0 for k, v in ph.items()},
                 "residual_phase_GBps": bmodel["residual"] * ncell / (ph["residual"] / 3.0 * 1e-3) / 1e9}
 

@@ -399,6 +399,8 @@ static void select_lu(ocfd_handle* h, int v, int ver) {
   if (ver == 5 && h->lus_v != v) ver = 4;   // records exist for one tile table only
   h->lu = h->lu_var[v];
   h->lu_tc = v == 0 ? 32 : 64;
+  h->info.lu_fused = ver == 6 ? 1 : 0;      // 6: version 4 with both sweeps in one launch
+  if (ver == 6) ver = 4;
   h->info.lu_version = ver;
   h->info.lu = &h->lu;
   h->info.lu_tc = h->lu_tc;
@@ -456,6 +458,9 @@ static void autotune_lu(ocfd_handle* h, const std::vector<std::pair<int, int>>& 
 
 extern "C" int ocfd_lu_tile_width(const ocfd_handle* h) { return h ? h->lu_tc : 0; }
 extern "C" int ocfd_lu_kernel_version(const ocfd_handle* h) { return h ? h->info.lu_version : 0; }
+extern "C" int ocfd_lu_one_launch(const ocfd_handle* h) {
+  return h && !h->info.lu_planes && h->info.lu_version == 4 && h->info.lu_fused ? 1 : 0;
+}
 
 // all solves of a handle share the model switches that select kernels; Mach, angles, Re, CFL,
 // schemes, fluxes and limits may differ per solve
@@ -994,14 +999,33 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     }
     std::stable_sort(order.begin(), order.end(), [](const std::pair<int, LuTile>& a, const std::pair<int, LuTile>& b) { return a.first < b.first; });
     for (auto& o : order) tiles.push_back(o.second);
+    // the upper sweep's order when both sweeps share one launch: by the step at which a tile could
+    // start (its block's lower sweep done, then the skew of its upstream tiles); an upstream tile
+    // (J+1 or K+1) always sorts strictly earlier, so every wait is on a tile handed out before
+    std::vector<std::pair<long long, LuTile>> uorder;
+    for (const LuTile& t : tiles) {
+      const BlkD& B = h->blk[t.blk];
+      const int nJ = tile_of[3 * t.blk + 1], nK = tile_of[3 * t.blk + 2];
+      const int J = (t.j0 - 1) / TJ, K = (t.k0 - 1) / TK;
+      const long long lower_done = (long long)(nJ - 1) * TJ + (long long)(nK - 1) * TK + (B.nx - 1 + TJ + TK - 2);
+      uorder.push_back({lower_done + (long long)(nJ - 1 - J) * TJ + (long long)(nK - 1 - K) * TK, t});
+    }
+    std::stable_sort(uorder.begin(), uorder.end(), [](const std::pair<long long, LuTile>& a, const std::pair<long long, LuTile>& b) { return a.first < b.first; });
+    std::vector<LuTile> utiles;
+    for (auto& o : uorder) utiles.push_back(o.second);
     LuTile* d_tiles = M.alloc<LuTile>(tiles.size(), e);
+    LuTile* d_utiles = M.alloc<LuTile>(utiles.size(), e);
     int* d_tile_of = M.alloc<int>(tile_of.size(), e);
     int* d_progress = M.alloc<int>(first, e);
+    int* d_progress_up = M.alloc<int>(first, e);
+    int* d_blkdone = M.alloc<int>(nblk, e);
     if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "lu tables"); }
     cudaMemcpy(d_tiles, tiles.data(), tiles.size() * sizeof(LuTile), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_utiles, utiles.data(), utiles.size() * sizeof(LuTile), cudaMemcpyHostToDevice);
     cudaMemcpy(d_tile_of, tile_of.data(), tile_of.size() * sizeof(int), cudaMemcpyHostToDevice);
     LuArgs& L = h->lu_var[v];
-    L.tiles = d_tiles; L.ntiles = first; L.counter = d_counter; L.progress = d_progress;
+    L.tiles = d_tiles; L.utiles = d_utiles; L.ntiles = first; L.counter = d_counter; L.progress = d_progress;
+    L.progress_up = d_progress_up; L.blkdone = d_blkdone;
     L.tile_of = d_tile_of; L.err = h->d_lu_err; L.TJ = TJ; L.TK = TK;
     L.spin_limit = 4000000;  // x ~64 ns: a few hundred ms before a stuck wait gives up
     if (const char* sl = std::getenv("OCFD_LU_SPIN_LIMIT")) L.spin_limit = std::max(0LL, std::atoll(sl));
@@ -1077,6 +1101,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   {
     const char* fz = std::getenv("OCFD_RES_FUSED");  // the tile forms of the residual (opt-in: slower on config 2)
     h->info.res_fused = fz ? std::max(0, std::min(3, std::atoi(fz))) : 0;
+
     // the SA residual as one tile kernel (config 2 FP64 residual 1.85 -> 1.82 ms); OCFD_SA_SPLIT
     // restores the face-flux kernels + k_sa_res
     h->info.sa_fused = std::getenv("OCFD_SA_SPLIT") ? 0 : 1;
@@ -1095,14 +1120,19 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   if (h->prec == OCFD_PREC_MIXED) fill_arena<float>(h, h->A32, h->d_Mf, h->d_volf, h->d_dtmf, h->d_dwf);
   else fill_arena<double>(h, h->A64, h->d_Md, h->d_vold, h->d_dtmd, h->d_dwd);
   // LU-SGS kernel candidates: OCFD_LU_TC fixes the tile width, OCFD_LU_V3 / OCFD_LU_V4 the
-  // wavefront version (OCFD_LU_V2 both); the autotuner picks among the rest
+  // wavefront version (OCFD_LU_V2 both); the autotuner picks among the rest.  Candidate 6 is
+  // version 4 with both sweeps in one launch (k_lusgs_wave4_ul: faster where blocks of very
+  // different depth run together, as in a batch; OCFD_LU_SPLIT leaves it out)
   const int lu_ver_force = lu_v2 ? 2 : (std::getenv("OCFD_LU_V3") ? 3 : (std::getenv("OCFD_LU_V4") ? 4 : (std::getenv("OCFD_LU_V5") ? 5 : 0)));
+  const bool lu_split = std::getenv("OCFD_LU_SPLIT") != nullptr, lu_one = std::getenv("OCFD_LU_ONE_LAUNCH") != nullptr;
   std::vector<std::pair<int, int>> lu_cand;
   for (int v = 0; v < 2; v++) {
     if (lu_force && (lu_force == 64) != (v == 1)) continue;
-    for (int ver : {5, 4, 3}) {
-      if (lu_ver_force && ver != lu_ver_force) continue;
+    for (int ver : {5, 4, 6, 3}) {
+      if (lu_ver_force && ver != lu_ver_force && !(ver == 6 && lu_ver_force == 4)) continue;
       if (ver == 5 && (h->lus_v != v || lu_ver_force != 5)) continue;
+      if (ver == 6 && lu_split) continue;
+      if (ver == 4 && lu_one && !lu_split) continue;
       lu_cand.push_back({v, ver});
     }
   }

@@ -61,6 +61,8 @@ class RunnerT : public Runner {
     lu_wave4_prepare<T, NV, true, 32>();
     lu_wave4_prepare<T, NV, false, 64>();
     lu_wave4_prepare<T, NV, true, 64>();
+    lu_wave4_ul_prepare<T, NV, 32>();
+    lu_wave4_ul_prepare<T, NV, 64>();
     if (I.sa_fused && NV == 6) {
       const size_t sm = sa_smem();
       if (sm > 48 * 1024) cudaFuncSetAttribute(k_sa_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -234,6 +236,7 @@ class RunnerT : public Runner {
       if (!upper) for (int p = 3; p <= I_.max_plane; p++) k_lusgs<T, NV, false><<<gc, 128, 0, st>>>(A, p);
       else for (int p = I_.max_plane; p >= 3; p--) k_lusgs<T, NV, true><<<gc, 128, 0, st>>>(A, p);
     } else {
+      if (upper && I_.lu_version == 4 && I_.lu_fused) return;  // ran with the lower sweep's launch
       if (!upper) cudaMemsetAsync(L_.counter, 0, 2 * sizeof(int), st);
       cudaMemsetAsync(L_.progress, 0, sizeof(int) * L_.ntiles, st);
       if (I_.lu_version == 5) {
@@ -250,6 +253,11 @@ class RunnerT : public Runner {
       } else if (I_.lu_version == 2) {
         if (!upper) k_lusgs_wave<T, NV, false><<<I_.lu_grid, 64, 0, st>>>(A, L_);
         else k_lusgs_wave<T, NV, true><<<I_.lu_grid, 64, 0, st>>>(A, L_);
+      } else if (I_.lu_version == 4 && I_.lu_fused) {  // both sweeps in one launch, issued with the lower one
+        cudaMemsetAsync(L_.progress_up, 0, sizeof(int) * L_.ntiles, st);
+        cudaMemsetAsync(L_.blkdone, 0, sizeof(int) * A.nblk, st);
+        if (I_.lu_tc == 64) k_lusgs_wave4_ul<T, NV, 64><<<I_.lu_grid, 4 * 64 + 64, lu_wave4_smem<T, NV, false, 64>(), st>>>(A, L_);
+        else k_lusgs_wave4_ul<T, NV, 32><<<I_.lu_grid, 4 * 32 + 64, lu_wave4_smem<T, NV, false, 32>(), st>>>(A, L_);
       } else if (I_.lu_version == 4 && I_.lu_tc == 64) {
         if (!upper) k_lusgs_wave4<T, NV, false, 64><<<I_.lu_grid, 4 * 64 + 64, lu_wave4_smem<T, NV, false, 64>(), st>>>(A, L_);
         else k_lusgs_wave4<T, NV, true, 64><<<I_.lu_grid, 4 * 64 + 64, lu_wave4_smem<T, NV, true, 64>(), st>>>(A, L_);
@@ -375,7 +383,7 @@ class RunnerT : public Runner {
       if (I_.turb == 2 && NV == 6) res += I_.sa_fused ? 3 : 6;  // sa_pre, (tile | 3 fluxes + res), mu_finish
       else if (I_.turb == 3 && NV == 7) res += 11;
     }
-    int lu = I_.lu_planes ? 2 * (I_.max_plane - 2) : (I_.lu_version == 5 ? 3 : 2);
+    int lu = I_.lu_planes ? 2 * (I_.max_plane - 2) : (I_.lu_version == 5 ? 3 : (I_.lu_version == 4 && I_.lu_fused ? 1 : 2));
     int upd = 1 + 1 + (NV == 6 ? 3 : 0);
     int nbc = 0;
     for (int r = 0; r < I_.nround; r++) nbc += I_.bc_rounds[3 * r + 2] > 0;

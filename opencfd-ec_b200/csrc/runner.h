@@ -23,6 +23,7 @@ struct RunInfo {
   const LuStream* lus;    // version 5: record layout and buffers (host copy of the kernel argument)
   int lu5_grid[2];        // version 5: CTAs of the lower / upper sweep (resident CTAs, at most the tiles)
   int lu_tc;              // columns per tile (32 or 64)
+  int lu_fused;           // version 4: both sweeps in one launch (k_lusgs_wave4_ul)
   int recon_prim;         // 1: every solve reconstructs primitive variables
   int int_scheme;         // the interior scheme (Iflag_Scheme) if every solve uses the same one, else -1
   int int_flux;           // the flux (Iflag_Flux) if every solve uses the same one, else -1

@@ -22,7 +22,7 @@ EXPORTED = [
     "ocfd_limiter_status", "ocfd_array_shape", "ocfd_get_array", "ocfd_version", "ocfd_compute_residual",
     "ocfd_stream", "ocfd_profile", "ocfd_launches_per_step", "ocfd_create_batch", "ocfd_nsolve", "ocfd_reset_solve",
     "ocfd_residual_all", "ocfd_forces_all", "ocfd_footprint", "ocfd_synchronize", "ocfd_residual_static",
-    "ocfd_lu_tile_width", "ocfd_lu_kernel_version", "ocfd_create_part", "ocfd_part_blocks", "ocfd_part_plan",
+    "ocfd_lu_tile_width", "ocfd_lu_kernel_version", "ocfd_lu_one_launch", "ocfd_create_part", "ocfd_part_blocks", "ocfd_part_plan",
 ]
 
 
@@ -74,6 +74,7 @@ def lib():
         L.ocfd_residual_static.argtypes = [vp, dp, dp]
         L.ocfd_lu_tile_width.argtypes = [vp]
         L.ocfd_lu_kernel_version.argtypes = [vp]
+        L.ocfd_lu_one_launch.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -233,6 +234,10 @@ class Solver:
     def lu_kernel_version(self):
         """LU-SGS wavefront kernel version in use (3 or 4; 2 with OCFD_LU_V2), as picked at creation."""
         return int(lib().ocfd_lu_kernel_version(self.h))
+
+    def lu_one_launch(self):
+        """True when both LU-SGS sweeps run as one launch (profile() then reports them as the lower one)."""
+        return bool(lib().ocfd_lu_one_launch(self.h))
 
     def synchronize(self):
         self._check(lib().ocfd_synchronize(self.h), "synchronize")

@@ -1,7 +1,8 @@
 """Every LU-SGS wavefront variant gives the hyperplane-order bits.
 
 The creation-time autotuner picks a tile width (32 or 64 columns) and a wavefront kernel version
-(3: inputs staged by element; 4: staged by 32-byte sector, helper warps off the step phases; 5:
+(3: inputs staged by element; 4: staged by 32-byte sector, helper warps off the step phases, both
+sweeps in one launch unless OCFD_LU_SPLIT; 5:
 inputs packed in sweep order and fetched by one bulk copy per step, 64-column tiles) per case; the
 choice must never change a result.  Each variant is forced here through its switches and
 compared bit for bit with the one-launch-per-hyperplane sweep (OCFD_LUSGS_PLANES=1), on cases that
@@ -16,8 +17,13 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SWITCHES = ("OCFD_LU_V3", "OCFD_LU_V4", "OCFD_LU_V5", "OCFD_LU_TC", "OCFD_LUSGS_PLANES", "OCFD_NO_AUTOTUNE")
-VARIANTS = (("3", "32"), ("3", "64"), ("4", "32"), ("4", "64"), ("5", "64"))
+SWITCHES = ("OCFD_LU_V3", "OCFD_LU_V4", "OCFD_LU_V5", "OCFD_LU_TC", "OCFD_LUSGS_PLANES", "OCFD_NO_AUTOTUNE", "OCFD_LU_SPLIT",
+            "OCFD_LU_ONE_LAUNCH")
+# (version, tile width, extra switches): version 4 as two launches (OCFD_LU_SPLIT) and with both
+# sweeps in one launch (OCFD_LU_ONE_LAUNCH)
+SPLIT, ONE = {"OCFD_LU_SPLIT": "1"}, {"OCFD_LU_ONE_LAUNCH": "1"}
+VARIANTS = (("3", "32", {}), ("3", "64", {}), ("4", "32", SPLIT), ("4", "64", SPLIT), ("4", "32", ONE), ("4", "64", ONE),
+            ("5", "64", {}))
 
 
 def run(gpu, p, case, env, nsteps):
@@ -34,6 +40,7 @@ def run(gpu, p, case, env, nsteps):
             else:
                 os.environ[k] = v
     ver, tc = s.lu_kernel_version(), s.lu_tile_width()
+    run.one_launch = s.lu_one_launch()
     s.advance(nsteps)
     U = [s.get_state(b) for b in range(s.nblk)]
     DU = [s.get_array(b, "DU")[0] for b in range(s.nblk)]
@@ -68,11 +75,12 @@ NAMES = ["config2_small_sa", "config3_small_sst", "config1_euler_2blk", "config2
 def test_every_wavefront_variant_equals_hyperplanes(gpu, name):
     p, case = case_list()[name]
     refU, refDU, _, _ = run(gpu, p, case, {"OCFD_LUSGS_PLANES": "1"}, 3)
-    for ver, tc in VARIANTS:
-        U, DU, v, t = run(gpu, p, case, {"OCFD_LU_V" + ver: "1", "OCFD_LU_TC": tc}, 3)
+    for ver, tc, extra in VARIANTS:
+        U, DU, v, t = run(gpu, p, case, dict({"OCFD_LU_V" + ver: "1", "OCFD_LU_TC": tc}, **extra), 3)
         assert (v, t) == (int(ver), int(tc))
-        assert bits_equal(U, refU), (name, ver, tc)
-        assert bits_equal(DU, refDU), (name, ver, tc)
+        assert run.one_launch == (extra is ONE)
+        assert bits_equal(U, refU), (name, ver, tc, extra)
+        assert bits_equal(DU, refDU), (name, ver, tc, extra)
 
 
 @pytest.mark.parametrize("name", ["config2_small_sa", "config3_small_sst"])
@@ -88,8 +96,8 @@ def test_mixed_wavefront_versions_agree(gpu, name):
     p = p.copy()
     p.precision = 1
     base = None
-    for ver, tc in VARIANTS:
-        U, DU, v, t = run(gpu, p, case, {"OCFD_LU_V" + ver: "1", "OCFD_LU_TC": tc}, 3)
+    for ver, tc, extra in VARIANTS:
+        U, DU, v, t = run(gpu, p, case, dict({"OCFD_LU_V" + ver: "1", "OCFD_LU_TC": tc}, **extra), 3)
         assert (v, t) == (int(ver), int(tc))
         if base is None:
             base = (U, DU)
@@ -107,5 +115,6 @@ def test_autotuner_picks_a_known_variant(gpu):
     p, case = cases.config2_small()
     _, _, v, t = run(gpu, p, case, {}, 1)
     assert v in (3, 4, 5) and t in (32, 64)
+    assert not run.one_launch or v == 4
     _, _, v, t = run(gpu, p, case, {"OCFD_NO_AUTOTUNE": "1"}, 1)
     assert (v, t) == (4, 32)

@@ -738,12 +738,16 @@ struct Lu4Smem {
   static constexpr int SU = 0, SR = NV, SVOL = 2 * NV, SDT = 2 * NV + 1, SLC = 2 * NV + 2, SLV = 2 * NV + 5;
 };
 
-// one tile of a version-4 sweep (lower or upper), its progress published in progress[]
+// one tile of a version-4 sweep (lower or upper) for k_lusgs_wave4_ul, its progress published in
+// progress[]; the shared arrays are declared here, the dynamic ring is the kernel's
 template <class T, int NV, bool UPPER, int TC>
-__device__ __forceinline__ void lu4_tile(const Arena<T>& A, const LuArgs& L, const LuTile tl, int* progress, unsigned char* s_dyn,
-                                         double (&s_acc)[3][NV][TC], double (&s_pub)[NV][TC], double (&s_diag)[2][TC]) {
+__device__ __forceinline__ void lu4_tile(const Arena<T>& A, const LuArgs& L, const LuTile tl, int* progress) {
   using SM = Lu4Smem<NV, TC>;
   constexpr int CS = SM::CS, XS = SM::XS;
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  __shared__ double s_acc[3][NV][TC];      // direction terms of the current step
+  __shared__ double s_pub[NV][TC];         // DU of each column's last cell
+  __shared__ double s_diag[2][TC];         // the diagonal of the current step (all variables; the SA variable's)
   const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
   const int TJ = L.TJ, TK = L.TK;
   constexpr int NT = 4 * TC + 64, NC = 4 * TC;
@@ -755,329 +759,45 @@ __device__ __forceinline__ void lu4_tile(const Arena<T>& A, const LuArgs& L, con
   unsigned char* const dbuf = s_dyn + SM::DIR + (d < 3 ? d : 0) * 16 * CS + c * 16;  // stream s at + 4 s CS
   unsigned char* const xbuf = s_dyn + SM::XT + (d == 1 ? lk : TK + lj) * 16;        // stream s at + 4 s XS
   using RT = typename std::conditional<UPPER, double, T>::type;  // R: Res (lower) or DU* (upper)
-  const BlkD& B = A.blk[tl.blk];
-  const SolveP& s = A.sp[B.solve];
-  const int nxm = B.nx - 1, nym = B.ny - 1, nzm = B.nz - 1;
-  const int j = UPPER ? (tl.j0 + TJ - 1 - lj) : (tl.j0 + lj);
-  const int k = UPPER ? (tl.k0 + TK - 1 - lk) : (tl.k0 + lk);
-  const bool active = j >= 1 && j <= nym && k >= 1 && k <= nzm;
-  const int* tb3 = L.tile_of + 3 * tl.blk;
-  const int first = tb3[0], nJ = tb3[1], nK = tb3[2];
-  const int J = (tl.j0 - 1) / TJ, K = (tl.k0 - 1) / TK;
-  int pj = -1, pk = -1;
-  if (!UPPER) {
-    if (J > 0) pj = first + (J - 1) + nJ * K;
-    if (K > 0) pk = first + J + nJ * (K - 1);
-  } else {
-    if (J < nJ - 1) pj = first + (J + 1) + nJ * K;
-    if (K < nK - 1) pk = first + J + nJ * (K + 1);
-  }
-  const int my = first + J + nJ * K;
-  const int nsteps = nxm + TJ + TK - 2;
-  const double w = s.w_lu, gamma = s.gamma;
-  const bool visc = s.viscous == 1;
-  const bool dual = s.time_method == -1;
-  const double sfac1 = dual ? A.sfac[1] : 0.0;
-  const int off = UPPER ? 1 : -1;
-  auto i_of = [&](int t) { int il = t - lj - lk; return UPPER ? (nxm - il) : (il + 1); };
-  auto on_at = [&](int t) { int il = t - lj - lk; return active && il >= 0 && il < nxm; };
-  auto has_at = [&](int t) {
-    const int i = i_of(t);
-    return UPPER ? (d == 0 ? i != nxm : (d == 1 ? j != nym : k != nzm)) : (d == 0 ? i != 1 : (d == 1 ? j != 1 : k != 1));
-  };
-  auto need_dir = [&](int t) { return on_at(t) && has_at(t); };
-  const bool xt = !owner && ((d == 1 && lj == 0) || (d == 2 && lk == 0));
-  const int pubcol = d == 0 ? c : (d == 1 ? c - 1 : c - TJ);
-  const long long cb = B.ocell - 1 + (long long)nxm * ((j - 1) + (long long)nym * (k - 1));
-  const long long bb = B.obox + 3 + (long long)B.NX * ((j + 3) + (long long)B.NY * (k + 3));
-  const long long fb = B.oface - 1 + (long long)B.nx * ((j - 1) + (long long)B.ny * (k - 1));
-  const long long dcn = d == 0 ? off : (d == 1 ? (long long)off * nxm : (long long)off * nxm * nym);
-  const long long dbn = d == 0 ? off : (d == 1 ? (long long)off * B.NX : (long long)off * B.NX * B.NY);
-  const long long dfs = !UPPER ? 0 : (d == 0 ? 1 : (d == 1 ? (long long)B.nx : (long long)B.nx * B.ny));
-  // the planes of the streams (element index: the column base + i)
-  auto Rp = [&](int m, long long ci) {
-    if (UPPER) return (const RT*)(A.DU + m * tc + ci);  // DU* of the lower sweep, read before this column overwrites it
-    return (const RT*)(A.Res + m * tc + ci);
-  };
-  const T* const pn1 = A.M + (M_NI1 + 3 * d) * tf + fb;
-  const T* const pn2 = A.M + (M_NI2 + 3 * d) * tf + fb;
-  const T* const pn3 = A.M + (M_NI3 + 3 * d) * tf + fb;
-  const T* const pS = A.M + (M_SI + d) * tf + fb + dfs;  // the lower face's area, or the upper face's (sub_LU_SGS.f90:96-97)
-
-  auto issue_dir = [&](int u) {
-    if (need_dir(u)) {
-      const bool fresh = !need_dir(u - 1);
-      const int i = i_of(u);
-      sec_stage<UPPER>(dbuf, CS, pn1 + i, fresh);
-      sec_stage<UPPER>(dbuf + 4 * CS, CS, pn2 + i, fresh);
-      sec_stage<UPPER>(dbuf + 8 * CS, CS, pn3 + i, fresh);
-      sec_stage<UPPER>(dbuf + 12 * CS, CS, pS + i, fresh);
-      if (xt) {  // in-tile neighbours read their owner's streams instead
-        const long long bn = bb + i + dbn, cn = cb + i + dcn;
-#pragma unroll
-        for (int m = 0; m < NV; m++) sec_stage<UPPER>(xbuf + m * 4 * XS, XS, A.U + m * tb + bn, fresh);
-        sec_stage<UPPER>(xbuf + NV * 4 * XS, XS, A.Lc + d * tc + cn, fresh);
-        sec_stage<UPPER>(xbuf + (NV + 1) * 4 * XS, XS, A.Lv + d * tc + cn, fresh);
-      }
-    }
-    cpa_commit();
-  };
-  auto issue_own = [&](int u) {
-    if (on_at(u)) {
-      const bool fresh = !on_at(u - 1);
-      const int i = i_of(u);
-      const long long bi = bb + i, ci = cb + i;
-#pragma unroll
-      for (int m = 0; m < NV; m++) {
-        sec_stage<UPPER>(obuf(SM::SU + m, c), CS, A.U + m * tb + bi, fresh);
-        sec_stage<UPPER>(obuf(SM::SR + m, c), CS, Rp(m, ci), fresh);
-      }
-      sec_stage<UPPER>(obuf(SM::SVOL, c), CS, A.vold + ci, fresh);
-      sec_stage<UPPER>(obuf(SM::SDT, c), CS, A.dt + ci, fresh);
-#pragma unroll
-      for (int q2 = 0; q2 < 3; q2++) {
-        sec_stage<UPPER>(obuf(SM::SLC + q2, c), CS, A.Lc + q2 * tc + ci, fresh);
-        sec_stage<UPPER>(obuf(SM::SLV + q2, c), CS, A.Lv + q2 * tc + ci, fresh);
-      }
-    }
-    cpa_commit();
-  };
-
-  // direction thread state for the current step (as version 3)
-  using DFT = T;
-  DFT un1 = 0, F1[NV], n1 = 0, n2 = 0, n3 = 0, Unb[NV];
-  double S = 0.0, wLc = 0.0, Lvn = 0.0;
-  bool has = false;
-  // comput_DFn's U terms (sub_LU_SGS.f90:135-157) of step t: face data from this thread's
-  // streams; the neighbour's old state from the edge streams (cross-tile) or from its owner's
-  // streams (in tile: the neighbour is the owner column pubcol's cell of step t-1, complete
-  // since that owner's wait in step t-1, ordered before this read by barrier B2 of step t-1)
-  auto prep_dir = [&](int t) {
-    has = need_dir(t);
-    if (!has) return;
-    const int i = i_of(t);
-    n1 = (DFT)sec_get(dbuf, CS, pn1 + i);
-    n2 = (DFT)sec_get(dbuf + 4 * CS, CS, pn2 + i);
-    n3 = (DFT)sec_get(dbuf + 8 * CS, CS, pn3 + i);
-    S = (double)sec_get(dbuf + 12 * CS, CS, pS + i);
-    const long long bn = bb + i + dbn, cn = cb + i + dcn;
-    if (xt) {
-      Lvn = (double)sec_get(xbuf + (NV + 1) * 4 * XS, XS, A.Lv + d * tc + cn);
-      wLc = w * (double)sec_get(xbuf + NV * 4 * XS, XS, A.Lc + d * tc + cn);
-#pragma unroll
-      for (int m = 0; m < NV; m++) {
-        const double u = sec_get(xbuf + m * 4 * XS, XS, A.U + m * tb + bn);
-        Unb[m] = (DFT)(m >= 5 ? clamp0(u) : u);
-      }
-    } else {
-      Lvn = (double)sec_get(obuf(SM::SLV + d, pubcol), CS, A.Lv + d * tc + cn);
-      wLc = w * (double)sec_get(obuf(SM::SLC + d, pubcol), CS, A.Lc + d * tc + cn);
-#pragma unroll
-      for (int m = 0; m < NV; m++) {
-        const double u = sec_get(obuf(SM::SU + m, pubcol), CS, A.U + m * tb + bn);
-        Unb[m] = (DFT)(m >= 5 ? clamp0(u) : u);
-      }
-    }
-    const DFT g1 = (DFT)(gamma - 1.0), half = (DFT)0.5;
-    un1 = (Unb[1] * n1 + Unb[2] * n2 + Unb[3] * n3) / Unb[0];
-    const DFT p1 = g1 * (Unb[4] - half * (sq(Unb[1]) + sq(Unb[2]) + sq(Unb[3])) / Unb[0]);
-    F1[0] = Unb[0] * un1;
-    F1[1] = Unb[1] * un1 + p1 * n1;
-    F1[2] = Unb[2] * un1 + p1 * n2;
-    F1[3] = Unb[3] * un1 + p1 * n3;
-    F1[4] = (Unb[4] + p1) * un1;
-#pragma unroll
-    for (int m = 5; m < NV; m++) F1[m] = Unb[m] * un1;
-  };
-  // the diagonal of step t's cell (sub_LU_SGS.f90:50-62, 90-92), as version 3
-  auto diag_own = [&](int t) {
-    const long long ci = cb + i_of(t);
-    const double vol = sec_get(obuf(SM::SVOL, c), CS, A.vold + ci);
-    const double dt = (double)sec_get(obuf(SM::SDT, c), CS, A.dt + ci);
-    const double lc0 = (double)sec_get(obuf(SM::SLC, c), CS, A.Lc + ci);
-    const double lc1 = (double)sec_get(obuf(SM::SLC + 1, c), CS, A.Lc + tc + ci);
-    const double lc2 = (double)sec_get(obuf(SM::SLC + 2, c), CS, A.Lc + 2 * tc + ci);
-    const double a0 = vol / dt + w * (lc0 + lc1 + lc2);
-    double al = a0, als = a0;
-    if (visc) {
-      const double lv0 = (double)sec_get(obuf(SM::SLV, c), CS, A.Lv + ci);
-      const double lv1 = (double)sec_get(obuf(SM::SLV + 1, c), CS, A.Lv + tc + ci);
-      const double lv2 = (double)sec_get(obuf(SM::SLV + 2, c), CS, A.Lv + 2 * tc + ci);
-      const double lv = lv0 + lv1 + lv2;
-      al = al + 2.0 * lv;
-      als = als + 2.0 * lv;
-      if (NV == 6) {  // lower: + (Lv sum); upper: + Lv1 + Lv2 + Lv3 term by term (sub_LU_SGS.f90:60-62, 90-92)
-        if (!UPPER) als = als + lv;
-        else als = als + lv0 + lv1 + lv2;
-      }
-    }
-    if (dual) {  // dual time: + Sfac1 vol (sub_LU_SGS.f90:39, 92)
-      al = al + sfac1 * vol;
-      als = als + sfac1 * vol;
-    }
-    // the mixed form multiplies by the diagonal's FP64 reciprocal (taken here, off the chain);
-    // the FP64 form divides as the reference does
-    s_diag[0][c] = sizeof(T) == 4 ? 1.0 / al : al;
-    s_diag[1][c] = sizeof(T) == 4 ? 1.0 / (NV == 6 ? als : al) : (NV == 6 ? als : al);
-  };
-
-  int seen_j = 0, seen_k = 0;
-  auto poll = [&](int t) {  // upstream tiles far enough for step t
-    bool ok = true;
-    if (pj >= 0 && seen_j < min(t + TJ, nsteps)) ok &= wait_ge(progress + pj, min(t + TJ, nsteps), L.spin_limit, seen_j);
-    if (pk >= 0 && seen_k < min(t + TK, nsteps)) ok &= wait_ge(progress + pk, min(t + TK, nsteps), L.spin_limit, seen_k);
-    if (!ok) atomicExch(L.err, 1);
-  };
-
-  auto diag_of = [&](int m) { return (NV == 6 && m == 5) ? s_diag[1][c] : s_diag[0][c]; };
-  auto finish_val = [&](int m, long long ci) {  // sub_LU_SGS.f90:63-72 (lower), 108-117 (upper)
-    const double rm = (double)sec_get(obuf(SM::SR + m, c), CS, Rp(m, ci));
-    double r;
-    if (sizeof(T) == 4) {
-      if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) * diag_of(m);
-      else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) * diag_of(m);
-    } else {
-      if (!UPPER) r = (rm + s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
-      else r = rm + (s_acc[0][m][c] + s_acc[1][m][c] + s_acc[2][m][c]) / diag_of(m);
-    }
-    return r;
-  };
-  auto finish = [&](int m, long long ci) {
-    const double r = finish_val(m, ci);
-    A.DU[m * tc + ci] = r;
-    s_pub[m][c] = r;
-  };
-  if (grp == 4) {
-    // poller warp: the upstream tiles' progress for step t+2 during step t (before B1 of step
-    // t+1), so the cross-tile DU of step t+2 can be loaded at the end of step t+1
-    if (tid == 4 * TC) { poll(0); if (1 < nsteps) poll(1); }
-    cta_bar<NT>();  // B0
-    for (int t = 0; t < nsteps; t++) {
-      cta_bar<NT>();  // B1
-      if (tid == 4 * TC && t + 2 < nsteps) poll(t + 2);
-    }
-  } else if (grp == 5) {
-    // publisher warp: after B1 of step t every DU of the steps before t is stored (the barrier
-    // orders the compute threads' stores before this release)
-    cta_bar<NT>();  // B0
-    for (int t = 0; t < nsteps; t++) {
-      cta_bar<NT>();  // B1
-      if (tid == 4 * TC + 32 && t > 0) st_release(progress + my, t);
-    }
-  } else if (owner) {
-#pragma unroll
-    for (int u = 0; u < LU4_D; u++) issue_own(u);
-    cta_bar<NT>();  // B0
-    for (int t = 0; t < nsteps; t++) {
-      cta_bar<NT>();  // B1
-      cpa_wait<LU4_D - 1>();  // step t's sectors (only the groups of steps t+1.. may be outstanding)
-      if (on_at(t)) diag_own(t);
-      issue_own(t + LU4_D);
-      cta_bar_id<2, NC>();  // B2: the three direction terms of step t are in shared memory
-      if (on_at(t)) {
-        const long long ci = cb + i_of(t);
-        double r[NV];  // every value before the stores, so the divisions overlap
-#pragma unroll
-        for (int m = 3; m < NV; m++) r[m] = finish_val(m, ci);
-#pragma unroll
-        for (int m = 3; m < NV; m++) { A.DU[m * tc + ci] = r[m]; s_pub[m][c] = r[m]; }
-      }
-    }
-  } else {
-#pragma unroll
-    for (int u = 0; u < LU4_D; u++) issue_dir(u);
-    cpa_wait<LU4_D - 1>();
-    prep_dir(0);
-    double xdu[NV];  // cross-tile neighbour's DU of the current step, loaded one step early
-    auto load_xdu = [&](int t) {
-      const long long cn = cb + i_of(t) + dcn;
-#pragma unroll
-      for (int m = 0; m < NV; m++) xdu[m] = __ldcg(A.DU + m * tc + cn);
-    };
-    cta_bar<NT>();  // B0: the poller's first waits are done
-    if (xt && has) load_xdu(0);
-    for (int t = 0; t < nsteps; t++) {
-      cta_bar<NT>();  // B1: step t-1 finished (DU in s_pub and in HBM), upstream tiles ready
-      issue_dir(t + LU4_D);
-      if (has) {
-        double DUn[NV];
-        if (!xt) {
-#pragma unroll
-          for (int m = 0; m < NV; m++) DUn[m] = s_pub[m][pubcol];
-        } else {
-#pragma unroll
-          for (int m = 0; m < NV; m++) DUn[m] = xdu[m];
-        }
-        DFT U2[NV];
-#pragma unroll
-        for (int m = 0; m < NV; m++) U2[m] = (DFT)((double)Unb[m] + DUn[m]);
-        const DFT g1 = (DFT)(gamma - 1.0), half = (DFT)0.5;
-        const DFT un2 = (U2[1] * n1 + U2[2] * n2 + U2[3] * n3) / U2[0];
-        const DFT pp2 = g1 * (U2[4] - half * (sq(U2[1]) + sq(U2[2]) + sq(U2[3])) / U2[0]);
-        DFT DF[NV];
-        DF[0] = U2[0] * un2 - F1[0];
-        DF[1] = (U2[1] * un2 + pp2 * n1) - F1[1];
-        DF[2] = (U2[2] * un2 + pp2 * n2) - F1[2];
-        DF[3] = (U2[3] * un2 + pp2 * n3) - F1[3];
-        DF[4] = (U2[4] + pp2) * un2 - F1[4];
-#pragma unroll
-        for (int m = 5; m < NV; m++) DF[m] = U2[m] * un2 - F1[m];
-#pragma unroll
-        for (int m = 0; m < NV; m++) {
-          double v;
-          if (sizeof(T) == 4) {   // the mixed form: off-diagonal products in FP32, the sum stays FP64
-            const float du = (float)DUn[m];
-            float x;
-            if (!UPPER) x = 0.5f * ((float)DF[m] * (float)S + (float)wLc * du);
-            else x = -(0.5f * ((float)DF[m] * (float)S - (float)wLc * du));
-            if (visc) x = x + (float)Lvn * du;
-            v = (double)x;
-          } else {
-            if (!UPPER) v = 0.5 * ((double)DF[m] * S + wLc * DUn[m]);
-            else v = -(0.5 * ((double)DF[m] * S - wLc * DUn[m]));
-            if (visc) v = v + Lvn * DUn[m];
-          }
-          s_acc[d][m][c] = v;
-        }
-      } else if (on_at(t)) {
-#pragma unroll
-        for (int m = 0; m < NV; m++) s_acc[d][m][c] = 0.0;
-      }
-      cta_bar_id<2, NC>();  // B2
-      if (on_at(t)) finish(d, cb + i_of(t));
-      cpa_wait<LU4_D - 1>();  // step t+1's sectors
-      prep_dir(t + 1);
-      if (xt && has) load_xdu(t + 1);  // ready since the poller's wait of step t-1
-    }
-  }
-  cpa_wait<0>();  // no copy of this tile is still landing when the next tile reuses the slots
-  __syncthreads();
-  if (tid == 0) st_release(progress + my, nsteps);
+#include "lusgs4_tile.inc"
 }
 
 template <class T, int NV, bool UPPER, int TC>
 __global__ void __launch_bounds__(4 * TC + 64, OCFD_LU_MINB) k_lusgs_wave4(Arena<T> A, LuArgs L) {
   using SM = Lu4Smem<NV, TC>;
+  constexpr int CS = SM::CS, XS = SM::XS;
   extern __shared__ __align__(16) unsigned char s_dyn[];
   __shared__ int s_tile;
   __shared__ double s_acc[3][NV][TC];      // direction terms of the current step
   __shared__ double s_pub[NV][TC];         // DU of each column's last cell
   __shared__ double s_diag[2][TC];         // the diagonal of the current step (all variables; the SA variable's)
+  const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
+  const int TJ = L.TJ, TK = L.TK;
   // thread groups: 0..2 direction threads, 3 owner (TC threads each), 4 the poller warp (waits
   // for the upstream tiles' progress), 5 the publisher warp (releases this tile's progress).  The
   // two helper warps take barriers B0 and B1 only; B2 is a separate named barrier of the 4 TC
   // compute threads, so neither a release fence nor an acquire poll sits inside a step's phase.
-  const int tid = threadIdx.x;
-  if (L.TJ * L.TK != TC || L.TJ + L.TK > SM::XN) {  // tile shape outside the edge-stream table: refuse
+  constexpr int NT = 4 * TC + 64, NC = 4 * TC;
+  const int tid = threadIdx.x, grp = tid < 4 * TC ? tid / TC : (tid < 4 * TC + 32 ? 4 : 5), c = tid % TC;
+  const int lj = c % TJ, lk = c / TJ;
+  const bool owner = grp == 3;
+  const int d = grp;  // direction of a direction thread
+  if (TJ * TK != TC || TJ + TK > SM::XN) {  // tile shape outside the edge-stream table: refuse
     if (tid == 0) atomicExch(L.err, 1);
     return;
   }
+  auto obuf = [&](int s, int cc) { return s_dyn + SM::OWN + s * 4 * CS + cc * 16; };
+  unsigned char* const dbuf = s_dyn + SM::DIR + (d < 3 ? d : 0) * 16 * CS + c * 16;  // stream s at + 4 s CS
+  unsigned char* const xbuf = s_dyn + SM::XT + (d == 1 ? lk : TK + lj) * 16;        // stream s at + 4 s XS
+  using RT = typename std::conditional<UPPER, double, T>::type;  // R: Res (lower) or DU* (upper)
   for (;;) {
     if (tid == 0) s_tile = atomicAdd(&L.counter[UPPER ? 1 : 0], 1);
     __syncthreads();
     const int q = s_tile;
     if (q >= L.ntiles) break;
-    lu4_tile<T, NV, UPPER, TC>(A, L, L.tiles[UPPER ? (L.ntiles - 1 - q) : q], L.progress, s_dyn, s_acc, s_pub, s_diag);
+    const LuTile tl = L.tiles[UPPER ? (L.ntiles - 1 - q) : q];
+    int* const progress = L.progress;
+#include "lusgs4_tile.inc"
   }
 }
 
@@ -1095,11 +815,7 @@ __device__ __forceinline__ void red_release_add(int* p, int v) {
 template <class T, int NV, int TC>
 __global__ void __launch_bounds__(4 * TC + 64, OCFD_LU_MINB) k_lusgs_wave4_ul(Arena<T> A, LuArgs L) {
   using SM = Lu4Smem<NV, TC>;
-  extern __shared__ __align__(16) unsigned char s_dyn[];
   __shared__ int s_tile;
-  __shared__ double s_acc[3][NV][TC];
-  __shared__ double s_pub[NV][TC];
-  __shared__ double s_diag[2][TC];
   const int tid = threadIdx.x;
   if (L.TJ * L.TK != TC || L.TJ + L.TK > SM::XN) {
     if (tid == 0) atomicExch(L.err, 1);
@@ -1112,7 +828,7 @@ __global__ void __launch_bounds__(4 * TC + 64, OCFD_LU_MINB) k_lusgs_wave4_ul(Ar
     if (q >= 2 * L.ntiles) break;
     if (q < L.ntiles) {
       const LuTile tl = L.tiles[q];
-      lu4_tile<T, NV, false, TC>(A, L, tl, L.progress, s_dyn, s_acc, s_pub, s_diag);
+      lu4_tile<T, NV, false, TC>(A, L, tl, L.progress);
       if (tid == 0) red_release_add(L.blkdone + tl.blk, 1);  // after this tile's release of its progress
     } else {
       const LuTile tl = L.utiles[q - L.ntiles];
@@ -1122,7 +838,7 @@ __global__ void __launch_bounds__(4 * TC + 64, OCFD_LU_MINB) k_lusgs_wave4_ul(Ar
         if (!wait_ge(L.blkdone + tl.blk, tb3[1] * tb3[2], L.spin_limit, seen)) atomicExch(L.err, 1);
       }
       __syncthreads();
-      lu4_tile<T, NV, true, TC>(A, L, tl, L.progress_up, s_dyn, s_acc, s_pub, s_diag);
+      lu4_tile<T, NV, true, TC>(A, L, tl, L.progress_up);
     }
   }
 }

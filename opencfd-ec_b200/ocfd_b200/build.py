@@ -28,7 +28,7 @@ UNITS = [
 
 def sources():
     """Everything the library depends on, this file (its compiler flags) included."""
-    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))] + [
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h", ".inc"))] + [
         os.path.join(os.path.dirname(ROOT_DIR), "include", "ocfd_ec_gpu.h"), os.path.abspath(__file__)]
 
 

@@ -148,9 +148,12 @@ class RunnerT : public Runner {
       }
       k_amut<T><<<grid_of(A.tot_subcell), 256, 0, cs>>>(A);
     }
-    // forked: the spectral radii and dt (they need mu and mu_t) follow the inviscid fluxes on their
-    // stream, beside the viscous fluxes, and the assembly stores Res only
-    if (fork) {
+    // forked, FP64: the spectral radii and dt (they need mu and mu_t) follow the inviscid fluxes on
+    // their stream, beside the viscous fluxes, and the assembly stores Res only (config 2 step
+    // -36 us).  The mixed form keeps them in the assembly: written just before the LU-SGS sweeps,
+    // its FP32 Lc, Lv and dt are still in L2 when the sweeps read them (-19 us; batch -47 us)
+    const bool ldt_apart = fork && sizeof(T) == 8;
+    if (ldt_apart) {
       cudaEventRecord(ev_mu_, cs);
       cudaStreamWaitEvent(is, ev_mu_, 0);
       k_cell_dt<T><<<grid_of(tc), 256, 0, is>>>(A);
@@ -183,7 +186,8 @@ class RunnerT : public Runner {
         cudaStream_t other = cs == st ? is : cs;
         cudaEventRecord(ev_join_, other);
         cudaStreamWaitEvent(st, ev_join_, 0);
-        k_assemble<T, true><<<grid_of(tc), 256, 0, st>>>(A);
+        if (ldt_apart) k_assemble<T, true><<<grid_of(tc), 256, 0, st>>>(A);
+        else k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
       } else {
         k_assemble<T><<<grid_of(tc), 256, 0, st>>>(A);
       }
@@ -377,7 +381,7 @@ class RunnerT : public Runner {
     if (I_.res_fused == 1) res += 1;
     else if (I_.res_fused == 2) res += vis + 1;
     else if (I_.res_fused == 3) res += 4 + 1;
-    else res += 4 + vis + 1 + (st2_ ? 1 : 0);  // forked: k_cell_dt beside the viscous fluxes
+    else res += 4 + vis + 1 + (st2_ && sizeof(T) == 8 ? 1 : 0);  // forked FP64: k_cell_dt beside the viscous fluxes
     if (I_.viscous) {
       res += 1 + 1;  // mu, amut
       if (I_.turb == 2 && NV == 6) res += I_.sa_fused ? 3 : 6;  // sa_pre, (tile | 3 fluxes + res), mu_finish

@@ -241,12 +241,21 @@ def batch_leg(args, nsteps=100):
     launches = b.launches_per_step()
     phases = {k: v / 3 for k, v in b.profile(3).items()}   # ms per step, CUDA events on the handle's stream
     lu = (b.lu_kernel_version(), b.lu_tile_width())
+    one_launch = b.lu_one_launch()
     b.close()
-    # roofline per phase: the phase's algorithmic bytes per cell (mixed, NV = 6) x cells / its time
+    # roofline per phase: the phase's algorithmic bytes per cell (mixed, NV = 6) x cells / its time;
+    # when both LU-SGS sweeps run as one launch, profile() reports their joint time as the lower one
     peak, peak_kind = peaks()
-    bm = BYTES[("mixed", 6)]
+    bm = dict(BYTES[("mixed", 6)])
+    keys = ("residual", "lusgs_lower", "lusgs_upper")
+    if one_launch:
+        bm["lusgs_both"] = bm["lusgs_lower"] + bm["lusgs_upper"]
+        phases = dict(phases)
+        phases["lusgs_both"] = phases.pop("lusgs_lower")
+        phases.pop("lusgs_upper", None)
+        keys = ("residual", "lusgs_both")
     roof = {}
-    for k in ("residual", "lusgs_lower", "lusgs_upper"):
+    for k in keys:
         if phases.get(k, 0.0) > 0.0:
             gbs = bm[k] * cells / (phases[k] * 1e-3) / 1e9
             roof[k] = {"bytes_per_cell": bm[k], "achieved_GBps": gbs, "frac": gbs / peak}
@@ -254,7 +263,7 @@ def batch_leg(args, nsteps=100):
             "cells": cells, "value": cells * n / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms / n,
             "steps": n, "launches_per_step": launches, "phase_ms_per_step": phases,
             "phase_roofline": roof, "peak_GBps": peak, "peak_kind": peak_kind,
-            "lu_kernel": {"version": lu[0], "tile_columns": lu[1]}}
+            "lu_kernel": {"version": lu[0], "tile_columns": lu[1], "both_sweeps_one_launch": one_launch}}
 
 
 def sweep_serving_leg(max_iters=3000, rate=4.0, seed=99):

@@ -340,11 +340,10 @@ int ocfd_launches_per_step(ocfd_handle* h);
 int ocfd_lu_tile_width(const ocfd_handle* h);
 int ocfd_lu_kernel_version(const ocfd_handle* h);
 /* 1 when the two LU-SGS sweeps run as one launch: version 4 in which a block's upper sweep starts
- * as soon as its own lower sweep is done, while deeper blocks still run theirs.  The creation-time
- * autotuner times it beside the two-launch forms (it wins where blocks of very different depth run
- * together, as in a batch of airfoils); OCFD_LU_SPLIT=1 leaves it out, OCFD_LU_ONE_LAUNCH=1 keeps
- * only it for version 4.  ocfd_profile then reports the joint time as the lower sweep's and 0 for
- * the upper. */
+ * as soon as its own lower sweep is done, while deeper blocks still run theirs (OCFD_LU_ONE_LAUNCH=1
+ * puts it in version 4's place; same results, measured slower than the two launches once tiles are
+ * taken longest first within a level).  ocfd_profile then reports the joint time as the lower
+ * sweep's and 0 for the upper. */
 int ocfd_lu_one_launch(const ocfd_handle* h);
 
 #ifdef __cplusplus

@@ -997,8 +997,21 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
         for (int J = 0; J < nJ; J++) order.push_back({J + K, LuTile{b, 1 + J * TJ, 1 + K * TK, 0}});
       first += nJ * nK;
     }
-    std::stable_sort(order.begin(), order.end(), [](const std::pair<int, LuTile>& a, const std::pair<int, LuTile>& b) { return a.first < b.first; });
+    // within a level (tiles that do not wait on one another) the longer tiles first, so that the
+    // blocks with the longest i-lines start their march early
+    auto longer = [&](const LuTile& a, const LuTile& c) { return h->blk[a.blk].nx > h->blk[c.blk].nx; };
+    std::stable_sort(order.begin(), order.end(), [&](const std::pair<int, LuTile>& a, const std::pair<int, LuTile>& b) {
+      return a.first != b.first ? a.first < b.first : longer(a.second, b.second);
+    });
     for (auto& o : order) tiles.push_back(o.second);
+    std::vector<std::pair<int, LuTile>> rorder(order.begin(), order.end());
+    std::stable_sort(rorder.begin(), rorder.end(), [&](const std::pair<int, LuTile>& a, const std::pair<int, LuTile>& b) {
+      // the upper sweep: a tile waits on the next level's tiles of its block (J+1, K+1)
+      const int la = -(a.first + 0), lb = -(b.first + 0);
+      return la != lb ? la < lb : longer(a.second, b.second);
+    });
+    std::vector<LuTile> rtiles;
+    for (auto& o : rorder) rtiles.push_back(o.second);
     // the upper sweep's order when both sweeps share one launch: by the step at which a tile could
     // start (its block's lower sweep done, then the skew of its upstream tiles); an upstream tile
     // (J+1 or K+1) always sorts strictly earlier, so every wait is on a tile handed out before
@@ -1015,6 +1028,7 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     for (auto& o : uorder) utiles.push_back(o.second);
     LuTile* d_tiles = M.alloc<LuTile>(tiles.size(), e);
     LuTile* d_utiles = M.alloc<LuTile>(utiles.size(), e);
+    LuTile* d_rtiles = M.alloc<LuTile>(rtiles.size(), e);
     int* d_tile_of = M.alloc<int>(tile_of.size(), e);
     int* d_progress = M.alloc<int>(first, e);
     int* d_progress_up = M.alloc<int>(first, e);
@@ -1022,9 +1036,10 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
     if (e != cudaSuccess) { M.release(); return cuda_fail(nullptr, e, "lu tables"); }
     cudaMemcpy(d_tiles, tiles.data(), tiles.size() * sizeof(LuTile), cudaMemcpyHostToDevice);
     cudaMemcpy(d_utiles, utiles.data(), utiles.size() * sizeof(LuTile), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_rtiles, rtiles.data(), rtiles.size() * sizeof(LuTile), cudaMemcpyHostToDevice);
     cudaMemcpy(d_tile_of, tile_of.data(), tile_of.size() * sizeof(int), cudaMemcpyHostToDevice);
     LuArgs& L = h->lu_var[v];
-    L.tiles = d_tiles; L.utiles = d_utiles; L.ntiles = first; L.counter = d_counter; L.progress = d_progress;
+    L.tiles = d_tiles; L.rtiles = d_rtiles; L.utiles = d_utiles; L.ntiles = first; L.counter = d_counter; L.progress = d_progress;
     L.progress_up = d_progress_up; L.blkdone = d_blkdone;
     L.tile_of = d_tile_of; L.err = h->d_lu_err; L.TJ = TJ; L.TK = TK;
     L.spin_limit = 4000000;  // x ~64 ns: a few hundred ms before a stuck wait gives up
@@ -1120,20 +1135,17 @@ static int create_impl(const ocfd_params* ps, int nsolve, const int* nblk_s, con
   if (h->prec == OCFD_PREC_MIXED) fill_arena<float>(h, h->A32, h->d_Mf, h->d_volf, h->d_dtmf, h->d_dwf);
   else fill_arena<double>(h, h->A64, h->d_Md, h->d_vold, h->d_dtmd, h->d_dwd);
   // LU-SGS kernel candidates: OCFD_LU_TC fixes the tile width, OCFD_LU_V3 / OCFD_LU_V4 the
-  // wavefront version (OCFD_LU_V2 both); the autotuner picks among the rest.  Candidate 6 is
-  // version 4 with both sweeps in one launch (k_lusgs_wave4_ul: faster where blocks of very
-  // different depth run together, as in a batch; OCFD_LU_SPLIT leaves it out)
+  // wavefront version (OCFD_LU_V2 both); the autotuner picks among the rest.  OCFD_LU_ONE_LAUNCH
+  // replaces version 4 by its one-launch form (candidate 6: k_lusgs_wave4_ul)
   const int lu_ver_force = lu_v2 ? 2 : (std::getenv("OCFD_LU_V3") ? 3 : (std::getenv("OCFD_LU_V4") ? 4 : (std::getenv("OCFD_LU_V5") ? 5 : 0)));
-  const bool lu_split = std::getenv("OCFD_LU_SPLIT") != nullptr, lu_one = std::getenv("OCFD_LU_ONE_LAUNCH") != nullptr;
+  const bool lu_one = std::getenv("OCFD_LU_ONE_LAUNCH") != nullptr;
   std::vector<std::pair<int, int>> lu_cand;
   for (int v = 0; v < 2; v++) {
     if (lu_force && (lu_force == 64) != (v == 1)) continue;
-    for (int ver : {5, 4, 6, 3}) {
-      if (lu_ver_force && ver != lu_ver_force && !(ver == 6 && lu_ver_force == 4)) continue;
+    for (int ver : {5, 4, 3}) {
+      if (lu_ver_force && ver != lu_ver_force) continue;
       if (ver == 5 && (h->lus_v != v || lu_ver_force != 5)) continue;
-      if (ver == 6 && lu_split) continue;
-      if (ver == 4 && lu_one && !lu_split) continue;
-      lu_cand.push_back({v, ver});
+      lu_cand.push_back({v, ver == 4 && lu_one ? 6 : ver});
     }
   }
   if (lu_cand.empty()) lu_cand.push_back({1, 4});

@@ -31,7 +31,8 @@ struct LuTile {
 };
 
 struct LuArgs {
-  const LuTile* tiles;  // lower-sweep order (J+K ascending); the upper sweep walks it backwards
+  const LuTile* tiles;  // lower-sweep order: J+K ascending, the longer tiles first within a level
+  const LuTile* rtiles; // upper-sweep order: J+K descending, the longer tiles first within a level
   const LuTile* utiles; // the upper sweep's order when both sweeps share one launch (k_lusgs_wave4_ul)
   int ntiles;
   int* counter;         // [0] lower, [1] upper tile counters
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(64) k_lusgs_wave(Arena<T> A, LuArgs L) {
     __syncthreads();
     const int q = s_tile;
     if (q >= L.ntiles) break;
-    const LuTile tl = L.tiles[UPPER ? (L.ntiles - 1 - q) : q];
+    const LuTile tl = UPPER ? L.rtiles[q] : L.tiles[q];
     const BlkD& B = A.blk[tl.blk];
     const SolveP& s = A.sp[B.solve];
     const int nxm = B.nx - 1, nym = B.ny - 1, nzm = B.nz - 1;
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(4 * TC + 32, OCFD_LU_MINB) k_lusgs_wave3(Arena
     __syncthreads();
     const int q = s_tile;
     if (q >= L.ntiles) break;
-    const LuTile tl = L.tiles[UPPER ? (L.ntiles - 1 - q) : q];
+    const LuTile tl = UPPER ? L.rtiles[q] : L.tiles[q];
     const BlkD& B = A.blk[tl.blk];
     const SolveP& s = A.sp[B.solve];
     const int nxm = B.nx - 1, nym = B.ny - 1, nzm = B.nz - 1;
@@ -795,7 +796,7 @@ __global__ void __launch_bounds__(4 * TC + 64, OCFD_LU_MINB) k_lusgs_wave4(Arena
     __syncthreads();
     const int q = s_tile;
     if (q >= L.ntiles) break;
-    const LuTile tl = L.tiles[UPPER ? (L.ntiles - 1 - q) : q];
+    const LuTile tl = UPPER ? L.rtiles[q] : L.tiles[q];
     int* const progress = L.progress;
 #include "lusgs4_tile.inc"
   }

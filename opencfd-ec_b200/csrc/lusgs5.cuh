@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(4 * TC + 32, 2) k_lusgs_wave5(Arena<T> A, LuAr
     __syncthreads();
     const int qq = s_tile;
     if (qq >= L.ntiles) break;
-    const LuTile tl = L.tiles[UPPER ? (L.ntiles - 1 - qq) : qq];
+    const LuTile tl = UPPER ? L.rtiles[qq] : L.tiles[qq];
     const BlkD& B = A.blk[tl.blk];
     const SolveP& sp = A.sp[B.solve];
     const int nxm = B.nx - 1, nym = B.ny - 1, nzm = B.nz - 1;

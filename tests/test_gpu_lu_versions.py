@@ -1,8 +1,8 @@
 """Every LU-SGS wavefront variant gives the hyperplane-order bits.
 
 The creation-time autotuner picks a tile width (32 or 64 columns) and a wavefront kernel version
-(3: inputs staged by element; 4: staged by 32-byte sector, helper warps off the step phases, both
-sweeps in one launch unless OCFD_LU_SPLIT; 5:
+(3: inputs staged by element; 4: staged by 32-byte sector, helper warps off the step phases, or
+with both sweeps in one launch when OCFD_LU_ONE_LAUNCH is set; 5:
 inputs packed in sweep order and fetched by one bulk copy per step, 64-column tiles) per case; the
 choice must never change a result.  Each variant is forced here through its switches and
 compared bit for bit with the one-launch-per-hyperplane sweep (OCFD_LUSGS_PLANES=1), on cases that
@@ -17,12 +17,11 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SWITCHES = ("OCFD_LU_V3", "OCFD_LU_V4", "OCFD_LU_V5", "OCFD_LU_TC", "OCFD_LUSGS_PLANES", "OCFD_NO_AUTOTUNE", "OCFD_LU_SPLIT",
+SWITCHES = ("OCFD_LU_V3", "OCFD_LU_V4", "OCFD_LU_V5", "OCFD_LU_TC", "OCFD_LUSGS_PLANES", "OCFD_NO_AUTOTUNE",
             "OCFD_LU_ONE_LAUNCH")
-# (version, tile width, extra switches): version 4 as two launches (OCFD_LU_SPLIT) and with both
-# sweeps in one launch (OCFD_LU_ONE_LAUNCH)
-SPLIT, ONE = {"OCFD_LU_SPLIT": "1"}, {"OCFD_LU_ONE_LAUNCH": "1"}
-VARIANTS = (("3", "32", {}), ("3", "64", {}), ("4", "32", SPLIT), ("4", "64", SPLIT), ("4", "32", ONE), ("4", "64", ONE),
+# (version, tile width, extra switches): version 4 also with both sweeps in one launch
+ONE = {"OCFD_LU_ONE_LAUNCH": "1"}
+VARIANTS = (("3", "32", {}), ("3", "64", {}), ("4", "32", {}), ("4", "64", {}), ("4", "32", ONE), ("4", "64", ONE),
             ("5", "64", {}))
 
 

@@ -94,13 +94,13 @@ class RunnerT : public Runner {
     const Arena<T>& A = A_;
     const long long tb = A.tot_box, tf = A.tot_face, tc = A.tot_cell;
     k_prim<T><<<grid_of(tb), 256, 0, st>>>(A);  // sized for the box: the region is read on the device
-    // the inviscid fluxes read only the primitives and the metrics: on two streams they run beside
-    // the viscosity / turbulence chain and the viscous fluxes (FP64 arithmetic beside memory
-    // latency), joined before the assembly; the chain, the longer path, gets the higher priority
     // specialised instantiations for the WENO5 / MUSCL3 + Roe pairs (residual phase -3 % on
     // config 2 FP64, -8 % on config 1; MUSCL3 + AUSMPW was measured slower and is left general)
     const bool weno5_roe = I_.recon_prim && I_.int_scheme == S_WENO5 && I_.int_flux == F_ROE;
     const bool muscl3_roe = I_.recon_prim && I_.int_scheme == S_MUSCL3 && I_.int_flux == F_ROE;
+    // the inviscid fluxes read only the primitives and the metrics: on two streams they run beside
+    // the viscosity / turbulence chain and the viscous fluxes (FP64 arithmetic beside memory
+    // latency), joined before the assembly; the chain, the longer path, gets the higher priority
     const bool fork = st2_ != nullptr;
     auto inviscid = [&](cudaStream_t s) {
       if (weno5_roe) inv_flux<true, S_WENO5, F_ROE>(s);
@@ -159,11 +159,7 @@ class RunnerT : public Runner {
       k_cell_dt<T><<<grid_of(tc), 256, 0, is>>>(A);
     }
     if (I_.res_fused == 3) {
-      if (weno5_roe) inv_flux<true, S_WENO5, F_ROE>(st);
-      else if (muscl3_roe) inv_flux<true, S_MUSCL3, F_ROE>(st);
-      else if (I_.recon_prim) inv_flux<true, -1, -1>(st);
-      else inv_flux<false, -1, -1>(st);
-      k_inv_kbc<T><<<grid_of(A.tot_subcell), 256, 0, st>>>(A);
+      inviscid(st);
       k_ns_tile<T, true, -1, -1, true, false><<<ns_grid_[4], 256, sizeof(T) * 5 * ((size_t)A.tile_maxf + A.tile_maxc), st>>>(A);
     } else if (I_.res_fused) {
       if (I_.res_fused == 2 && I_.viscous) {

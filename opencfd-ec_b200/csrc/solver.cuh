@@ -744,6 +744,9 @@ __global__ void __launch_bounds__(256, InvFluxOccS<T, ISCH>::value) k_inv_flux(A
     if (DIR == 0 && (j == B.ny || k == B.nz)) continue;
     if (DIR == 1 && (i == B.nx || k == B.nz)) continue;
     if (DIR == 2 && (i == B.nx || j == B.ny)) continue;
+    // a physical k face with bc > 0 takes k_inv_kbc's central flux, which overwrites this one: skip
+    // it (two of the three k planes of the batch's two-cell-thick airfoils)
+    if (DIR == 2 && (k == 1 || k == B.nz) && (A.bck[B.obck + (i - 1) + (long long)(B.nx - 1) * (j - 1)] & (k == 1 ? 4 : 8))) continue;
     T F[5];
     inv_face<T, DIR, PRIM, ISCH, IFLUX>(A, B, A.sp[B.solve], b, i, j, k, g, F);
     T* Fo = A.Fi + (long long)DIR * 5 * tf + g;

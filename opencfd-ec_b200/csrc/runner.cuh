@@ -174,9 +174,16 @@ class RunnerT : public Runner {
     } else {
       if (!fork) inviscid(st);
       if (I_.viscous) {
+        // forked: the k-direction viscous fluxes follow the inviscid ones (and k_cell_dt) on their
+        // stream once mu and mu_t are final, which evens the two streams (same-box A/B: config 2
+        // FP64 step -6 us, mixed -16 us, batch -24 us; moving a second direction measured slower)
+        if (fork && !ldt_apart) {
+          cudaEventRecord(ev_mu_, cs);
+          cudaStreamWaitEvent(is, ev_mu_, 0);
+        }
         k_visc_flux<T, 0><<<grid_of(tf), 256, 0, cs>>>(A);
         k_visc_flux<T, 1><<<grid_of(tf), 256, 0, cs>>>(A);
-        k_visc_flux<T, 2><<<grid_of(tf), 256, 0, cs>>>(A);
+        k_visc_flux<T, 2><<<grid_of(tf), 256, 0, fork ? is : cs>>>(A);
       }
       if (fork) {  // join the second stream back into the handle's
         cudaStream_t other = cs == st ? is : cs;

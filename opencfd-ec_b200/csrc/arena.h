@@ -104,6 +104,7 @@ struct Arena {
   long long tot_r1;
   const int4* tiles;  // residual tiles (block, first cell i, j, k), block by block, i fastest
   int ntile, tile_maxf, tile_maxc;  // largest face count of one direction / cell count of a tile
+  int tile_maxb;                     // largest (tile + one layer) box, (ti+2)(tj+2)(tk+2) cells
   // geometry
   const double *x, *y, *z;   // node
   const double* Md;          // 48 FP64 metric planes (face)

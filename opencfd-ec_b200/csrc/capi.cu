@@ -90,7 +90,7 @@ struct ocfd_handle {
   long long tot_reg = 0, tot_r1 = 0;
   std::vector<unsigned char> phys;  // per block and face (d*2+side): every face cell physical
   int4* d_tiles = nullptr;
-  int ntile = 0, tile_maxf = 0, tile_maxc = 0;
+  int ntile = 0, tile_maxf = 0, tile_maxc = 0, tile_maxb = 0;
   long long *d_pre_reg = nullptr, *d_pre_r1 = nullptr;
   int *d_hint_reg = nullptr, *d_hint_r1 = nullptr;
   std::vector<int4> cchunk, wchunk;
@@ -315,7 +315,7 @@ static void fill_arena(ocfd_handle* h, Arena<T>& A, const T* M, const T* vol, co
   A.hint_box = h->d_hint_box; A.hint_cell = h->d_hint_cell; A.hint_face = h->d_hint_face;
   A.pre_reg = h->d_pre_reg; A.pre_r1 = h->d_pre_r1; A.hint_reg = h->d_hint_reg; A.hint_r1 = h->d_hint_r1;
   A.tot_r1 = h->tot_r1;
-  A.tiles = h->d_tiles; A.ntile = h->ntile; A.tile_maxf = h->tile_maxf; A.tile_maxc = h->tile_maxc;
+  A.tiles = h->d_tiles; A.ntile = h->ntile; A.tile_maxf = h->tile_maxf; A.tile_maxc = h->tile_maxc; A.tile_maxb = h->tile_maxb;
   A.pre_lnj = h->d_pre_lnj; A.pre_lnk = h->d_pre_lnk; A.tot_lnj = h->pre_lnj[h->nblk]; A.tot_lnk = h->pre_lnk[h->nblk];
   A.sub = h->d_sub; A.nsub = (int)h->sub.size();
   A.pre_subcell = h->d_pre_subcell; A.pre_halo = h->d_pre_halo;
@@ -527,6 +527,7 @@ static std::vector<int4> tile_table(ocfd_handle* h) {
   std::vector<int4> t;
   h->tile_maxf = 1;
   h->tile_maxc = 1;
+  h->tile_maxb = 1;
   int TI = 16, TK = 4, NC = 512;  // OCFD_RES_TILE="i,k,cells" overrides (tile-shape measurements)
   if (const char* e = std::getenv("OCFD_RES_TILE")) {
     int a = 0, c = 0, n = 0;
@@ -538,6 +539,7 @@ static std::vector<int4> tile_table(ocfd_handle* h) {
     const int tj = std::min(B.ny - 1, std::max(1, NC / (ti * tk)));
     B.tdim[0] = ti; B.tdim[1] = tj; B.tdim[2] = tk;
     h->tile_maxc = std::max(h->tile_maxc, ti * tj * tk);
+    h->tile_maxb = std::max(h->tile_maxb, (ti + 2) * (tj + 2) * (tk + 2));
     h->tile_maxf = std::max({h->tile_maxf, (ti + 1) * tj * tk, ti * (tj + 1) * tk, ti * tj * (tk + 1)});
     for (int k = 1; k < B.nz; k += tk)
       for (int j = 1; j < B.ny; j += tj)

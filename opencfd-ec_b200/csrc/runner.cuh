@@ -207,7 +207,7 @@ class RunnerT : public Runner {
     }
   }
 
-  size_t sa_smem() const { return sizeof(T) * (2 * (size_t)A_.tile_maxf + 2 * (size_t)A_.tile_maxc); }
+  size_t sa_smem() const { return sizeof(T) * (2 * (size_t)A_.tile_maxf + 2 * (size_t)A_.tile_maxc + (size_t)A_.tile_maxb); }
   template <bool PRIM, int ISCH, int IFLUX>
   size_t ns_smem() const { return sizeof(T) * 5 * ((size_t)A_.tile_maxf + A_.tile_maxc); }
   template <bool PRIM, int ISCH, int IFLUX>

@@ -172,13 +172,22 @@ __global__ void k_sa_pre(Arena<T> A) {
 }
 
 // SA face fluxes Fluxv / Fluxv2 (SA.f90:74-96, 110-131, 145-167) for direction DIR
+template <class T, int DIR, class VT>
+__device__ __forceinline__ void sa_face_vt(const Arena<T>& A, const BlkD& B, const SolveP& s, int i, int j, int k, long long g, T& Fo,
+                                           T& Go, VT vt);
 // one face of direction DIR: the SA convection + diffusion flux F and the gradient flux G (the
 // face's two Ft plane entries)
 template <class T, int DIR>
 __device__ __forceinline__ void sa_face(const Arena<T>& A, const BlkD& B, const SolveP& s, int i, int j, int k, long long g, T& Fo,
                                         T& Go) {
+  const long long tb = A.tot_box;
+  sa_face_vt<T, DIR>(A, B, s, i, j, k, g, Fo, Go, [&](int a, int c, int e) -> T { return T(clamp0(A.U[5 * tb + bix(B, a, c, e)])); });
+}
+// the same, the SA variable's values (clamped at 0) from vt(i, j, k)
+template <class T, int DIR, class VT>
+__device__ __forceinline__ void sa_face_vt(const Arena<T>& A, const BlkD& B, const SolveP& s, int i, int j, int k, long long g, T& Fo,
+                                           T& Go, VT vt) {
   const long long tb = A.tot_box, tf = A.tot_face;
-  auto vt = [&](int a, int c, int e) -> T { return T(clamp0(A.U[5 * tb + bix(B, a, c, e)])); };
   const int di = DIR == 0, dj = DIR == 1, dk = DIR == 2;
   const int im = i - di, jm = j - dj, km = k - dk;  // the other cell of the face
   T s1x = A.M[(M_NI1 + 3 * DIR) * tf + g], s1y = A.M[(M_NI2 + 3 * DIR) * tf + g], s1z = A.M[(M_NI3 + 3 * DIR) * tf + g];
@@ -297,16 +306,20 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_res(Arena<T> A) {
 // Res(6) of a tile of cells in one pass: the SA face fluxes F, G of direction i, then j, then k, in
 // shared memory, each cell adding its two faces' terms in the order of k_sa_res, then the source;
 // bit-equal to k_sa_flux + k_sa_res without the Ft planes (faces on a tile border are computed by
-// both tiles that share them)
+// both tiles that share them).  The SA variable of the tile and one layer around it, which every
+// face's gradient stencil reads about ten times, is staged in shared memory first.
 template <class T, int DIR>
 __device__ __forceinline__ void tile_sa_dir(const Arena<T>& A, const BlkD& B, const SolveP& s, int i0, int j0, int k0, int ni, int nj,
-                                            int nk, T* Fs, T* Rs, const T* Vs) {
+                                            int nk, T* Fs, T* Rs, const T* Vs, const T* Vt) {
   const int fa = ni + (DIR == 0), fb = nj + (DIR == 1), fc = nk + (DIR == 2);
   const int nf = fa * fb * fc, MF = A.tile_maxf;
+  // the tile's SA values with one layer around it, staged in shared memory (box ni+2 x nj+2 x nk+2)
+  const int bx = ni + 2, by = nj + 2;
+  auto vt = [&](int a, int c, int e) -> T { return Vt[(a - i0 + 1) + bx * ((c - j0 + 1) + by * (e - k0 + 1))]; };
   for (int q = threadIdx.x; q < nf; q += blockDim.x) {
     const int a = q % fa, r = q / fa, bb = r % fb, c = r / fb;
     T F, G;
-    sa_face<T, DIR>(A, B, s, i0 + a, j0 + bb, k0 + c, fix_(B, i0 + a, j0 + bb, k0 + c), F, G);
+    sa_face_vt<T, DIR>(A, B, s, i0 + a, j0 + bb, k0 + c, fix_(B, i0 + a, j0 + bb, k0 + c), F, G, vt);
     Fs[q] = F;
     Fs[MF + q] = G;
   }
@@ -331,6 +344,7 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_tile(Arena<T> A) {
   T* Fs = reinterpret_cast<T*>(sa_smem);
   T* Rs = Fs + 2 * A.tile_maxf;
   T* Vs = Rs + A.tile_maxc;
+  T* Vt = Vs + A.tile_maxc;  // (tile + 1 layer) box of the SA variable, at most tile_maxb values
   const long long tb = A.tot_box;
   for (int t = blockIdx.x; t < A.ntile; t += gridDim.x) {
     const int4 tl = A.tiles[t];
@@ -345,9 +359,15 @@ __global__ void __launch_bounds__(256, OCFD_MEM_MINB) k_sa_tile(Arena<T> A) {
       T vt0 = T(clamp0(A.U[5 * tb + c])), mu0 = A.mu[c], d0 = A.P[P_D * tb + c];
       Vs[q] = (vt0 + mu0 / d0) * T(sa::Cb2) / T(sa::sigma);
     }
-    tile_sa_dir<T, 0>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs, Vs);
-    tile_sa_dir<T, 1>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs, Vs);
-    tile_sa_dir<T, 2>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs, Vs);
+    const int bx = ni + 2, by = nj + 2, nb = bx * by * (nk + 2);
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+      const int a = q % bx, r = q / bx;
+      Vt[q] = T(clamp0(A.U[5 * tb + bix(B, i0 - 1 + a, j0 - 1 + r % by, k0 - 1 + r / by)]));
+    }
+    __syncthreads();  // the faces of direction i read the staged box
+    tile_sa_dir<T, 0>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs, Vs, Vt);
+    tile_sa_dir<T, 1>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs, Vs, Vt);
+    tile_sa_dir<T, 2>(A, B, s, i0, j0, k0, ni, nj, nk, Fs, Rs, Vs, Vt);
     for (int q = threadIdx.x; q < nc; q += blockDim.x) {
       const int i = i0 + q % ni, r = q / ni, j = j0 + r % nj, k = k0 + r / nj;
       const long long c = bix(B, i, j, k);
